@@ -1,0 +1,459 @@
+// p3m_fft.cu — real 2D FFT with the Green's-function multiply fused in.
+//
+// Replaces fft_init.comp, fft_shared.comp (forward + two inverse complex 2D
+// transforms, GravityPipeline.kt:944-972), convolve.comp and the kernel
+// spectra of kernel_init.comp (GravityPipeline.kt:1341-1357).
+//
+// The reference transforms the real density as a full complex mesh, convolves
+// with two complex kernel spectra and runs two complex inverses. Here:
+//   1. forward rows: two real density rows form one complex line
+//      (z = row_a + i row_b); one complex FFT gives both rows' half spectra.
+//   2. columns: for each half-spectrum column kx in [0, MW/2]: forward FFT
+//      along y, multiply by the Green's function with its gradient and the CIC
+//      deconvolution folded in (one table, (gx, gy) per bin), inverse FFT of
+//      Fx and of Fy along y.
+//   3. inverse rows: fx and fy are real, so one complex inverse of
+//      Z = Fx + i Fy per row gives fx in the real and fy in the imaginary part.
+// This moves 3 complex line-FFTs per mesh row/column pair instead of 6.
+//
+// The Green's table. The force kernels Kx, Ky of kernel_init.comp are real
+// and odd (the Nyquist component is zeroed for that, kernel_init.comp:37-40),
+// so their spectra are purely imaginary: K^x = i*ax, K^y = i*ay. The table
+// holds g = (ax, ay) * deconvolution / (MW*MH) for unit total mass, computed
+// in FP64 on the device (one packed complex FFT of Kx + i*Ky) and rounded
+// once to FP32; the step multiplies by 1/M_tot. The spectral multiply is then
+//   F = rho^ * i*g = (-rho^.y * g, rho^.x * g).
+//
+// Each line FFT is a Stockham autosort transform in shared memory, radix 8
+// with a final radix-4 or -2 pass, twiddles from one FP32 table of 4096 roots
+// e^{-2 pi i m / 4096} (computed in FP64 on the host).
+
+#include "p3m_internal.cuh"
+
+#include <cmath>
+
+namespace p3m {
+namespace {
+
+__device__ __forceinline__ float2 cmulf(float2 a, float2 b) {
+    return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+__device__ __forceinline__ float2 caddf(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ float2 csubf(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
+// multiply by -i (forward) or +i (inverse)
+__device__ __forceinline__ float2 rot(float2 a, bool inverse) {
+    return inverse ? make_float2(-a.y, a.x) : make_float2(a.y, -a.x);
+}
+
+template <int R>
+__device__ __forceinline__ void dft(float2 (&v)[R], bool inverse);
+
+template <>
+__device__ __forceinline__ void dft<2>(float2 (&v)[2], bool) {
+    const float2 a = v[0], b = v[1];
+    v[0] = caddf(a, b);
+    v[1] = csubf(a, b);
+}
+
+template <>
+__device__ __forceinline__ void dft<4>(float2 (&v)[4], bool inverse) {
+    const float2 s02 = caddf(v[0], v[2]), d02 = csubf(v[0], v[2]);
+    const float2 s13 = caddf(v[1], v[3]), d13 = rot(csubf(v[1], v[3]), inverse);
+    v[0] = caddf(s02, s13);
+    v[2] = csubf(s02, s13);
+    v[1] = caddf(d02, d13);
+    v[3] = csubf(d02, d13);
+}
+
+template <>
+__device__ __forceinline__ void dft<8>(float2 (&v)[8], bool inverse) {
+    float2 e[4] = {v[0], v[2], v[4], v[6]};
+    float2 o[4] = {v[1], v[3], v[5], v[7]};
+    dft<4>(e, inverse);
+    dft<4>(o, inverse);
+    const float h = 0.70710678118654752440f;
+    // o[k] *= e^{-+2 pi i k / 8}
+    o[1] = inverse ? make_float2(h * (o[1].x - o[1].y), h * (o[1].x + o[1].y))
+                   : make_float2(h * (o[1].x + o[1].y), h * (o[1].y - o[1].x));
+    o[2] = rot(o[2], inverse);
+    o[3] = inverse ? make_float2(-h * (o[3].x + o[3].y), h * (o[3].x - o[3].y))
+                   : make_float2(h * (o[3].y - o[3].x), -h * (o[3].x + o[3].y));
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        v[k] = caddf(e[k], o[k]);
+        v[k + 4] = csubf(e[k], o[k]);
+    }
+}
+
+// One Stockham pass of radix R over `lines` lines of length L (line pitch
+// `pitch`), src -> dst. Ns = product of earlier radices; log2(Ns*R) <= 12.
+template <int R>
+__device__ __forceinline__ void stockham_pass(const float2* __restrict__ src, float2* __restrict__ dst,
+                                              int L, int lines, int pitch, int Ns, int log_ns_r,
+                                              bool inverse, const float2* __restrict__ tw) {
+    const int per_line = L / R;
+    const int total = lines * per_line;
+    const int shift = kTwiddleLog2 - log_ns_r;
+    for (int t = threadIdx.x; t < total; t += blockDim.x) {
+        const int line = t / per_line;
+        const int j = t - line * per_line;
+        const float2* s = src + line * pitch;
+        float2* d = dst + line * pitch;
+        const int k = j & (Ns - 1);
+        float2 v[R];
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+            float2 x = s[j + r * per_line];
+            if (r > 0 && k > 0) {
+                float2 w = __ldg(&tw[(k * r) << shift]);
+                if (inverse) w.y = -w.y;
+                x = cmulf(x, w);
+            }
+            v[r] = x;
+        }
+        dft<R>(v, inverse);
+        const int out = (j - k) * R + k;
+#pragma unroll
+        for (int r = 0; r < R; ++r) d[out + r * Ns] = v[r];
+    }
+}
+
+// Complex FFT of `lines` lines held in buffer a (ping-pong buffer b); returns
+// the buffer that holds the result. Ends with __syncthreads().
+__device__ float2* line_fft(float2* a, float2* b, int L, int log2L, int lines, int pitch,
+                            bool inverse, const float2* __restrict__ tw) {
+    int Ns = 1, logNs = 0;
+    while (Ns < L) {
+        const int remaining = log2L - logNs;
+        if (remaining >= 3) {
+            stockham_pass<8>(a, b, L, lines, pitch, Ns, logNs + 3, inverse, tw);
+            Ns <<= 3; logNs += 3;
+        } else if (remaining == 2) {
+            stockham_pass<4>(a, b, L, lines, pitch, Ns, logNs + 2, inverse, tw);
+            Ns <<= 2; logNs += 2;
+        } else {
+            stockham_pass<2>(a, b, L, lines, pitch, Ns, logNs + 1, inverse, tw);
+            Ns <<= 1; logNs += 1;
+        }
+        __syncthreads();
+        float2* t = a; a = b; b = t;
+    }
+    return a;
+}
+
+__device__ __forceinline__ int ilog2(int v) { return 31 - __clz(v); }
+
+// ---------------------------------------------------------------- kernels
+// 1. forward rows: fft_init.comp (fixed point -> float) fused with the row
+// transform. Two rows per complex line.
+template <typename T>
+__global__ void __launch_bounds__(256) fft_rows_forward_kernel(const T* __restrict__ density,
+                                                               float inv_scale, int MW, int MH,
+                                                               int pairs_per_cta,
+                                                               const float2* __restrict__ tw,
+                                                               float2* __restrict__ half) {
+    extern __shared__ __align__(16) float2 sm[];
+    const int pair0 = blockIdx.x * pairs_per_cta;
+    const int pairs = min(pairs_per_cta, MH / 2 - pair0);
+    float2* a = sm;
+    float2* b = sm + pairs_per_cta * MW;
+    for (int t = threadIdx.x; t < pairs * MW; t += blockDim.x) {
+        const int p = t / MW, x = t - p * MW;
+        const size_t row = (size_t)(pair0 + p) * 2;
+        const float re = (float)density[row * MW + x] * inv_scale;
+        const float im = (float)density[(row + 1) * MW + x] * inv_scale;
+        a[p * MW + x] = make_float2(re, im);
+    }
+    __syncthreads();
+    float2* z = line_fft(a, b, MW, ilog2(MW), pairs, MW, false, tw);
+    const int SW = MW / 2 + 1;
+    for (int t = threadIdx.x; t < pairs * SW; t += blockDim.x) {
+        const int p = t / SW, kx = t - p * SW;
+        const float2 zk = z[p * MW + kx];
+        const float2 zn = z[p * MW + ((MW - kx) & (MW - 1))];
+        const float2 A = make_float2(0.5f * (zk.x + zn.x), 0.5f * (zk.y - zn.y));
+        const float2 B = make_float2(0.5f * (zk.y + zn.y), 0.5f * (zn.x - zk.x));
+        const size_t row = (size_t)(pair0 + p) * 2;
+        half[row * SW + kx] = A;
+        half[(row + 1) * SW + kx] = B;
+    }
+}
+
+// 2. columns: forward along y, Green's multiply (convolve.comp), inverse of Fx
+// and Fy along y. Shared memory: [A: G lines | B: G lines | C: 2G lines].
+__global__ void __launch_bounds__(256) fft_columns_kernel(const float2* __restrict__ half,
+                                                          const float2* __restrict__ green,
+                                                          float inv_total, int MW, int MH, int G,
+                                                          const float2* __restrict__ tw,
+                                                          float4* __restrict__ cols) {
+    extern __shared__ __align__(16) float2 sm[];
+    const int SW = MW / 2 + 1;
+    const int kx0 = blockIdx.x * G;
+    const int ncols = min(G, SW - kx0);
+    const int logH = ilog2(MH);
+    float2* A = sm;
+    float2* B = sm + G * MH;
+    float2* C = sm + 2 * G * MH;
+    for (int t = threadIdx.x; t < ncols * MH; t += blockDim.x) {
+        const int y = t / ncols, c = t - y * ncols;
+        A[c * MH + y] = half[(size_t)y * SW + kx0 + c];
+    }
+    __syncthreads();
+    const float2* R = line_fft(A, B, MH, logH, ncols, MH, false, tw);
+    for (int t = threadIdx.x; t < ncols * MH; t += blockDim.x) {
+        const int y = t / ncols, c = t - y * ncols;
+        const float2 rho = R[c * MH + y];
+        const float2 g = __ldg(&green[(size_t)y * SW + kx0 + c]);
+        const float gx = g.x * inv_total, gy = g.y * inv_total;
+        C[c * MH + y] = make_float2(-rho.y * gx, rho.x * gx);
+        C[(ncols + c) * MH + y] = make_float2(-rho.y * gy, rho.x * gy);
+    }
+    __syncthreads();
+    const float2* F = line_fft(C, A, MH, logH, 2 * ncols, MH, true, tw);
+    for (int t = threadIdx.x; t < ncols * MH; t += blockDim.x) {
+        const int y = t / ncols, c = t - y * ncols;
+        const float2 fx = F[c * MH + y], fy = F[(ncols + c) * MH + y];
+        cols[(size_t)y * SW + kx0 + c] = make_float4(fx.x, fx.y, fy.x, fy.y);
+    }
+}
+
+// Forward column transform only (the density spectrum, for diagnostics).
+__global__ void __launch_bounds__(256) fft_columns_forward_kernel(float2* half, int MW, int MH,
+                                                                  int G,
+                                                                  const float2* __restrict__ tw) {
+    extern __shared__ __align__(16) float2 sm[];
+    const int SW = MW / 2 + 1;
+    const int kx0 = blockIdx.x * G;
+    const int ncols = min(G, SW - kx0);
+    float2* A = sm;
+    float2* B = sm + G * MH;
+    for (int t = threadIdx.x; t < ncols * MH; t += blockDim.x) {
+        const int y = t / ncols, c = t - y * ncols;
+        A[c * MH + y] = half[(size_t)y * SW + kx0 + c];
+    }
+    __syncthreads();
+    const float2* R = line_fft(A, B, MH, ilog2(MH), ncols, MH, false, tw);
+    for (int t = threadIdx.x; t < ncols * MH; t += blockDim.x) {
+        const int y = t / ncols, c = t - y * ncols;
+        half[(size_t)y * SW + kx0 + c] = R[c * MH + y];
+    }
+}
+
+// 3. inverse rows: Z = Fx + i Fy over the full row from the two half spectra
+// (each Hermitian in kx), one complex inverse, (fx, fy) = (Re, Im).
+__global__ void __launch_bounds__(256) fft_rows_inverse_kernel(const float4* __restrict__ cols,
+                                                               int MW, int MH, int rows_per_cta,
+                                                               const float2* __restrict__ tw,
+                                                               float2* __restrict__ force) {
+    extern __shared__ __align__(16) float2 sm[];
+    const int row0 = blockIdx.x * rows_per_cta;
+    const int rows = min(rows_per_cta, MH - row0);
+    const int SW = MW / 2 + 1;
+    float2* a = sm;
+    float2* b = sm + rows_per_cta * MW;
+    for (int t = threadIdx.x; t < rows * SW; t += blockDim.x) {
+        const int r = t / SW, kx = t - r * SW;
+        const float4 q = cols[(size_t)(row0 + r) * SW + kx];  // (Fx.re, Fx.im, Fy.re, Fy.im)
+        if (kx == 0 || kx == MW / 2) {
+            // DC and Nyquist bins of a real row are real.
+            a[r * MW + kx] = make_float2(q.x, q.z);
+        } else {
+            a[r * MW + kx] = make_float2(q.x - q.w, q.y + q.z);
+            a[r * MW + (MW - kx)] = make_float2(q.x + q.w, q.z - q.y);
+        }
+    }
+    __syncthreads();
+    const float2* z = line_fft(a, b, MW, ilog2(MW), rows, MW, true, tw);
+    for (int t = threadIdx.x; t < rows * MW; t += blockDim.x) {
+        const int r = t / MW, x = t - r * MW;
+        force[(size_t)(row0 + r) * MW + x] = z[r * MW + x];
+    }
+}
+
+// ------------------------------------------------------- FP64 Green's table
+// kernel_init.comp:16-46 in FP64 with unit total mass, packed as Kx + i Ky.
+__global__ void green_real_kernel(double2* z, int MW, int MH, int W, int H, double aspect,
+                                  double gravity, double sigma_cells) {
+    const long long id = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (id >= (long long)MW * MH) return;
+    const int raw_x = (int)(id % MW), raw_y = (int)(id / MW);
+    const int off_x = raw_x <= MW / 2 ? raw_x : raw_x - MW;
+    const int off_y = raw_y <= MH / 2 ? raw_y : raw_y - MH;
+    const double dx = (double)off_x * aspect / (double)W;
+    const double dy = (double)off_y / (double)H;
+    const double r2 = dx * dx + dy * dy;
+    if (r2 == 0.0) {
+        z[id] = make_double2(0.0, 0.0);
+        return;
+    }
+    const double sigma = sigma_cells / (double)H;
+    const double long_w = 1.0 - exp(-r2 / (2.0 * sigma * sigma));
+    const double dir_x = raw_x * 2 == MW ? 0.0 : dx;
+    const double dir_y = raw_y * 2 == MH ? 0.0 : dy;
+    const double scale = -gravity * long_w / r2;
+    z[id] = make_double2(scale * dir_x / aspect, scale * dir_y);
+}
+
+// FP64 radix-2 in-place FFT of one line per CTA (the layout of
+// fft_shared.comp, exact twiddles from sincospi). axis 0 = rows, 1 = columns.
+__global__ void fft64_line_kernel(double2* z, int MW, int MH, int axis) {
+    extern __shared__ __align__(16) double2 ld[];
+    const int L = axis == 0 ? MW : MH;
+    const int bits = ilog2(L);
+    const int line = blockIdx.x;
+    auto gidx = [&](int c) -> size_t {
+        return axis == 0 ? (size_t)line * MW + c : (size_t)c * MW + line;
+    };
+    for (int c = threadIdx.x; c < L; c += blockDim.x) {
+        const int src = bits ? (int)(__brev((unsigned)c) >> (32 - bits)) : 0;
+        ld[c] = z[gidx(src)];
+    }
+    __syncthreads();
+    for (int stage = 2; stage <= L; stage <<= 1) {
+        const int h = stage >> 1;
+        for (int bf = threadIdx.x; bf < L / 2; bf += blockDim.x) {
+            const int within = bf & (h - 1);
+            const int lower = (bf / h) * stage + within;
+            double s, c;
+            sincospi(-2.0 * (double)within / (double)stage, &s, &c);
+            const double2 lo = ld[lower], up = ld[lower + h];
+            const double2 u = make_double2(c * up.x - s * up.y, c * up.y + s * up.x);
+            ld[lower] = make_double2(lo.x + u.x, lo.y + u.y);
+            ld[lower + h] = make_double2(lo.x - u.x, lo.y - u.y);
+        }
+        __syncthreads();
+    }
+    for (int c = threadIdx.x; c < L; c += blockDim.x) z[gidx(c)] = ld[c];
+}
+
+// Z = K^x + i K^y = i ax - ay, so ax = Im Z, ay = -Re Z. Deconvolution of
+// convolve.comp:30-42 in FP64.
+__global__ void green_final_kernel(const double2* z, int MW, int MH, double window_floor,
+                                   float2* green) {
+    const int SW = MW / 2 + 1;
+    const long long id = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (id >= (long long)SW * MH) return;
+    const int kx = (int)(id % SW), ky = (int)(id / SW);
+    const int ikx = kx;  // kx <= MW/2
+    const int iky = ky <= MH / 2 ? ky : ky - MH;
+    auto sinc = [](double v) { return fabs(v) < 1e-12 ? 1.0 : sin(v) / v; };
+    const double sx = sinc(M_PI * (double)ikx / (double)MW);
+    const double sy = sinc(M_PI * (double)iky / (double)MH);
+    const double window = sx * sx * sy * sy;
+    const double deconv = 1.0 / fmax(window * window, window_floor);
+    const double scale = deconv / ((double)MW * (double)MH);
+    const double2 v = z[(size_t)ky * MW + kx];
+    green[id] = make_float2((float)(v.y * scale), (float)(-v.x * scale));
+}
+
+inline int ilog2_host(int v) {
+    int b = 0;
+    while ((1 << (b + 1)) <= v) ++b;
+    return b;
+}
+
+cudaError_t set_smem(const void* fn, size_t bytes) {
+    return cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+}
+
+// Columns per CTA of the column kernels: enough CTAs to fill the GPU, at most
+// 16 and at most what 128 KB of shared memory holds.
+int column_group(int MW, int MH, int lines_factor) {
+    const int SW = MW / 2 + 1;
+    int g = SW / 296;
+    const int cap = (128 * 1024) / (lines_factor * MH * (int)sizeof(float2));
+    if (g > cap) g = cap;
+    if (g > 16) g = 16;
+    if (g < 1) g = 1;
+    return g;
+}
+
+}  // namespace
+
+void host_twiddles(float2* out) {
+    for (int m = 0; m < kTwiddleLength; ++m) {
+        const double a = -2.0 * M_PI * (double)m / (double)kTwiddleLength;
+        out[m] = make_float2((float)std::cos(a), (float)std::sin(a));
+    }
+}
+
+cudaError_t launch_fft_forward_rows(const void* density, int deposit_mode, float inv_scale,
+                                    GridShape g, const float2* twiddles, float2* half,
+                                    cudaStream_t stream) {
+    const int pairs_per_cta = g.MW >= 4096 ? 1 : 4096 / g.MW;
+    const int pairs = g.MH / 2;
+    const int blocks = (pairs + pairs_per_cta - 1) / pairs_per_cta;
+    const size_t smem = (size_t)2 * pairs_per_cta * g.MW * sizeof(float2);
+    cudaError_t e;
+    if (deposit_mode == P3M_DEPOSIT_I64) {
+        e = set_smem((const void*)fft_rows_forward_kernel<long long>, smem);
+        if (e != cudaSuccess) return e;
+        fft_rows_forward_kernel<long long><<<blocks, 256, smem, stream>>>(
+            static_cast<const long long*>(density), inv_scale, g.MW, g.MH, pairs_per_cta, twiddles,
+            half);
+    } else {
+        e = set_smem((const void*)fft_rows_forward_kernel<uint32_t>, smem);
+        if (e != cudaSuccess) return e;
+        fft_rows_forward_kernel<uint32_t><<<blocks, 256, smem, stream>>>(
+            static_cast<const uint32_t*>(density), inv_scale, g.MW, g.MH, pairs_per_cta, twiddles,
+            half);
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_fft_columns(const float2* half, const float2* green, float inv_total,
+                               GridShape g, const float2* twiddles, float4* cols,
+                               cudaStream_t stream) {
+    const int G = column_group(g.MW, g.MH, 4);
+    const int SW = g.MW / 2 + 1;
+    const int blocks = (SW + G - 1) / G;
+    const size_t smem = (size_t)4 * G * g.MH * sizeof(float2);
+    cudaError_t e = set_smem((const void*)fft_columns_kernel, smem);
+    if (e != cudaSuccess) return e;
+    fft_columns_kernel<<<blocks, 256, smem, stream>>>(half, green, inv_total, g.MW, g.MH, G,
+                                                      twiddles, cols);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_fft_forward_columns(float2* half, GridShape g, const float2* twiddles,
+                                       cudaStream_t stream) {
+    const int G = column_group(g.MW, g.MH, 2);
+    const int SW = g.MW / 2 + 1;
+    const int blocks = (SW + G - 1) / G;
+    const size_t smem = (size_t)2 * G * g.MH * sizeof(float2);
+    cudaError_t e = set_smem((const void*)fft_columns_forward_kernel, smem);
+    if (e != cudaSuccess) return e;
+    fft_columns_forward_kernel<<<blocks, 256, smem, stream>>>(half, g.MW, g.MH, G, twiddles);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_fft_inverse_rows(const float4* cols, GridShape g, const float2* twiddles,
+                                    float2* force, cudaStream_t stream) {
+    const int rows_per_cta = g.MW >= 4096 ? 1 : 4096 / g.MW;
+    const int blocks = (g.MH + rows_per_cta - 1) / rows_per_cta;
+    const size_t smem = (size_t)2 * rows_per_cta * g.MW * sizeof(float2);
+    cudaError_t e = set_smem((const void*)fft_rows_inverse_kernel, smem);
+    if (e != cudaSuccess) return e;
+    fft_rows_inverse_kernel<<<blocks, 256, smem, stream>>>(cols, g.MW, g.MH, rows_per_cta,
+                                                           twiddles, force);
+    return cudaGetLastError();
+}
+
+cudaError_t build_green(GridShape g, GreenParams p, double2* work, float2* green,
+                        cudaStream_t stream) {
+    const long long M = (long long)g.MW * g.MH;
+    green_real_kernel<<<(int)((M + 255) / 256), 256, 0, stream>>>(
+        work, g.MW, g.MH, g.W, g.H, (double)p.aspect, (double)p.gravity, (double)p.sigma_cells);
+    cudaError_t e = set_smem((const void*)fft64_line_kernel,
+                             (size_t)std::max(g.MW, g.MH) * sizeof(double2));
+    if (e != cudaSuccess) return e;
+    fft64_line_kernel<<<g.MH, 256, (size_t)g.MW * sizeof(double2), stream>>>(work, g.MW, g.MH, 0);
+    fft64_line_kernel<<<g.MW, 256, (size_t)g.MH * sizeof(double2), stream>>>(work, g.MW, g.MH, 1);
+    const long long SWH = (long long)(g.MW / 2 + 1) * g.MH;
+    green_final_kernel<<<(int)((SWH + 255) / 256), 256, 0, stream>>>(
+        work, g.MW, g.MH, (double)p.window_floor, green);
+    (void)ilog2_host;
+    return cudaGetLastError();
+}
+
+}  // namespace p3m

@@ -1,0 +1,209 @@
+// p3m_internal.cuh — shared declarations of the sm_100a P3M library.
+//
+// Layout in HBM (one context):
+//   bodies      float4[cap]  (x, y, vx, vy) in unit coordinates, ID order
+//   materials   float4[cap]  (mass, friction, solid, block)
+//   accel       float2[cap]
+//   keys/ids    uint32[cap] x2 ping-pong   cell-key radix sort
+//   entries     float4[cap]  bodies gathered into cell order (x, y, mass, id bits)
+//   cell_start / cell_count / cell_mass    int32/int32/uint32 [P]
+//   density     uint32[M] or int64[M]      fixed-point CIC mesh
+//   half        float2[(MW/2+1) * MH]      row-transformed density
+//   cols        float4[(MW/2+1) * MH]      column-inverted (Fx, Fy) spectra
+//   force       float2[M]                  (fx, fy) long-range mesh force
+//   green       float2[(MW/2+1) * MH]      spectral multipliers (gx, gy)
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cstdint>
+#include <string>
+
+#include "../../include/p3m.h"
+
+namespace p3m {
+
+constexpr float kCellMassUnits = 256.0f;        // build_grid.comp:19
+constexpr float kMaximumUnit = 0.99999994f;      // collision_build.comp:21
+constexpr int kMaxMeshAxis = 4096;
+constexpr int kTwiddleLog2 = 12;                 // one table of 4096 roots
+constexpr int kTwiddleLength = 1 << kTwiddleLog2;
+
+// ------------------------------------------------------------- index helpers
+// floor(x) converted to int the way the GPU's cvt.rzi.s32.f32 converts:
+// NaN -> 0, saturation at the int range (the value is already integral).
+__host__ __device__ __forceinline__ int float_to_int(float f) {
+    if (f != f) return 0;
+    if (f >= 2147483647.0f) return 2147483647;
+    if (f <= -2147483648.0f) return (int)0x80000000;
+    return (int)f;
+}
+
+// wrapCell / wrapMesh (build_grid.comp:21-37, kick.comp:38-59): one period
+// added or subtracted. Every index a position in [0, 1] produces needs no
+// more; a position outside that range, handed in by a caller, is reduced
+// modulo the size so that no index ever leaves its buffer.
+__host__ __device__ __forceinline__ int wrap_index(int v, int size) {
+    if (v < 0) v += size;
+    else if (v >= size) v -= size;
+    if ((unsigned)v >= (unsigned)size) {
+        v %= size;
+        if (v < 0) v += size;
+    }
+    return v;
+}
+
+// A cell coordinate that stencil offsets (|d| <= size) are added to: kept as
+// it is for positions in [0, 1], folded into [0, size) only when it lies so
+// far out that adding an offset could overflow.
+__host__ __device__ __forceinline__ int guard_coord(int v, int size) {
+    return (v < -size || v > 2 * size) ? wrap_index(v, size) : v;
+}
+
+// ---------------------------------------------------------------- radix sort
+constexpr int kSortThreads = 256;
+constexpr int kSortItems = 16;
+constexpr int kSortTile = kSortThreads * kSortItems;  // 4096 keys per tile
+constexpr int kSortMaxRadix = 256;
+
+struct SortScratch {
+    uint32_t* keys_alt = nullptr;
+    uint32_t* vals_alt = nullptr;
+    uint32_t* hist = nullptr;       // kSortMaxRadix * tiles
+    uint32_t* block_sums = nullptr; // scan partials
+    int capacity = 0;
+};
+
+size_t sort_hist_entries(int capacity);
+size_t sort_block_sum_entries(int capacity);
+
+// Stable LSD radix sort of (keys, vals) on bits [0, key_bits). Passes
+// alternate between the inputs and the scratch pair; *out_keys/*out_vals
+// name the pair that holds the result. Launches only; no allocation, no
+// synchronisation.
+cudaError_t radix_sort_pairs(uint32_t* keys, uint32_t* vals, const SortScratch& s, int n,
+                             int key_bits, cudaStream_t stream, uint32_t** out_keys,
+                             uint32_t** out_vals);
+
+// Exclusive scan of n uint32 in place (n <= 4096 * 4096).
+cudaError_t exclusive_scan_u32(uint32_t* data, int n, uint32_t* block_sums,
+                               cudaStream_t stream);
+
+// ------------------------------------------------------------- step kernels
+struct GridShape {
+    int W, H;     // physical grid
+    int MW, MH;   // mesh (= physical on the torus, 2x on walls)
+    int bounded;
+};
+
+// Half kick + drift substeps (collision_build.comp:40-51), then the home-cell
+// key of each body, written in descending ID order for the cell sort.
+cudaError_t launch_drift(float4* bodies, const float2* accel, int n, float half_kick,
+                         float drift_dt, int substeps, GridShape g, uint32_t* keys,
+                         uint32_t* vals, unsigned int* nonfinite, cudaStream_t stream);
+// Home-cell keys of the current positions (no drift).
+cudaError_t launch_cell_keys(const float4* bodies, int n, GridShape g, uint32_t* keys,
+                             uint32_t* vals, cudaStream_t stream);
+// Morton tile keys (spatial_sort_key.glsl), ascending ID order.
+cudaError_t launch_morton_keys(const float4* bodies, int n, int wbits, int hbits,
+                               uint32_t* keys, uint32_t* vals, cudaStream_t stream);
+// Permutation of the Morton reorder (spatial_sort_scatter / _materials.comp).
+cudaError_t launch_permute(const uint32_t* order, int n, const float4* bodies, const float2* accel,
+                           const float4* materials, float4* bodies_out, float2* accel_out,
+                           float4* materials_out, uint32_t* destinations, cudaStream_t stream);
+// Cell lists from sorted keys: start, count, mass; gathers entries.
+cudaError_t launch_cell_build(const uint32_t* keys, const uint32_t* ids, int n,
+                              const float4* bodies, const float4* materials, int* cell_start,
+                              int* cell_count, uint32_t* cell_mass, float4* entries,
+                              cudaStream_t stream);
+
+// Tile-reduced CIC deposit (build_grid.comp:53-69) over cell-ordered entries.
+cudaError_t launch_deposit(const float4* entries, const uint32_t* keys, int n, GridShape g,
+                           int deposit_mode, float mass_scale, void* density,
+                           cudaStream_t stream);
+
+// Real 2D FFT, spectral multiply and inverse (fft_shared.comp, convolve.comp).
+cudaError_t launch_fft_forward_rows(const void* density, int deposit_mode, float inv_scale,
+                                    GridShape g, const float2* twiddles, float2* half,
+                                    cudaStream_t stream);
+cudaError_t launch_fft_columns(const float2* half, const float2* green, float inv_total,
+                               GridShape g, const float2* twiddles, float4* cols,
+                               cudaStream_t stream);
+cudaError_t launch_fft_inverse_rows(const float4* cols, GridShape g, const float2* twiddles,
+                                    float2* force, cudaStream_t stream);
+// Forward spectrum only (diagnostic): half-spectrum columns transformed.
+cudaError_t launch_fft_forward_columns(float2* half, GridShape g, const float2* twiddles,
+                                       cudaStream_t stream);
+
+// FP64 Green's function precompute (kernel_init.comp + 2 forward FFTs +
+// convolve.comp's deconvolution), unit total mass.
+struct GreenParams {
+    float aspect, gravity, sigma_cells, window_floor;
+};
+cudaError_t build_green(GridShape g, GreenParams p, double2* work, float2* green,
+                        cudaStream_t stream);
+
+// Interpolation + short range + half kick (kick.comp:66-156).
+struct KickParams {
+    int n, W, H, MW, MH, bounded, rx, ry, exact, home_limit, initial, mutual;
+    float aspect, gravity, sigma_cells, total_mass, min_frac, dt, field_x, field_y;
+};
+cudaError_t launch_kick(float4* bodies, float2* accel, const float2* force, const int* cell_start,
+                        const int* cell_count, const uint32_t* cell_mass, const float4* entries,
+                        KickParams p, cudaStream_t stream);
+
+// Host-side twiddle table: e^{-2 pi i m / 4096}, computed in double.
+void host_twiddles(float2* out);
+
+}  // namespace p3m
+
+// ------------------------------------------------------------------ context
+struct p3m_ctx {
+    p3m_config cfg{};
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    p3m::GridShape grid{};
+    bool walls_supported = false;
+    float aspect = 1.0f;
+    int rx = 1, ry = 1;
+    int sort_wbits = 0, sort_hbits = 0;
+    int bounded = 0;
+    int mutual = 1;
+    float field_x = 0.0f, field_y = 0.0f;  // unit/s^2
+    float mass_excess = 0.0f;
+    float normalization_mass = -1.0f;
+    int mass_scale = 1;
+    long long physics_steps = 0;
+    int green_bounded = -1;  // which mesh the Green's table was built for
+
+    // body state
+    float4* bodies = nullptr;
+    float4* bodies_alt = nullptr;
+    float2* accel = nullptr;
+    float2* accel_alt = nullptr;
+    float4* materials = nullptr;
+    float4* materials_alt = nullptr;
+    uint32_t* destinations = nullptr;
+    unsigned int* status = nullptr;  // [0] non-finite bodies seen by the drift
+
+    // cell lists
+    uint32_t* keys = nullptr;
+    uint32_t* vals = nullptr;
+    p3m::SortScratch sort;
+    uint32_t* sorted_keys = nullptr;  // where the last sort left its result
+    uint32_t* sorted_ids = nullptr;
+    int* cell_start = nullptr;
+    int* cell_count = nullptr;
+    uint32_t* cell_mass = nullptr;
+    float4* entries = nullptr;
+
+    // mesh
+    void* density = nullptr;
+    float2* half = nullptr;
+    float4* cols = nullptr;
+    float2* force = nullptr;
+    float2* green = nullptr;
+    float2* twiddles = nullptr;
+    size_t mesh_capacity = 0;  // cells the mesh buffers hold
+
+    std::string last_error;
+};

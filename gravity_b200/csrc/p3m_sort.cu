@@ -1,0 +1,434 @@
+// p3m_sort.cu — cell keys, 64-bit-key radix sort, cell lists, Morton reorder.
+//
+// Replaces the home-cell linked lists of build_grid.comp:71-75 and the
+// spatial reorder of spatial_sort_{count,scan,scatter,materials}.comp
+// (GravityPipeline.kt:1269-1319).
+//
+// The cell lists. build_grid.comp pushes every body onto its home cell's list
+// with atomicExchange, so each list's order depends on thread timing; kick.comp
+// walks only the first few entries of a list (kick.comp:137-148), so that order
+// changes forces. Here the order is fixed: a list runs in DESCENDING body ID,
+// the order a single thread pushing IDs 0..n-1 would leave. It is produced by
+// sorting the 64-bit key (cell << 32) | ~id ascending. The sort input is
+// written in descending ID order, i.e. already sorted on the low 32 bits, and
+// an LSD radix sort is stable, so the passes over the low 32 bits would be
+// identity permutations and are skipped: only the ceil(log2 P) cell bits are
+// sorted. The result is identical to sorting the full 64-bit key.
+//
+// The Morton reorder sorts the 32-bit tile key the same way, with ties in
+// ascending ID (the reference's scatter rank is an atomic and its order inside
+// a tile is nondeterministic, spatial_sort_scatter.comp:21).
+
+#include "p3m_internal.cuh"
+
+namespace p3m {
+namespace {
+
+constexpr unsigned kFull = 0xffffffffu;
+
+__device__ __forceinline__ unsigned lanemask_lt() {
+    unsigned m;
+    asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+    return m;
+}
+
+// Inclusive warp scan.
+__device__ __forceinline__ uint32_t warp_inclusive_scan(uint32_t v, int lane) {
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        uint32_t u = __shfl_up_sync(kFull, v, o);
+        if (lane >= o) v += u;
+    }
+    return v;
+}
+
+// Block-wide exclusive scan of one value per thread (blockDim multiple of 32,
+// at most 1024). `warp_tot` needs blockDim/32 entries. Returns the block total.
+__device__ uint32_t block_exclusive_scan(uint32_t v, uint32_t* warp_tot, uint32_t* out) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, warps = blockDim.x >> 5;
+    uint32_t inc = warp_inclusive_scan(v, lane);
+    if (lane == 31) warp_tot[warp] = inc;
+    __syncthreads();
+    if (warp == 0) {
+        uint32_t t = lane < warps ? warp_tot[lane] : 0u;
+        uint32_t ti = warp_inclusive_scan(t, lane);
+        if (lane < warps) warp_tot[lane] = ti - t;
+        if (lane == warps - 1) warp_tot[32] = ti;
+    }
+    __syncthreads();
+    *out = inc - v + warp_tot[warp];
+    uint32_t total = warp_tot[32];
+    __syncthreads();
+    return total;
+}
+
+// ----------------------------------------------------------------- scan
+constexpr int kScanThreads = 1024;
+constexpr int kScanItems = 4;
+constexpr int kScanBlock = kScanThreads * kScanItems;
+
+__global__ void __launch_bounds__(kScanThreads) scan_local_kernel(uint32_t* data, int n,
+                                                                  uint32_t* sums) {
+    __shared__ uint32_t warp_tot[33];
+    const int base = blockIdx.x * kScanBlock + threadIdx.x * kScanItems;
+    uint32_t v[kScanItems];
+    uint32_t s = 0;
+#pragma unroll
+    for (int i = 0; i < kScanItems; ++i) {
+        v[i] = base + i < n ? data[base + i] : 0u;
+        s += v[i];
+    }
+    uint32_t pre;
+    uint32_t total = block_exclusive_scan(s, warp_tot, &pre);
+#pragma unroll
+    for (int i = 0; i < kScanItems; ++i) {
+        if (base + i < n) data[base + i] = pre;
+        pre += v[i];
+    }
+    if (threadIdx.x == 0 && sums) sums[blockIdx.x] = total;
+}
+
+__global__ void __launch_bounds__(kScanThreads) scan_add_kernel(uint32_t* data, int n,
+                                                                const uint32_t* sums) {
+    const uint32_t add = sums[blockIdx.x];
+    const int base = blockIdx.x * kScanBlock + threadIdx.x * kScanItems;
+#pragma unroll
+    for (int i = 0; i < kScanItems; ++i)
+        if (base + i < n) data[base + i] += add;
+}
+
+// ------------------------------------------------------------ radix sort
+constexpr int kSortWarps = kSortThreads / 32;
+
+// Per-tile digit histogram, written digit-major (hist[d * tiles + tile]) so
+// that one exclusive scan of the whole array yields every tile's output base
+// for every digit.
+__global__ void __launch_bounds__(kSortThreads) radix_hist_kernel(const uint32_t* __restrict__ keys,
+                                                                  int n, int shift, int bits,
+                                                                  int tiles, uint32_t* hist) {
+    __shared__ uint32_t h[kSortMaxRadix];
+    const int radix = 1 << bits;
+    const uint32_t mask = (uint32_t)radix - 1u;
+    for (int i = threadIdx.x; i < radix; i += blockDim.x) h[i] = 0;
+    __syncthreads();
+    const int tile = blockIdx.x;
+    const int base = tile * kSortTile;
+    const int lane = threadIdx.x & 31;
+    // Vectorised: each thread reads kSortItems/4 uint4 (the tile base is a
+    // multiple of 4096 keys, so every uint4 is 16-byte aligned).
+#pragma unroll
+    for (int j = 0; j < kSortItems / 4; ++j) {
+        const int idx = base + (j * kSortThreads + threadIdx.x) * 4;
+        uint32_t k[4];
+        if (idx + 3 < n) {
+            uint4 q = __ldg(reinterpret_cast<const uint4*>(keys + idx));
+            k[0] = q.x; k[1] = q.y; k[2] = q.z; k[3] = q.w;
+        } else {
+#pragma unroll
+            for (int e = 0; e < 4; ++e) k[e] = idx + e < n ? keys[idx + e] : 0xffffffffu;
+        }
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+            const bool valid = idx + e < n;
+            const uint32_t d = valid ? (k[e] >> shift) & mask : 0xffffffffu;
+            // Aggregate equal digits across the warp before the shared atomic.
+            const unsigned peers = __match_any_sync(kFull, d);
+            if (valid && lane == __ffs(peers) - 1) atomicAdd(&h[d], (uint32_t)__popc(peers));
+        }
+    }
+    __syncthreads();
+    (void)lane;
+    for (int d = threadIdx.x; d < radix; d += blockDim.x) hist[(size_t)d * tiles + tile] = h[d];
+}
+
+// Stable scatter of one tile. Keys of warp w are the contiguous sub-tile
+// [w*32*items, (w+1)*32*items), visited item-major so that (item, lane)
+// increases with the input position. Each key's rank among equal digits comes
+// from __match_any_sync + popc of lower lanes, plus a per-warp running count.
+__global__ void __launch_bounds__(kSortThreads) radix_scatter_kernel(
+    const uint32_t* __restrict__ keys_in, const uint32_t* __restrict__ vals_in,
+    uint32_t* __restrict__ keys_out, uint32_t* __restrict__ vals_out, int n, int shift, int bits,
+    int tiles, const uint32_t* __restrict__ hist_scanned) {
+    __shared__ uint32_t warp_hist[kSortWarps][kSortMaxRadix];
+    __shared__ uint32_t tile_start[kSortMaxRadix];
+    __shared__ uint32_t out_base[kSortMaxRadix];
+    __shared__ uint32_t warp_tot[33];
+    __shared__ uint32_t s_keys[kSortTile];
+    __shared__ uint32_t s_vals[kSortTile];
+
+    const int radix = 1 << bits;
+    const uint32_t mask = (uint32_t)radix - 1u;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int tile = blockIdx.x;
+    const int tile_base = tile * kSortTile;
+    const int sub_base = tile_base + warp * 32 * kSortItems;
+
+    for (int i = threadIdx.x; i < kSortWarps * kSortMaxRadix; i += blockDim.x)
+        (&warp_hist[0][0])[i] = 0;
+    __syncthreads();
+
+    uint32_t key[kSortItems], val[kSortItems], rank[kSortItems];
+#pragma unroll
+    for (int j = 0; j < kSortItems; ++j) {
+        const int idx = sub_base + j * 32 + lane;
+        const bool valid = idx < n;
+        key[j] = valid ? keys_in[idx] : 0u;
+        val[j] = valid ? vals_in[idx] : 0u;
+        const uint32_t d = valid ? (key[j] >> shift) & mask : 0xffffffffu;
+        const unsigned peers = __match_any_sync(kFull, d);
+        const uint32_t below = (uint32_t)__popc(peers & lanemask_lt());
+        const uint32_t seen = valid ? warp_hist[warp][d] : 0u;
+        __syncwarp();
+        if (valid && lane == __ffs(peers) - 1) warp_hist[warp][d] = seen + (uint32_t)__popc(peers);
+        __syncwarp();
+        rank[j] = seen + below;
+    }
+    __syncthreads();
+
+    // Per digit: exclusive prefix over warps, and the tile's count.
+    uint32_t count = 0;
+    if (threadIdx.x < radix) {
+        const int d = threadIdx.x;
+#pragma unroll
+        for (int w = 0; w < kSortWarps; ++w) {
+            uint32_t t = warp_hist[w][d];
+            warp_hist[w][d] = count;
+            count += t;
+        }
+        out_base[d] = hist_scanned[(size_t)d * tiles + tile];
+    }
+    uint32_t start;
+    block_exclusive_scan(threadIdx.x < radix ? count : 0u, warp_tot, &start);
+    if (threadIdx.x < radix) tile_start[threadIdx.x] = start;
+    __syncthreads();
+
+#pragma unroll
+    for (int j = 0; j < kSortItems; ++j) {
+        const int idx = sub_base + j * 32 + lane;
+        if (idx < n) {
+            const uint32_t d = (key[j] >> shift) & mask;
+            const uint32_t pos = tile_start[d] + warp_hist[warp][d] + rank[j];
+            s_keys[pos] = key[j];
+            s_vals[pos] = val[j];
+        }
+    }
+    __syncthreads();
+
+    // Write the tile back in digit order: consecutive threads write
+    // consecutive addresses inside each digit's run.
+    const int tile_n = min(kSortTile, n - tile_base);
+    for (int p = threadIdx.x; p < tile_n; p += blockDim.x) {
+        const uint32_t k = s_keys[p];
+        const uint32_t d = (k >> shift) & mask;
+        const uint32_t o = out_base[d] + ((uint32_t)p - tile_start[d]);
+        keys_out[o] = k;
+        vals_out[o] = s_vals[p];
+    }
+}
+
+// ----------------------------------------------------------- key kernels
+// build_grid.comp:71-72: home = ivec2(floor(p * vec2(W, H))), then wrapCell.
+__device__ __forceinline__ uint32_t home_cell(float x, float y, int W, int H) {
+    const int hx = wrap_index(float_to_int(floorf(__fmul_rn(x, (float)W))), W);
+    const int hy = wrap_index(float_to_int(floorf(__fmul_rn(y, (float)H))), H);
+    return (uint32_t)hx + (uint32_t)hy * (uint32_t)W;
+}
+
+__global__ void cell_keys_kernel(const float4* __restrict__ bodies, int n, int W, int H,
+                                 uint32_t* keys, uint32_t* vals) {
+    const int id = blockIdx.x * blockDim.x + threadIdx.x;
+    if (id >= n) return;
+    const float4 b = bodies[id];
+    const int slot = n - 1 - id;  // descending ID order
+    keys[slot] = home_cell(b.x, b.y, W, H);
+    vals[slot] = (uint32_t)id;
+}
+
+// spatial_sort_key.glsl:7-25.
+__device__ __forceinline__ uint32_t spread_bits(uint32_t v) {
+    v &= 0xffffu;
+    v = (v | (v << 8)) & 0x00ff00ffu;
+    v = (v | (v << 4)) & 0x0f0f0f0fu;
+    v = (v | (v << 2)) & 0x33333333u;
+    v = (v | (v << 1)) & 0x55555555u;
+    return v;
+}
+
+__device__ __forceinline__ uint32_t tile_coord(float p, int size) {
+    // floor then clamp; NaN maps to tile 0, +-inf to the clamp limits.
+    const float f = floorf(__fmul_rn(p, (float)size));
+    int t;
+    if (f != f) t = 0;
+    else if (f >= 2147483647.0f) t = 2147483647;
+    else if (f <= -2147483648.0f) t = (int)0x80000000;
+    else t = (int)f;
+    return (uint32_t)min(max(t, 0), size - 1);
+}
+
+__global__ void morton_keys_kernel(const float4* __restrict__ bodies, int n, int wbits, int hbits,
+                                   uint32_t* keys, uint32_t* vals) {
+    const int id = blockIdx.x * blockDim.x + threadIdx.x;
+    if (id >= n) return;
+    const float4 b = bodies[id];
+    const uint32_t tx = tile_coord(b.x, 1 << wbits), ty = tile_coord(b.y, 1 << hbits);
+    const int common = min(wbits, hbits);
+    const uint32_t low = (1u << common) - 1u;
+    const uint32_t morton = spread_bits(tx & low) | (spread_bits(ty & low) << 1);
+    keys[id] = morton | (((tx | ty) >> common) << (2 * common));
+    vals[id] = (uint32_t)id;
+}
+
+// spatial_sort_scatter.comp:14-28 and spatial_sort_materials.comp:9-13: a
+// bit-for-bit permutation; destinations[src] = new ID.
+__global__ void permute_kernel(const uint32_t* __restrict__ order, int n,
+                               const float4* __restrict__ bodies, const float2* __restrict__ accel,
+                               const float4* __restrict__ materials, float4* bodies_out,
+                               float2* accel_out, float4* materials_out, uint32_t* destinations) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    const uint32_t src = order[t];
+    bodies_out[t] = bodies[src];
+    accel_out[t] = accel[src];
+    materials_out[t] = materials[src];
+    destinations[src] = (uint32_t)t;
+}
+
+// Cell lists from the sorted keys. Run starts write cell_start; counts and
+// the fixed-point cell masses (build_grid.comp:74-75) are reduced over each
+// warp's segment of equal keys, then added with one atomic per segment
+// (integer sums, so the result does not depend on the order).
+__global__ void cell_build_kernel(const uint32_t* __restrict__ keys, const uint32_t* __restrict__ ids,
+                                  int n, const float4* __restrict__ bodies,
+                                  const float4* __restrict__ materials, int* cell_start,
+                                  int* cell_count, uint32_t* cell_mass, float4* entries) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int lane = threadIdx.x & 31;
+    const bool valid = i < n;
+    const uint32_t c = valid ? keys[i] : 0xffffffffu;
+    uint32_t prev = __shfl_up_sync(kFull, c, 1);
+    if (lane == 0) prev = (valid && i > 0) ? keys[i - 1] : 0xfffffffeu;
+    uint32_t next = __shfl_down_sync(kFull, c, 1);
+    if (lane == 31) next = (i + 1 < n) ? keys[i + 1] : 0xfffffffeu;
+
+    uint32_t cnt = 0, mq = 0;
+    if (valid) {
+        const uint32_t id = ids[i];
+        const float4 b = bodies[id];
+        const float m = materials[id].x;
+        entries[i] = make_float4(b.x, b.y, m, __uint_as_float(id));
+        cnt = 1;
+        mq = (uint32_t)__float2uint_rn(__fmul_rn(m, kCellMassUnits));
+        if (i == 0 || prev != c) cell_start[c] = i;
+    }
+    // Segmented inclusive sum over equal keys (keys are sorted, so equal keys
+    // are contiguous lanes).
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t oc = __shfl_up_sync(kFull, cnt, o);
+        const uint32_t om = __shfl_up_sync(kFull, mq, o);
+        const uint32_t ok = __shfl_up_sync(kFull, c, o);
+        if (lane >= o && ok == c) {
+            cnt += oc;
+            mq += om;
+        }
+    }
+    const bool tail = valid && (lane == 31 || next != c);
+    if (tail) {
+        atomicAdd(&cell_count[c], (int)cnt);
+        atomicAdd(&cell_mass[c], mq);
+    }
+}
+
+inline int blocks_for(long long n, int threads) { return (int)((n + threads - 1) / threads); }
+
+}  // namespace
+
+size_t sort_hist_entries(int capacity) {
+    const size_t tiles = ((size_t)capacity + kSortTile - 1) / kSortTile;
+    return (size_t)kSortMaxRadix * (tiles > 0 ? tiles : 1);
+}
+
+size_t sort_block_sum_entries(int capacity) {
+    const size_t h = sort_hist_entries(capacity);
+    return (h + kScanBlock - 1) / kScanBlock + 1;
+}
+
+cudaError_t exclusive_scan_u32(uint32_t* data, int n, uint32_t* block_sums, cudaStream_t stream) {
+    if (n <= 0) return cudaSuccess;
+    const int blocks = blocks_for(n, kScanBlock);
+    if (blocks == 1) {
+        scan_local_kernel<<<1, kScanThreads, 0, stream>>>(data, n, nullptr);
+        return cudaGetLastError();
+    }
+    if (blocks > kScanBlock) return cudaErrorInvalidValue;
+    scan_local_kernel<<<blocks, kScanThreads, 0, stream>>>(data, n, block_sums);
+    scan_local_kernel<<<1, kScanThreads, 0, stream>>>(block_sums, blocks, nullptr);
+    scan_add_kernel<<<blocks, kScanThreads, 0, stream>>>(data, n, block_sums);
+    return cudaGetLastError();
+}
+
+cudaError_t radix_sort_pairs(uint32_t* keys, uint32_t* vals, const SortScratch& s, int n,
+                             int key_bits, cudaStream_t stream, uint32_t** out_keys,
+                             uint32_t** out_vals) {
+    *out_keys = keys;
+    *out_vals = vals;
+    if (n <= 1 || key_bits <= 0) return cudaSuccess;
+    if (n > s.capacity) return cudaErrorInvalidValue;
+    const int passes = (key_bits + 7) / 8;
+    const int bits = (key_bits + passes - 1) / passes;
+    const int tiles = blocks_for(n, kSortTile);
+    uint32_t* kin = keys;
+    uint32_t* vin = vals;
+    uint32_t* kout = s.keys_alt;
+    uint32_t* vout = s.vals_alt;
+    for (int p = 0; p < passes; ++p) {
+        const int shift = p * bits;
+        const int pbits = min(bits, key_bits - shift);
+        radix_hist_kernel<<<tiles, kSortThreads, 0, stream>>>(kin, n, shift, pbits, tiles, s.hist);
+        cudaError_t e = exclusive_scan_u32(s.hist, (1 << pbits) * tiles, s.block_sums, stream);
+        if (e != cudaSuccess) return e;
+        radix_scatter_kernel<<<tiles, kSortThreads, 0, stream>>>(kin, vin, kout, vout, n, shift,
+                                                                 pbits, tiles, s.hist);
+        uint32_t* tk = kin; kin = kout; kout = tk;
+        uint32_t* tv = vin; vin = vout; vout = tv;
+    }
+    *out_keys = kin;
+    *out_vals = vin;
+    return cudaGetLastError();
+}
+
+cudaError_t launch_cell_keys(const float4* bodies, int n, GridShape g, uint32_t* keys,
+                             uint32_t* vals, cudaStream_t stream) {
+    if (n <= 0) return cudaSuccess;
+    cell_keys_kernel<<<blocks_for(n, 256), 256, 0, stream>>>(bodies, n, g.W, g.H, keys, vals);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_morton_keys(const float4* bodies, int n, int wbits, int hbits, uint32_t* keys,
+                               uint32_t* vals, cudaStream_t stream) {
+    if (n <= 0) return cudaSuccess;
+    morton_keys_kernel<<<blocks_for(n, 256), 256, 0, stream>>>(bodies, n, wbits, hbits, keys, vals);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_permute(const uint32_t* order, int n, const float4* bodies, const float2* accel,
+                           const float4* materials, float4* bodies_out, float2* accel_out,
+                           float4* materials_out, uint32_t* destinations, cudaStream_t stream) {
+    if (n <= 0) return cudaSuccess;
+    permute_kernel<<<blocks_for(n, 256), 256, 0, stream>>>(order, n, bodies, accel, materials,
+                                                           bodies_out, accel_out, materials_out,
+                                                           destinations);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_cell_build(const uint32_t* keys, const uint32_t* ids, int n, const float4* bodies,
+                              const float4* materials, int* cell_start, int* cell_count,
+                              uint32_t* cell_mass, float4* entries, cudaStream_t stream) {
+    if (n <= 0) return cudaSuccess;
+    cell_build_kernel<<<blocks_for(n, 256), 256, 0, stream>>>(keys, ids, n, bodies, materials,
+                                                              cell_start, cell_count, cell_mass,
+                                                              entries);
+    return cudaGetLastError();
+}
+
+}  // namespace p3m

@@ -1,0 +1,218 @@
+"""``GravityPipeline``: the host-side mirror of the reference's P3M seam.
+
+The reference's gravity solver is the Kotlin class ``GravityPipeline``
+(src/main/kotlin/dev/gravity/GravityPipeline.kt:73-81). This class keeps the
+names and meaning of its P3M surface — ``initialize_acceleration(n)``
+(:366-370), ``step(n)`` (:445-494), the ``bounded`` / ``field_acceleration_*``
+/ ``mutual_gravity`` properties (:97-121) and the private stages
+``build_force`` (:907), ``apply_kick`` (:1213), ``sort_bodies`` (:1269) — and
+runs every one of them through the C-ABI of include/p3m.h on the GPU.
+
+Errors follow the reference: invalid arguments raise ``ValueError``
+(Kotlin ``require``), invalid state raises ``RuntimeError`` (``check``).
+There is no CPU path: without the CUDA library or a GPU, construction fails.
+"""
+
+from __future__ import annotations
+
+import ctypes
+from typing import Optional
+
+import numpy as np
+
+from . import _abi
+from .config import P3MConfig
+
+
+class P3MArgumentError(_abi.P3MError, ValueError):
+    """Invalid argument, capacity or unsupported configuration."""
+
+
+_ARG_STATUSES = {_abi.P3M_ERR_INVALID_ARGUMENT, _abi.P3M_ERR_CAPACITY, _abi.P3M_ERR_UNSUPPORTED}
+
+
+def _ptr(a: Optional[np.ndarray]):
+    return None if a is None else a.ctypes.data_as(ctypes.c_void_p)
+
+
+class GravityPipeline:
+    """A P3M gravity context on the current CUDA device."""
+
+    def __init__(self, config: P3MConfig | None = None):
+        self.config = config or P3MConfig()
+        self._lib = _abi.load()
+        self._ctx = ctypes.c_void_p()
+        abi_cfg = self.config.to_abi()
+        rc = self._lib.p3m_create(ctypes.byref(abi_cfg), ctypes.byref(self._ctx))
+        if rc != _abi.P3M_OK:
+            msg = self._lib.p3m_last_error(None).decode()
+            raise (P3MArgumentError if rc in _ARG_STATUSES else _abi.P3MError)(rc, msg)
+        self._bounded = bool(self.config.bounded)
+        self._mutual = bool(self.config.mutual_gravity)
+        self._field = (0.0, 0.0)
+        self._mass_excess = 0.0
+
+    # ------------------------------------------------------------ plumbing
+    def _check(self, rc: int) -> None:
+        if rc != _abi.P3M_OK:
+            msg = self._lib.p3m_last_error(self._ctx).decode()
+            raise (P3MArgumentError if rc in _ARG_STATUSES else _abi.P3MError)(rc, msg)
+
+    @property
+    def handle(self) -> ctypes.c_void_p:
+        return self._ctx
+
+    def close(self) -> None:
+        if self._ctx:
+            self._lib.p3m_destroy(self._ctx)
+            self._ctx = ctypes.c_void_p()
+
+    def __enter__(self) -> "GravityPipeline":
+        return self
+
+    def __exit__(self, *exc) -> None:
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # ---------------------------------------------------------- properties
+    @property
+    def bounded(self) -> bool:
+        return self._bounded
+
+    @bounded.setter
+    def bounded(self, value: bool) -> None:
+        self._check(self._lib.p3m_set_bounded(self._ctx, 1 if value else 0))
+        self._bounded = bool(value)
+
+    @property
+    def mutual_gravity(self) -> bool:
+        return self._mutual
+
+    @mutual_gravity.setter
+    def mutual_gravity(self, value: bool) -> None:
+        self._check(self._lib.p3m_set_mutual_gravity(self._ctx, 1 if value else 0))
+        self._mutual = bool(value)
+
+    @property
+    def field_acceleration_x(self) -> float:
+        return self._field[0]
+
+    @field_acceleration_x.setter
+    def field_acceleration_x(self, value: float) -> None:
+        self.set_field_acceleration(value, self._field[1])
+
+    @property
+    def field_acceleration_y(self) -> float:
+        return self._field[1]
+
+    @field_acceleration_y.setter
+    def field_acceleration_y(self, value: float) -> None:
+        self.set_field_acceleration(self._field[0], value)
+
+    def set_field_acceleration(self, ax_px: float, ay_px: float) -> None:
+        """Uniform field in px/s^2 (GravityPipeline.kt:105-107)."""
+        self._check(self._lib.p3m_set_field_acceleration(self._ctx, float(ax_px), float(ay_px)))
+        self._field = (float(ax_px), float(ay_px))
+
+    @property
+    def mass_excess(self) -> float:
+        return self._mass_excess
+
+    @mass_excess.setter
+    def mass_excess(self, value: float) -> None:
+        self._check(self._lib.p3m_set_mass_excess(self._ctx, float(value)))
+        self._mass_excess = float(value)
+
+    # --------------------------------------------------------------- state
+    def upload(self, bodies: np.ndarray, materials: np.ndarray | None = None,
+               acceleration: np.ndarray | None = None) -> None:
+        """Upload float32 (n, 4) bodies [, (n, 4) materials, (n, 2) accelerations]."""
+        b = np.ascontiguousarray(bodies, dtype=np.float32).reshape(-1, 4)
+        n = b.shape[0]
+        m = None if materials is None else np.ascontiguousarray(materials, dtype=np.float32).reshape(n, 4)
+        a = None if acceleration is None else np.ascontiguousarray(acceleration, dtype=np.float32).reshape(n, 2)
+        self._check(self._lib.p3m_upload_state(self._ctx, _ptr(b), _ptr(m), _ptr(a), n))
+
+    def download(self, n: int):
+        """(bodies (n,4), materials (n,4), acceleration (n,2)) as float32."""
+        b = np.empty((n, 4), np.float32)
+        m = np.empty((n, 4), np.float32)
+        a = np.empty((n, 2), np.float32)
+        self._check(self._lib.p3m_download_state(self._ctx, _ptr(b), _ptr(m), _ptr(a), n))
+        return b, m, a
+
+    def bodies(self, n: int) -> np.ndarray:
+        return self.download(n)[0]
+
+    def acceleration(self, n: int) -> np.ndarray:
+        return self.download(n)[2]
+
+    def debug_get(self, which: int, dtype, count: int) -> np.ndarray:
+        out = np.empty(count, dtype=dtype)
+        self._check(self._lib.p3m_debug_get(self._ctx, which, _ptr(out), out.nbytes))
+        return out
+
+    def synchronize(self) -> None:
+        self._check(self._lib.p3m_synchronize(self._ctx))
+
+    # ----------------------------------------------------------- the step
+    def initialize_acceleration(self, active_bodies: int) -> None:
+        self._check(self._lib.p3m_initialize_acceleration(self._ctx, active_bodies))
+
+    def step(self, active_bodies: int, steps: int = 1) -> None:
+        self._check(self._lib.p3m_step(self._ctx, active_bodies, steps))
+
+    def build_force(self, active_bodies: int) -> None:
+        self._check(self._lib.p3m_build_force(self._ctx, active_bodies))
+
+    def apply_kick(self, active_bodies: int, initial: bool) -> None:
+        self._check(self._lib.p3m_apply_kick(self._ctx, active_bodies, 1 if initial else 0))
+
+    def sort_bodies(self, active_bodies: int) -> None:
+        self._check(self._lib.p3m_sort_bodies(self._ctx, active_bodies))
+
+    def drift(self, active_bodies: int, kick_dt: float, drift_dt: float) -> None:
+        self._check(self._lib.p3m_drift(self._ctx, active_bodies, float(kick_dt), float(drift_dt)))
+
+    def build_cell_lists(self, active_bodies: int) -> None:
+        self._check(self._lib.p3m_build_cell_lists(self._ctx, active_bodies))
+
+    # ------------------------------------------------------ intermediates
+    @property
+    def mesh_shape(self) -> tuple[int, int]:
+        g = self.config.gravity
+        k = 2 if self._bounded else 1
+        return g.grid_width * k, g.grid_height * k
+
+    def cell_lists(self, n: int):
+        """(keys[n], bodies[n], start[P], count[P], mass[P]) of the last cell sort."""
+        g = self.config.gravity
+        P = g.grid_width * g.grid_height
+        keys = self.debug_get(_abi.BUF_CELL_KEYS, np.uint32, n)
+        ids = self.debug_get(_abi.BUF_CELL_BODIES, np.int32, n)
+        start = self.debug_get(_abi.BUF_CELL_START, np.int32, P)
+        count = self.debug_get(_abi.BUF_CELL_COUNT, np.int32, P)
+        mass = self.debug_get(_abi.BUF_CELL_MASS, np.uint32, P)
+        return keys, ids, start, count, mass
+
+    def density(self) -> np.ndarray:
+        mw, mh = self.mesh_shape
+        dt = np.int64 if self.config.deposit_mode == _abi.P3M_DEPOSIT_I64 else np.uint32
+        return self.debug_get(_abi.BUF_DENSITY, dt, mw * mh).reshape(mh, mw)
+
+    def force(self) -> np.ndarray:
+        """Long-range mesh force, (MH, MW, 2) float32 (fx, fy)."""
+        mw, mh = self.mesh_shape
+        return self.debug_get(_abi.BUF_FORCE, np.float32, mw * mh * 2).reshape(mh, mw, 2)
+
+    def destinations(self, n: int) -> np.ndarray:
+        return self.debug_get(_abi.BUF_DESTINATIONS, np.uint32, n)
+
+    def green(self) -> np.ndarray:
+        mw, mh = self.mesh_shape
+        return self.debug_get(_abi.BUF_GREEN, np.float32, (mw // 2 + 1) * mh * 2).reshape(mh, mw // 2 + 1, 2)

@@ -1,0 +1,178 @@
+/*
+ * p3m.h — C-ABI of the B200 (sm_100a) P3M gravity step.
+ *
+ * This library replaces the P3M seam of Gravity's Kotlin `GravityPipeline`
+ * (src/main/kotlin/dev/gravity/GravityPipeline.kt). That class has no FFI of
+ * its own: the seam is the set of private methods that dispatch the GLSL
+ * compute shaders. Each entry point below names the reference method or shader
+ * it stands in for. The intended caller is a JNI shim inside `GravityPipeline`
+ * (JDK 18 toolchain: build.gradle.kts:39-41), so every signature uses plain C
+ * types, host or device pointers and sizes.
+ *
+ * Conventions
+ *  - Every function returns an int status: P3M_OK (0) or a negative
+ *    p3m_status. Nothing throws across the ABI. p3m_last_error() gives a
+ *    one-line message for the last failing call of a context.
+ *  - The library owns every device buffer of a context; the caller owns host
+ *    arrays. Host arrays are read or written before the call returns.
+ *  - All work of a context is ordered on its own CUDA stream. A context is
+ *    used from one host thread at a time, like the GL context thread the
+ *    reference runs on.
+ *  - Units follow the reference: positions in unit coordinates [0,1)^2,
+ *    velocities in unit/s, accelerations in unit/s^2
+ *    (GravityPipeline.kt:752-756). Bodies are float4 (x, y, vx, vy); materials
+ *    are float4 (mass, friction, solid, block) (GravityPipeline.kt:183-192).
+ */
+#ifndef GRAVITY_P3M_H
+#define GRAVITY_P3M_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define P3M_ABI_VERSION 1
+
+typedef enum p3m_status {
+    P3M_OK = 0,
+    P3M_ERR_INVALID_ARGUMENT = -1, /* Kotlin require() -> IllegalArgumentException */
+    P3M_ERR_OUT_OF_MEMORY = -2,
+    P3M_ERR_CUDA = -3,             /* a CUDA runtime call failed */
+    P3M_ERR_TIMEOUT = -4,          /* a bounded device wait gave up */
+    P3M_ERR_NON_FINITE = -5,       /* non-finite body state detected */
+    P3M_ERR_CAPACITY = -6,         /* more bodies than the context holds */
+    P3M_ERR_UNSUPPORTED = -7,      /* configuration outside the supported range */
+    P3M_ERR_STATE = -8             /* Kotlin check() -> IllegalStateException */
+} p3m_status;
+
+/* Mass deposit arithmetic. U32 is the reference's uint32 fixed point with
+ * massScale = clamp(4e9 / M_tot, 1, 65536) quanta per unit mass
+ * (build_grid.comp:64-69, GravityPipeline.kt:1546-1547). I64 is the precision
+ * form: int64 atomics with 2^-32 mass quanta, bit-reproducible at any size. */
+typedef enum p3m_deposit_mode {
+    P3M_DEPOSIT_U32 = 0,
+    P3M_DEPOSIT_I64 = 1
+} p3m_deposit_mode;
+
+/* Gravity configuration; defaults from GravityFieldConfig
+ * (GravityConfig.kt:641-654), CollisionConfig.timeStep / maximumSubsteps
+ * (GravityConfig.kt:677-678) and ParticleConfig.spatialSortInterval
+ * (GravityConfig.kt:621). Fill with p3m_config_default() first. */
+typedef struct p3m_config {
+    int32_t struct_size;                    /* sizeof(p3m_config) */
+    int32_t viewport_width;                 /* domain width in px (aspect = w/h) */
+    int32_t viewport_height;                /* domain height in px */
+    int32_t grid_width;                     /* physical grid, power of two, 16..4096 */
+    int32_t grid_height;                    /* physical grid, power of two, 16..4096 */
+    float gravitational_constant;           /* 0.035 */
+    float softening_cells;                  /* sigma in cells, 0.85 */
+    float local_search_sigma_multiplier;    /* 3 */
+    int32_t minimum_neighbor_radius_cells;  /* 1 */
+    int32_t maximum_neighbor_radius_cells;  /* 6 */
+    int32_t exact_neighbor_body_limit;      /* 2 */
+    int32_t maximum_home_body_interactions; /* 8 */
+    float minimum_distance_cell_fraction;   /* 0.05 */
+    float minimum_assignment_window_power;  /* 0.08 */
+    float time_step;                        /* 1/120 s */
+    int32_t drift_substeps;                 /* 16 (collision substeps drift the bodies) */
+    int32_t spatial_sort_interval;          /* 2; 0 disables the Morton reorder */
+    int32_t capacity;                       /* bodies the context can hold */
+    int32_t bounded;                        /* 0 torus, 1 walls (Hockney 2x mesh) */
+    int32_t deposit_mode;                   /* p3m_deposit_mode */
+    int32_t mutual_gravity;                 /* 1; 0 = uniform field only */
+} p3m_config;
+
+typedef struct p3m_ctx p3m_ctx;
+
+/* Device buffers readable through p3m_debug_get / p3m_device_pointer. */
+typedef enum p3m_buffer {
+    P3M_BUF_BODIES = 0,       /* float4[n]  (x, y, vx, vy) */
+    P3M_BUF_ACCELERATION = 1, /* float2[n]  last acceleration */
+    P3M_BUF_MATERIALS = 2,    /* float4[n]  (mass, friction, solid, block) */
+    P3M_BUF_CELL_KEYS = 3,    /* uint32[n]  home cell of each sorted entry */
+    P3M_BUF_CELL_BODIES = 4,  /* int32[n]   body IDs sorted by (cell asc, ID desc) */
+    P3M_BUF_CELL_START = 5,   /* int32[P]   first sorted entry of a cell (valid where count > 0) */
+    P3M_BUF_CELL_COUNT = 6,   /* int32[P]   bodies per cell */
+    P3M_BUF_CELL_MASS = 7,    /* uint32[P]  sum of round(mass * 256) per cell */
+    P3M_BUF_DENSITY = 8,      /* uint32[M] (U32) or int64[M] (I64) fixed-point mesh */
+    P3M_BUF_FORCE = 9,        /* float2[M]  long-range mesh force (fx, fy) */
+    P3M_BUF_DESTINATIONS = 10,/* uint32[n]  new ID of every body after the last reorder */
+    P3M_BUF_GREEN = 11,       /* float2[(MW/2+1)*MH] spectral multipliers (gx, gy) */
+    P3M_BUF_COUNT_ = 12
+} p3m_buffer;
+
+/* ---- lifecycle ---------------------------------------------------------- */
+
+/* Defaults of GravityFieldConfig / CollisionConfig / ParticleConfig for a
+ * 2560x1440 domain and a 512x256 grid. */
+int p3m_config_default(p3m_config* config);
+
+/* Replaces the GravityPipeline constructor's P3M part: buffers
+ * (GravityPipeline.kt:183-246), twiddles (initializeTwiddles, :1359-1371) and
+ * the Green's-function spectra (initializeKernel, :1341-1357). Validation
+ * mirrors GravityFieldConfig.init (GravityConfig.kt:655-673). */
+int p3m_create(const p3m_config* config, p3m_ctx** out);
+
+/* Replaces GravityPipeline.close (GravityPipeline.kt:1556-1620). */
+int p3m_destroy(p3m_ctx* ctx);
+
+/* Message of the last failing call of ctx (or of p3m_create when ctx is
+ * NULL); never NULL. */
+const char* p3m_last_error(const p3m_ctx* ctx);
+const char* p3m_status_string(int status);
+
+/* ---- state hand-off ----------------------------------------------------- */
+
+/* Replaces seedBodies / glBufferSubData uploads (GravityPipeline.kt:724-770,
+ * :1438-1481). Any pointer may be NULL to leave that buffer unchanged. */
+int p3m_upload_state(p3m_ctx* ctx, const float* bodies4, const float* materials4,
+                     const float* acceleration2, int32_t n);
+/* Readback (the reference maps the SSBOs: GravityPipeline.kt:378-443). */
+int p3m_download_state(p3m_ctx* ctx, float* bodies4, float* materials4,
+                       float* acceleration2, int32_t n);
+/* Copy a whole buffer to host memory; bytes must equal the buffer's size. */
+int p3m_debug_get(p3m_ctx* ctx, int32_t which, void* host, size_t bytes);
+/* Device address and size of a buffer (for callers that share device memory,
+ * e.g. a renderer); the pointer stays valid until p3m_destroy. */
+int p3m_device_pointer(p3m_ctx* ctx, int32_t which, void** device, size_t* bytes);
+
+/* ---- properties (GravityPipeline.kt:97-121) ----------------------------- */
+
+/* `bounded` setter: walls need 2*max(grid) <= 4096 (GravityPipeline.kt:97-103). */
+int p3m_set_bounded(p3m_ctx* ctx, int32_t bounded);
+/* `fieldAccelerationX/Y` in px/s^2; stored as unit/s^2 like applyKick
+ * (GravityPipeline.kt:1230-1234). */
+int p3m_set_field_acceleration(p3m_ctx* ctx, float ax_px, float ay_px);
+int p3m_set_mutual_gravity(p3m_ctx* ctx, int32_t enabled);
+/* massExcess: mass of the active bodies minus their count (GravityPipeline.kt:213). */
+int p3m_set_mass_excess(p3m_ctx* ctx, float mass_excess);
+
+/* ---- the step (GravityPipeline.kt:366-370, :445-494) -------------------- */
+
+/* initializeAcceleration(n): normalizeTo, buildForce, applyKick(initial). */
+int p3m_initialize_acceleration(p3m_ctx* ctx, int32_t n);
+/* step(n) repeated `steps` times, gravity only: Morton reorder every
+ * spatial_sort_interval steps, half kick + drift substeps, buildForce,
+ * applyKick. Collisions, liquid and sleep are not part of this path. */
+int p3m_step(p3m_ctx* ctx, int32_t n, int32_t steps);
+
+/* Separately callable stages, for parity tests and for a host that keeps its
+ * own loop. */
+int p3m_sort_bodies(p3m_ctx* ctx, int32_t n);                   /* sortBodies, :1269-1319 */
+int p3m_drift(p3m_ctx* ctx, int32_t n, float kick_dt, float drift_dt); /* collision_build.comp:40-51 */
+int p3m_build_force(p3m_ctx* ctx, int32_t n);                   /* buildForce, :907-973 */
+int p3m_apply_kick(p3m_ctx* ctx, int32_t n, int32_t initial);   /* applyKick, :1213-1261 */
+/* Cell keys, 64-bit-key radix sort and cell lists only (the first part of
+ * build_grid.comp, as CSR lists). */
+int p3m_build_cell_lists(p3m_ctx* ctx, int32_t n);
+
+/* Wait for the context's stream; returns the first pending device error. */
+int p3m_synchronize(p3m_ctx* ctx);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* GRAVITY_P3M_H */

@@ -1,0 +1,170 @@
+"""GPU parity of the P3M path against the CPU oracle, through the C-ABI.
+
+Bit-exact: cell keys, cell lists (IDs in walk order), cell occupancy and
+cell masses, the fixed-point density mesh (uint32 and int64 forms), the
+Morton reorder. Within REL_RMS_TOL (1e-5 relative RMS): the long-range force
+mesh, accelerations, velocities and positions.
+"""
+
+import numpy as np
+import pytest
+
+import oracle
+from gravity_b200 import _abi
+from gravity_b200.pipeline import GravityPipeline
+
+from helpers import REL_RMS_TOL, clustered, rel_rms, small_torus
+
+pytestmark = pytest.mark.gpu
+
+
+def pair(sc, **overrides):
+    cfg = sc.config.with_(**overrides) if overrides else sc.config
+    gpu = GravityPipeline(cfg)
+    ref = oracle.OracleSim(cfg)
+    gpu.upload(sc.bodies, sc.materials)
+    ref.upload(sc.bodies, sc.materials)
+    return gpu, ref
+
+
+def assert_lists_equal(gpu, ref, n):
+    gk, gi, gs, gc, gm = gpu.cell_lists(n)
+    rk, ri, rs, rc, rm = ref.cell_lists(n)
+    np.testing.assert_array_equal(gc, rc, err_msg="cell occupancy")
+    np.testing.assert_array_equal(gm, rm, err_msg="cell masses")
+    np.testing.assert_array_equal(gk, rk, err_msg="sorted cell keys")
+    np.testing.assert_array_equal(gi, ri, err_msg="cell list order (body IDs)")
+    occupied = rc > 0
+    np.testing.assert_array_equal(gs[occupied], rs[occupied], err_msg="cell starts")
+
+
+SCENES = {
+    "uniform": lambda: small_torus(n=4000),
+    "clustered": lambda: clustered(n=6000),
+    "clustered_walls": lambda: clustered(n=6000, bounded=True),
+    "wide_grid": lambda: small_torus(n=20000, grid=(512, 256)),
+}
+
+
+@pytest.mark.parametrize("name", sorted(SCENES))
+def test_initial_acceleration_matches_oracle(cuda_device, name):
+    sc = SCENES[name]()
+    n = sc.n
+    gpu, ref = pair(sc)
+    with gpu, ref:
+        gpu.initialize_acceleration(n)
+        ref.initialize_acceleration(n)
+        assert_lists_equal(gpu, ref, n)
+        np.testing.assert_array_equal(gpu.density(), ref.density(), err_msg="density mesh")
+        f_gpu, f_ref = gpu.force(), ref.force()
+        assert rel_rms(f_gpu, f_ref) < REL_RMS_TOL, rel_rms(f_gpu, f_ref)
+        b_gpu, _, a_gpu = gpu.download(n)
+        b_ref, _, a_ref = ref.download(n)
+        np.testing.assert_array_equal(b_gpu, b_ref, err_msg="initial pass must not move bodies")
+        assert rel_rms(a_gpu, a_ref) < REL_RMS_TOL, rel_rms(a_gpu, a_ref)
+
+
+def test_int64_deposit_bit_exact_and_reproducible(cuda_device):
+    sc = clustered(n=6000)
+    gpu, ref = pair(sc, deposit_mode=_abi.P3M_DEPOSIT_I64)
+    with gpu, ref:
+        gpu.initialize_acceleration(sc.n)
+        ref.initialize_acceleration(sc.n)
+        d1 = gpu.density()
+        np.testing.assert_array_equal(d1, ref.density())
+        # The total mass is conserved exactly up to rounding of each weight.
+        total = d1.astype(np.float64).sum() / 2.0 ** 32
+        assert abs(total - sc.materials[:, 0].sum()) < 1e-3
+        gpu.build_force(sc.n)
+        np.testing.assert_array_equal(gpu.density(), d1, err_msg="run-to-run bit reproducibility")
+        assert rel_rms(gpu.force(), ref.force()) < REL_RMS_TOL
+
+
+@pytest.mark.parametrize("name", ["uniform", "clustered", "clustered_walls"])
+def test_steps_match_oracle(cuda_device, name):
+    sc = SCENES[name]()
+    n = sc.n
+    gpu, ref = pair(sc)
+    with gpu, ref:
+        gpu.initialize_acceleration(n)
+        ref.initialize_acceleration(n)
+        for _ in range(5):
+            gpu.step(n)
+            ref.step(n)
+        b_gpu, m_gpu, a_gpu = gpu.download(n)
+        b_ref, m_ref, a_ref = ref.download(n)
+        # Morton reorders happened at steps 0, 2, 4: same permutation.
+        np.testing.assert_array_equal(m_gpu, m_ref, err_msg="materials follow the same permutation")
+        np.testing.assert_array_equal(gpu.destinations(n), ref.destinations(n))
+        assert rel_rms(b_gpu[:, :2], b_ref[:, :2]) < REL_RMS_TOL
+        assert rel_rms(b_gpu[:, 2:], b_ref[:, 2:]) < REL_RMS_TOL
+        assert rel_rms(a_gpu, a_ref) < REL_RMS_TOL
+
+
+def test_sort_bodies_is_bit_exact_permutation(cuda_device):
+    sc = clustered(n=6000)
+    n = sc.n
+    gpu, ref = pair(sc)
+    with gpu, ref:
+        acc = np.random.default_rng(1).uniform(-0.5, 0.5, (n, 2)).astype(np.float32)
+        gpu.upload(sc.bodies, sc.materials, acc)
+        ref.upload(sc.bodies, sc.materials, acc)
+        gpu.sort_bodies(n)
+        ref.sort_bodies(n)
+        bg, mg, ag = gpu.download(n)
+        br, mr, ar = ref.download(n)
+        np.testing.assert_array_equal(bg, br)
+        np.testing.assert_array_equal(mg, mr)
+        np.testing.assert_array_equal(ag, ar)
+        dest = gpu.destinations(n)
+        np.testing.assert_array_equal(np.sort(dest), np.arange(n, dtype=np.uint32))
+        np.testing.assert_array_equal(bg[dest], sc.bodies)
+
+
+def test_mutual_gravity_off_uses_field_only(cuda_device):
+    sc = small_torus(n=3000)
+    gpu, ref = pair(sc)
+    with gpu, ref:
+        for s in (gpu, ref):
+            s.set_field_acceleration(0.0, -300.0)
+        gpu.mutual_gravity = False
+        ref.set_mutual_gravity(False)
+        gpu.initialize_acceleration(sc.n)
+        ref.initialize_acceleration(sc.n)
+        gpu.step(sc.n, 3)
+        ref.step(sc.n, 3)
+        bg, _, ag = gpu.download(sc.n)
+        br, _, ar = ref.download(sc.n)
+        np.testing.assert_array_equal(bg, br)
+        np.testing.assert_array_equal(ag, ar)
+
+
+def test_edge_sizes(cuda_device):
+    """Empty, single-body and tiny systems. With one or two bodies the exact
+    mesh self-force is zero and both sides hold FFT round-off, so the
+    accelerations are compared against the scale of the force mesh."""
+    sc = small_torus(n=5)
+    gpu, ref = pair(sc)
+    with gpu, ref:
+        for n in (0, 1, 2, 5):
+            gpu.initialize_acceleration(n)
+            ref.initialize_acceleration(n)
+            gpu.step(n, 2)
+            ref.step(n, 2)
+            bg, _, ag = gpu.download(n)
+            br, _, ar = ref.download(n)
+            if n:
+                assert rel_rms(bg, br) < REL_RMS_TOL
+                scale = float(np.abs(ref.force()).max())
+                assert float(np.abs(ag - ar).max()) <= REL_RMS_TOL * scale
+
+
+def test_capacity_and_arguments_fail_loudly(cuda_device):
+    sc = small_torus(n=100)
+    with GravityPipeline(sc.config) as gpu:
+        with pytest.raises(ValueError):
+            gpu.step(sc.n + 1)
+        with pytest.raises(ValueError):
+            gpu.step(-1)
+    with pytest.raises(ValueError):
+        GravityPipeline(sc.config.with_(capacity=0))
