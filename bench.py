@@ -1,0 +1,459 @@
+#!/usr/bin/env python
+"""P3M bodies*steps/s on B200 — the benchmark of this library.
+
+One step = one gravity-only P3M leapfrog step of the workload
+(GravityPipeline.step without collisions): Morton reorder every second step,
+half kick + drift, cell-key sort and lists, CIC deposit, real FFT with the
+Green's multiply, inverse, interpolation + short range + half kick.
+
+Default workload (N=1): 400,000 bodies in two projected Plummer spheres
+inside walls, physical grid 512x256 (Hockney FFT mesh 1024x512), uint32
+fixed-point deposit, FP32 forces. The whole state and mesh (~40 MB) fit in the
+126 MB L2, so L2 is flushed (a 256 MiB write) before every timed step, outside
+the step's events.
+
+Printed (rank 0, one JSON line):
+  value     bodies*steps/s from CUDA events around each step, state resident
+            in HBM, summed over the K timed steps, max over ranks.
+  e2e       the same through the public API with host buffers: every step
+            uploads bodies + materials from page-locked memory, steps, and
+            reads the bodies back (host wall clock, synchronous).
+  roofline  the dominant stage's algorithmic bytes / its event-timed average
+            duration, against the measured HBM copy bandwidth.
+  cpu_baseline  the CPU oracle (the C++ restatement of the reference's
+            shaders) on this host's cores, on a bounded sample.
+
+`--impl reference` times the reference's CPU path, i.e. the oracle port (the
+reference has no CPU implementation and its GLSL cannot run here), with all
+host threads, on the same workload and metric.
+
+Multi-GPU (torchrun): replicas only. Every rank runs its own copy of the
+workload; value = all bodies*steps / the slowest rank's time.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import re
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+REPO = Path(__file__).resolve().parent
+if str(REPO) not in sys.path:
+    sys.path.insert(0, str(REPO))
+
+METRIC = ("P3M bodies·steps/s on 1 B200 (plain vs chosen form) at stated force RMS err "
+          "vs FP64")
+UNIT = "bodies*steps/s"
+L2_FLUSH_BYTES = 256 << 20
+FORCE_SAMPLE = 4096
+
+
+# ----------------------------------------------------------------- workloads
+def make_workload(name: str):
+    from gravity_b200 import scenarios
+
+    if name == "plummer_walls":
+        return scenarios.plummer_walls()
+    if name == "uniform_torus":
+        return scenarios.uniform_torus()
+    if name == "lattice_scale":
+        return scenarios.lattice_scale()
+    if name == "lattice_scale_u32":
+        from gravity_b200 import _abi
+        return scenarios.lattice_scale(deposit_mode=_abi.P3M_DEPOSIT_U32)
+    raise SystemExit(f"unknown workload {name}")
+
+
+def mesh_sizes(sc):
+    g = sc.config.gravity
+    P = g.grid_width * g.grid_height
+    k = 4 if sc.config.bounded else 1
+    return P, P * k
+
+
+def stage_bytes(sc, stage: str, radix_passes: int) -> float:
+    """Algorithmic bytes of one launch of a stage (the per-unit figures are
+    listed in DESIGN.md, section "Kernels and their rooflines")."""
+    n = sc.n
+    P, M = mesh_sizes(sc)
+    i64 = sc.config.deposit_mode == 1
+    d = 8 if i64 else 4
+    if stage == "drift":
+        return 48.0 * n
+    if stage == "cell_lists":
+        return 16.0 * radix_passes * n + 44.0 * n + 12.0 * P
+    if stage == "deposit":
+        return 16.0 * n + 2.0 * d * M
+    if stage == "forward_fft":
+        return (d + 4.0) * M
+    if stage == "spectral":
+        return 16.0 * M
+    if stage == "inverse_fft":
+        return 16.0 * M
+    if stage == "kick":
+        return 56.0 * n + 20.0 * P
+    if stage == "spatial_sort":
+        return 16.0 * radix_passes * n + 88.0 * n
+    return 0.0
+
+
+def radix_passes_for(count: int) -> int:
+    bits = max(1, (count - 1).bit_length())
+    return (bits + 7) // 8
+
+
+def read_traffic(stage: str, workload: str):
+    """DRAM bytes per launch from a committed ncu summary, if one exists
+    (a line `traffic_bytes_per_launch: <int>` in profiles/<stage>_<workload>*.md)."""
+    for f in sorted((REPO / "profiles").glob(f"{stage}_{workload}*.md")):
+        m = re.search(r"traffic_bytes_per_launch:\s*([0-9.eE+]+)", f.read_text())
+        if m:
+            return float(m.group(1))
+    return None
+
+
+def measured_peaks():
+    p = REPO / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+# -------------------------------------------------------------------- clocks
+class ClockSampler:
+    """nvidia-smi samples during the timed region."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.device_index = device_index
+        self.proc = None
+        self.lines: list[str] = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits",
+                 "-i", str(self.device_index), "-lms", "100"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self._t = threading.Thread(target=self._read, daemon=True)
+            self._t.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self._t.join(timeout=2)
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx.append(float(parts[2]))
+            except ValueError:
+                continue
+            for name, val in zip(names, parts[5:9]):
+                if val.lower().startswith("active"):
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# -------------------------------------------------------------- CPU baseline
+def cpu_oracle_rate(sc, budget_s: float, threads: int | None = None, warmup: int = 1,
+                    max_steps: int | None = None):
+    """bodies*steps/s of the CPU oracle on this workload: initialisation and
+    `warmup` steps untimed, then steps until `budget_s` is spent."""
+    import oracle
+
+    if threads:
+        oracle.set_threads(threads)
+    used = oracle.max_threads()
+    sim = oracle.OracleSim(sc.config)
+    sim.upload(sc.bodies, sc.materials)
+    sim.initialize_acceleration(sc.n)
+    for _ in range(warmup):
+        sim.step(sc.n)
+    steps = 0
+    t0 = time.perf_counter()
+    while True:
+        sim.step(sc.n)
+        steps += 1
+        el = time.perf_counter() - t0
+        if el >= budget_s or (max_steps and steps >= max_steps):
+            break
+    sim.close()
+    return sc.n * steps / el, steps, el, used
+
+
+# ------------------------------------------------------------------ helpers
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+def init_dist(ws: int, local: int):
+    import torch
+    import torch.distributed as dist
+
+    if ws > 1:
+        torch.cuda.set_device(local)
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    return dist if ws > 1 else None
+
+
+def allreduce_max(dist, value: float) -> float:
+    if dist is None:
+        return value
+    import torch
+
+    t = torch.tensor([value], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def force_error_vs_fp64(pipe, sc) -> float:
+    """Relative RMS error of the P3M accelerations of a seeded 4096-body
+    subsample against the FP64 direct sum, on the initial state."""
+    n = sc.n
+    rng = np.random.default_rng(4096)
+    targets = np.sort(rng.choice(n, size=min(FORCE_SAMPLE, n), replace=False)).astype(np.int32)
+    pipe.upload(sc.bodies, sc.materials)
+    pipe.initialize_acceleration(n)
+    a = pipe.acceleration(n)[targets].astype(np.float64)
+    ref = pipe.direct_accel_f64(n, targets)
+    return float(np.sqrt(np.sum((a - ref) ** 2) / np.sum(ref ** 2)))
+
+
+# -------------------------------------------------------------------- arms
+def run_reference(args, ws, rank):
+    if rank != 0:
+        return
+    sc = make_workload(args.workload)
+    threads = os.cpu_count() or 1
+    budget = max(5.0, min(90.0, float(args.steps) * 2.0))
+    rate, steps, el, used = cpu_oracle_rate(sc, budget, threads=threads,
+                                            warmup=min(args.warmup, 1), max_steps=args.steps)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": rate, "unit": UNIT, "n_gpus": ws,
+        "steps": steps, "warmup": min(args.warmup, 1), "ms_per_step": 1000.0 * el / steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic", "config": workload_config(sc, args),
+        "cpu_baseline": {"value": rate, "unit": UNIT, "cores": used, "kind": "port",
+                         "sample": f"{steps} P3M steps of the {sc.n}-body {args.workload} "
+                                   f"workload ({el:.1f} s) after initialisation and "
+                                   f"{min(args.warmup, 1)} untimed step(s)"},
+        "e2e": {"value": rate, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def workload_config(sc, args):
+    g = sc.config.gravity
+    P, M = mesh_sizes(sc)
+    mw = g.grid_width * (2 if sc.config.bounded else 1)
+    mh = g.grid_height * (2 if sc.config.bounded else 1)
+    return {
+        "workload": args.workload, "n_bodies": sc.n,
+        "grid": f"{g.grid_width}x{g.grid_height}", "fft_mesh": f"{mw}x{mh}",
+        "boundary": "walls" if sc.config.bounded else "torus",
+        "deposit": "int64" if sc.config.deposit_mode == 1 else "uint32",
+        "viewport_px": f"{sc.config.viewport_width}x{sc.config.viewport_height}",
+        "dt": sc.config.time_step, "drift_substeps": sc.config.drift_substeps,
+        "spatial_sort_interval": sc.config.spatial_sort_interval,
+        "l2": "flushed (256 MiB write) before every timed step",
+        "parallelism": "replicas" if args.gpus > 1 else "single",
+    }
+
+
+def run_b200(args, ws, rank, local):
+    import torch
+
+    from gravity_b200 import _abi
+    from gravity_b200.pipeline import GravityPipeline, PinnedArray, kernel_launches
+
+    dist = init_dist(ws, local)
+    torch.cuda.set_device(local)
+    sc = make_workload(args.workload)
+    n = sc.n
+    pipe = GravityPipeline(sc.config)
+    stream = torch.cuda.ExternalStream(pipe.stream_handle())
+    flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device="cuda")
+
+    force_err = force_error_vs_fp64(pipe, sc) if rank == 0 else None
+
+    # ---- value: state resident in HBM, device-timed
+    pipe.upload(sc.bodies, sc.materials)
+    pipe.initialize_acceleration(n)
+    for _ in range(args.warmup):
+        pipe.step(n)
+    pipe.synchronize()
+    if dist:
+        dist.barrier()
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    stops = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    clocks = ClockSampler(local)
+    clocks.start()
+    time.sleep(0.3)
+    launches0 = kernel_launches()
+    with torch.cuda.stream(stream):
+        for i in range(args.steps):
+            flush.zero_()
+            starts[i].record(stream)
+            pipe.step(n)
+            stops[i].record(stream)
+    torch.cuda.synchronize()
+    pipe.synchronize()
+    launches = kernel_launches() - launches0
+    clk = clocks.stop()
+    total_ms = sum(a.elapsed_time(b) for a, b in zip(starts, stops))
+    total_ms = allreduce_max(dist, total_ms)
+    if dist:
+        dist.barrier()
+    value = ws * n * args.steps / (total_ms / 1000.0)
+    ms_per_step = total_ms / args.steps
+
+    # ---- per-stage device time: the same steps with stage events recorded
+    # (kernels launched one by one; the value pass above replays graphs).
+    pipe.profile_enable(True)
+    with torch.cuda.stream(stream):
+        for i in range(args.steps):
+            flush.zero_()
+            pipe.step(n)
+    stages = pipe.profile_read()
+    pipe.profile_enable(False)
+
+    # ---- e2e: through the public API with page-locked host buffers
+    e2e_steps = args.steps if args.e2e_steps is None else min(args.steps, args.e2e_steps)
+    hb = PinnedArray((n, 4))
+    hm = PinnedArray((n, 4))
+    out = PinnedArray((n, 4))
+    hb.array[:] = sc.bodies
+    hm.array[:] = sc.materials
+    pipe.upload_n(n, hb.array, hm.array)
+    pipe.initialize_acceleration(n)
+    for _ in range(min(args.warmup, 3)):
+        pipe.upload_n(n, hb.array, hm.array)
+        pipe.step(n)
+        pipe.download_into(n, out.array)
+    if dist:
+        dist.barrier()
+    e2e_s = 0.0
+    for _ in range(e2e_steps):
+        with torch.cuda.stream(stream):
+            flush.zero_()
+        pipe.synchronize()
+        t0 = time.perf_counter()
+        pipe.upload_n(n, hb.array, hm.array)
+        pipe.step(n)
+        pipe.download_into(n, out.array)
+        e2e_s += time.perf_counter() - t0
+    e2e_s = allreduce_max(dist, e2e_s)
+    e2e_value = ws * n * e2e_steps / e2e_s
+    for a in (hb, hm, out):
+        a.free()
+
+    if rank == 0:
+        peak, peak_kind = measured_peaks()
+        P, M = mesh_sizes(sc)
+        g = sc.config.gravity
+        cell_passes = radix_passes_for(P)
+        from gravity_b200.config import sort_axis_bits
+        morton_bits = sort_axis_bits(sc.config.viewport_width) + sort_axis_bits(sc.config.viewport_height)
+        morton_passes = (morton_bits + 7) // 8
+        stage_rows = {}
+        for name, (ms, cnt) in stages.items():
+            if cnt == 0:
+                continue
+            passes = morton_passes if name == "spatial_sort" else cell_passes
+            avg_ms = ms / cnt
+            b = stage_bytes(sc, name, passes)
+            stage_rows[name] = {"ms_per_launch": avg_ms, "launches": cnt,
+                                "algorithmic_bytes": b,
+                                "gbs": b / (avg_ms / 1000.0) / 1e9 if avg_ms > 0 else None}
+        dominant = max(stage_rows, key=lambda k: stage_rows[k]["ms_per_launch"] * stage_rows[k]["launches"])
+        dom = stage_rows[dominant]
+        achieved = dom["gbs"]
+        traffic = read_traffic(dominant, args.workload)
+        cpu = None
+        if not args.no_cpu_baseline:
+            rate, steps, el, used = cpu_oracle_rate(sc, args.cpu_seconds, threads=os.cpu_count())
+            cpu = {"value": rate, "unit": UNIT, "cores": used, "kind": "port",
+                   "sample": f"{steps} P3M steps of the {n}-body {args.workload} workload "
+                             f"({el:.1f} s) after initialisation and 1 untimed step"}
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": workload_config(sc, args),
+            "force_rms_err_vs_fp64": force_err,
+            "roofline": {"bound": "hbm", "kernel": dominant, "achieved": achieved, "peak": peak,
+                         "unit": "GB/s", "frac": achieved / peak if achieved else None,
+                         "traffic": traffic, "peak_source": peak_kind},
+            "stages": stage_rows,
+            "cpu_baseline": cpu,
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 32 * n,
+                    "d2h_bytes_per_step": 16 * n, "steps": e2e_steps},
+            "gpu_launches": launches,
+            "clocks": clk,
+        }
+        print(json.dumps(line), flush=True)
+    pipe.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=2000)
+    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
+    ap.add_argument("--workload", default="plummer_walls",
+                    choices=["plummer_walls", "uniform_torus", "lattice_scale", "lattice_scale_u32"])
+    ap.add_argument("--e2e-steps", type=int, default=None)
+    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        raise SystemExit("--warmup must be >= 3")
+    ws, rank, local = dist_env()
+    if args.impl == "reference":
+        run_reference(args, ws, rank)
+        return
+    run_b200(args, ws, rank, local)
+
+
+if __name__ == "__main__":
+    main()

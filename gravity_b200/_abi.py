@@ -80,6 +80,7 @@ SIGNATURES = {
     "p3m_last_error": (ctypes.c_char_p, [_vp]),
     "p3m_status_string": (ctypes.c_char_p, [ctypes.c_int]),
     "p3m_upload_state": (ctypes.c_int, [_vp, _vp, _vp, _vp, _i32]),
+    "p3m_upload_range": (ctypes.c_int, [_vp, _i32, _i32, _vp, _vp, _vp]),
     "p3m_download_state": (ctypes.c_int, [_vp, _vp, _vp, _vp, _i32]),
     "p3m_debug_get": (ctypes.c_int, [_vp, _i32, _vp, ctypes.c_size_t]),
     "p3m_device_pointer": (ctypes.c_int, [_vp, _i32, ctypes.POINTER(_vp),
@@ -96,7 +97,20 @@ SIGNATURES = {
     "p3m_apply_kick": (ctypes.c_int, [_vp, _i32, _i32]),
     "p3m_build_cell_lists": (ctypes.c_int, [_vp, _i32]),
     "p3m_synchronize": (ctypes.c_int, [_vp]),
+    "p3m_set_graphs": (ctypes.c_int, [_vp, _i32]),
+    "p3m_profile_enable": (ctypes.c_int, [_vp, _i32]),
+    "p3m_profile_read": (ctypes.c_int, [_vp, _vp, _vp]),
+    "p3m_kernel_launches": (ctypes.c_int64, []),
+    "p3m_get_stream": (ctypes.c_int, [_vp, ctypes.POINTER(_vp)]),
+    "p3m_host_alloc": (ctypes.c_int, [ctypes.c_size_t, ctypes.POINTER(_vp)]),
+    "p3m_host_free": (ctypes.c_int, [_vp]),
+    "p3m_nonfinite_count": (ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_int64)]),
+    "p3m_direct_accel_f64": (ctypes.c_int, [_vp, _i32, _vp, _i32, _vp]),
+    "p3m_diagnostics_f64": (ctypes.c_int, [_vp, _i32, _vp]),
 }
+
+STAGES = ("spatial_sort", "drift", "cell_lists", "deposit", "forward_fft", "spectral",
+          "inverse_fft", "kick")
 
 _lock = threading.Lock()
 _lib = None

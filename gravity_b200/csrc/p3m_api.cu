@@ -5,12 +5,20 @@
 #include "p3m_internal.cuh"
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
 #include <new>
 #include <string>
 #include <vector>
+
+namespace p3m {
+namespace {
+std::atomic<long long> g_launches{0};
+}
+void count_launches(int kernels) { g_launches.fetch_add(kernels, std::memory_order_relaxed); }
+}  // namespace p3m
 
 namespace {
 
@@ -46,6 +54,55 @@ int bits_for(long long count) {  // ceil(log2(count)), at least 1
     while ((1LL << b) < count) ++b;
     return b;
 }
+
+// ------------------------------------------------------------ stage timing
+cudaEvent_t take_event(p3m_ctx* ctx) {
+    if (!ctx->free_events.empty()) {
+        cudaEvent_t e = ctx->free_events.back();
+        ctx->free_events.pop_back();
+        return e;
+    }
+    cudaEvent_t e = nullptr;
+    if (cudaEventCreate(&e) != cudaSuccess) return nullptr;
+    return e;
+}
+
+// Folds recorded intervals into the per-stage totals (waits for them).
+void fold_stages(p3m_ctx* ctx) {
+    if (ctx->pending.empty()) return;
+    cudaEventSynchronize(ctx->pending.back().stop);
+    for (const auto& p : ctx->pending) {
+        float ms = 0.0f;
+        if (cudaEventElapsedTime(&ms, p.start, p.stop) == cudaSuccess) {
+            ctx->stage_ms[p.stage] += ms;
+            ctx->stage_intervals[p.stage] += 1;
+        }
+        ctx->free_events.push_back(p.start);
+        ctx->free_events.push_back(p.stop);
+    }
+    ctx->pending.clear();
+}
+
+// Records one stage interval around a scope when profiling is on.
+struct StageScope {
+    p3m_ctx* ctx;
+    int stage;
+    cudaEvent_t start = nullptr;
+    StageScope(p3m_ctx* c, int s) : ctx(c), stage(s) {
+        if (ctx->profiling) {
+            start = take_event(ctx);
+            if (start) cudaEventRecord(start, ctx->stream);
+        }
+    }
+    ~StageScope() {
+        if (!start) return;
+        cudaEvent_t stop = take_event(ctx);
+        if (!stop) return;
+        cudaEventRecord(stop, ctx->stream);
+        ctx->pending.push_back({stage, start, stop});
+        if (ctx->pending.size() >= 4096) fold_stages(ctx);
+    }
+};
 
 // GravityPipeline.kt:1649-1650 sortAxisBits.
 int sort_axis_bits(int extent) { return std::min(10, log2_floor(std::max(1, extent / 4))); }
@@ -132,7 +189,12 @@ int dalloc(p3m_ctx* ctx, T** p, size_t count, const char* what) {
 }
 
 void free_all(p3m_ctx* ctx) {
-    void* ptrs[] = {ctx->bodies, ctx->bodies_alt, ctx->accel, ctx->accel_alt, ctx->materials,
+    fold_stages(ctx);
+    for (auto& g : ctx->graphs) cudaGraphExecDestroy(g.exec);
+    ctx->graphs.clear();
+    for (cudaEvent_t e : ctx->free_events) cudaEventDestroy(e);
+    ctx->free_events.clear();
+    void* ptrs[] = {ctx->diag, ctx->bodies, ctx->bodies_alt, ctx->accel, ctx->accel_alt, ctx->materials,
                     ctx->materials_alt, ctx->destinations, ctx->status, ctx->keys, ctx->vals,
                     ctx->sort.keys_alt, ctx->sort.vals_alt, ctx->sort.hist, ctx->sort.block_sums,
                     ctx->cell_start, ctx->cell_count, ctx->cell_mass, ctx->entries, ctx->density,
@@ -175,6 +237,7 @@ int check_n(p3m_ctx* ctx, int n) {
 
 // Cell lists from keys already written in descending ID order.
 int lists_from_keys(p3m_ctx* ctx, int n) {
+    StageScope scope(ctx, P3M_STAGE_CELL_LISTS);
     const long long P = (long long)phys_cells(ctx);
     uint32_t* sk = ctx->keys;
     uint32_t* sv = ctx->vals;
@@ -197,18 +260,32 @@ int mesh_force(p3m_ctx* ctx, int n) {
     if (st != P3M_OK) return st;
     const bool i64 = ctx->cfg.deposit_mode == P3M_DEPOSIT_I64;
     const size_t M = mesh_cells(ctx);
-    P3M_CUDA(ctx, cudaMemsetAsync(ctx->density, 0, M * (i64 ? 8 : 4), ctx->stream));
-    P3M_CUDA(ctx, p3m::launch_deposit(ctx->entries, ctx->sorted_keys, n, ctx->grid,
-                                      ctx->cfg.deposit_mode, (float)ctx->mass_scale, ctx->density,
-                                      ctx->stream));
+    {
+        StageScope scope(ctx, P3M_STAGE_DEPOSIT);
+        P3M_CUDA(ctx, cudaMemsetAsync(ctx->density, 0, M * (i64 ? 8 : 4), ctx->stream));
+        P3M_CUDA(ctx, p3m::launch_deposit(ctx->entries, ctx->sorted_keys, n, ctx->grid,
+                                          ctx->cfg.deposit_mode, (float)ctx->mass_scale,
+                                          ctx->density, ctx->stream));
+    }
     // fft_init.comp's uInverseMassScale = 1f / massScale (GravityPipeline.kt:942).
     const float inv_scale = i64 ? 1.0f / 4294967296.0f : 1.0f / (float)ctx->mass_scale;
-    P3M_CUDA(ctx, p3m::launch_fft_forward_rows(ctx->density, ctx->cfg.deposit_mode, inv_scale,
-                                               ctx->grid, ctx->twiddles, ctx->half, ctx->stream));
-    P3M_CUDA(ctx, p3m::launch_fft_columns(ctx->half, ctx->green, 1.0f / ctx->normalization_mass,
-                                          ctx->grid, ctx->twiddles, ctx->cols, ctx->stream));
-    P3M_CUDA(ctx, p3m::launch_fft_inverse_rows(ctx->cols, ctx->grid, ctx->twiddles, ctx->force,
-                                               ctx->stream));
+    {
+        StageScope scope(ctx, P3M_STAGE_FORWARD_FFT);
+        P3M_CUDA(ctx, p3m::launch_fft_forward_rows(ctx->density, ctx->cfg.deposit_mode, inv_scale,
+                                                   ctx->grid, ctx->twiddles, ctx->half,
+                                                   ctx->stream));
+    }
+    {
+        StageScope scope(ctx, P3M_STAGE_SPECTRAL);
+        P3M_CUDA(ctx, p3m::launch_fft_columns(ctx->half, ctx->green,
+                                              1.0f / ctx->normalization_mass, ctx->grid,
+                                              ctx->twiddles, ctx->cols, ctx->stream));
+    }
+    {
+        StageScope scope(ctx, P3M_STAGE_INVERSE_FFT);
+        P3M_CUDA(ctx, p3m::launch_fft_inverse_rows(ctx->cols, ctx->grid, ctx->twiddles,
+                                                   ctx->force, ctx->stream));
+    }
     return P3M_OK;
 }
 
@@ -231,6 +308,7 @@ int apply_kick(p3m_ctx* ctx, int n, int initial) {
     p.sigma_cells = ctx->cfg.softening_cells; p.total_mass = ctx->normalization_mass;
     p.min_frac = ctx->cfg.minimum_distance_cell_fraction; p.dt = ctx->cfg.time_step;
     p.field_x = ctx->field_x; p.field_y = ctx->field_y;
+    StageScope scope(ctx, P3M_STAGE_KICK);
     P3M_CUDA(ctx, p3m::launch_kick(ctx->bodies, ctx->accel, ctx->force, ctx->cell_start,
                                    ctx->cell_count, ctx->cell_mass, ctx->entries, p, ctx->stream));
     return P3M_OK;
@@ -239,6 +317,7 @@ int apply_kick(p3m_ctx* ctx, int n, int initial) {
 // GravityPipeline.kt:1269-1319 sortBodies.
 int sort_bodies(p3m_ctx* ctx, int n) {
     if (n <= 0) return P3M_OK;
+    StageScope scope(ctx, P3M_STAGE_SPATIAL_SORT);
     P3M_CUDA(ctx, p3m::launch_morton_keys(ctx->bodies, n, ctx->sort_wbits, ctx->sort_hbits,
                                           ctx->keys, ctx->vals, ctx->stream));
     uint32_t* sk = ctx->keys;
@@ -248,16 +327,27 @@ int sort_bodies(p3m_ctx* ctx, int n) {
     P3M_CUDA(ctx, p3m::launch_permute(sv, n, ctx->bodies, ctx->accel, ctx->materials,
                                       ctx->bodies_alt, ctx->accel_alt, ctx->materials_alt,
                                       ctx->destinations, ctx->stream));
+    // Slots beyond n (capacity reserved for bodies a caller adds later) keep
+    // their contents: carry them into the buffers that become current.
+    const size_t tail = (size_t)ctx->cfg.capacity - (size_t)n;
+    if (tail > 0) {
+        P3M_CUDA(ctx, cudaMemcpyAsync(ctx->bodies_alt + n, ctx->bodies + n, tail * sizeof(float4),
+                                      cudaMemcpyDeviceToDevice, ctx->stream));
+        P3M_CUDA(ctx, cudaMemcpyAsync(ctx->accel_alt + n, ctx->accel + n, tail * sizeof(float2),
+                                      cudaMemcpyDeviceToDevice, ctx->stream));
+        P3M_CUDA(ctx, cudaMemcpyAsync(ctx->materials_alt + n, ctx->materials + n,
+                                      tail * sizeof(float4), cudaMemcpyDeviceToDevice,
+                                      ctx->stream));
+    }
     std::swap(ctx->bodies, ctx->bodies_alt);
     std::swap(ctx->accel, ctx->accel_alt);
     std::swap(ctx->materials, ctx->materials_alt);
     return P3M_OK;
 }
 
-int one_step(p3m_ctx* ctx, int n) {
-    normalize_to(ctx, n);
-    const int interval = ctx->cfg.spatial_sort_interval;
-    if (interval > 0 && (ctx->physics_steps++ % interval) == 0) {
+// One gravity-only step (GravityPipeline.kt:445-494 without collisions).
+int enqueue_step(p3m_ctx* ctx, int n, bool do_sort) {
+    if (do_sort) {
         int st = sort_bodies(ctx, n);
         if (st != P3M_OK) return st;
     }
@@ -266,9 +356,12 @@ int one_step(p3m_ctx* ctx, int n) {
     // writes the home-cell keys.
     const float dt = ctx->cfg.time_step;
     const float drift_dt = dt / (float)ctx->cfg.drift_substeps;
-    P3M_CUDA(ctx, p3m::launch_drift(ctx->bodies, ctx->accel, n, 0.5f * dt, drift_dt,
-                                    ctx->cfg.drift_substeps, ctx->grid, ctx->keys, ctx->vals,
-                                    ctx->status, ctx->stream));
+    {
+        StageScope scope(ctx, P3M_STAGE_DRIFT);
+        P3M_CUDA(ctx, p3m::launch_drift(ctx->bodies, ctx->accel, n, 0.5f * dt, drift_dt,
+                                        ctx->cfg.drift_substeps, ctx->grid, ctx->keys, ctx->vals,
+                                        ctx->status, ctx->stream));
+    }
     if (ctx->mutual) {
         int st = lists_from_keys(ctx, n);
         if (st != P3M_OK) return st;
@@ -276,6 +369,87 @@ int one_step(p3m_ctx* ctx, int n) {
         if (st != P3M_OK) return st;
     }
     return apply_kick(ctx, n, 0);
+}
+
+void swap_body_buffers(p3m_ctx* ctx) {
+    std::swap(ctx->bodies, ctx->bodies_alt);
+    std::swap(ctx->accel, ctx->accel_alt);
+    std::swap(ctx->materials, ctx->materials_alt);
+}
+
+void drop_graphs(p3m_ctx* ctx) {
+    for (auto& g : ctx->graphs) cudaGraphExecDestroy(g.exec);
+    ctx->graphs.clear();
+}
+
+bool graph_matches(const p3m_step_graph& g, const p3m_ctx* ctx, int n, bool do_sort) {
+    return g.n == n && g.sort == do_sort && g.bodies == ctx->bodies && g.mutual == ctx->mutual &&
+           g.bounded == ctx->bounded && g.mass_scale == ctx->mass_scale &&
+           g.field_x == ctx->field_x && g.field_y == ctx->field_y &&
+           g.total_mass == ctx->normalization_mass;
+}
+
+int one_step(p3m_ctx* ctx, int n) {
+    normalize_to(ctx, n);
+    int st = ensure_green(ctx);
+    if (st != P3M_OK) return st;
+    const int interval = ctx->cfg.spatial_sort_interval;
+    const bool do_sort = interval > 0 && (ctx->physics_steps % interval) == 0;
+    if (interval > 0) ctx->physics_steps++;
+    if (!ctx->use_graphs || ctx->profiling || n == 0) return enqueue_step(ctx, n, do_sort);
+
+    for (const auto& g : ctx->graphs) {
+        if (!graph_matches(g, ctx, n, do_sort)) continue;
+        P3M_CUDA(ctx, cudaGraphLaunch(g.exec, ctx->stream));
+        p3m::count_launches((int)g.kernels);
+        if (do_sort) swap_body_buffers(ctx);
+        ctx->sorted_keys = g.sorted_keys;
+        ctx->sorted_ids = g.sorted_ids;
+        return P3M_OK;
+    }
+    // Capture the step once for this key, then launch it.
+    p3m_step_graph entry{};
+    entry.n = n;
+    entry.sort = do_sort;
+    entry.bodies = ctx->bodies;
+    entry.mutual = ctx->mutual;
+    entry.bounded = ctx->bounded;
+    entry.mass_scale = ctx->mass_scale;
+    entry.field_x = ctx->field_x;
+    entry.field_y = ctx->field_y;
+    entry.total_mass = ctx->normalization_mass;
+    float4* const saved[4] = {ctx->bodies, ctx->bodies_alt, ctx->materials, ctx->materials_alt};
+    float2* const saved_accel[2] = {ctx->accel, ctx->accel_alt};
+    const long long k0 = p3m_kernel_launches();
+    P3M_CUDA(ctx, cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+    st = enqueue_step(ctx, n, do_sort);
+    cudaGraph_t graph = nullptr;
+    cudaError_t e = cudaStreamEndCapture(ctx->stream, &graph);
+    if (st != P3M_OK || e != cudaSuccess) {
+        if (graph) cudaGraphDestroy(graph);
+        // Nothing ran: put the buffer roles back as they were.
+        ctx->bodies = saved[0];
+        ctx->bodies_alt = saved[1];
+        ctx->materials = saved[2];
+        ctx->materials_alt = saved[3];
+        ctx->accel = saved_accel[0];
+        ctx->accel_alt = saved_accel[1];
+        if (st != P3M_OK) return st;
+        return fail_cuda(ctx, "cudaStreamEndCapture", e);
+    }
+    entry.kernels = p3m_kernel_launches() - k0;
+    e = cudaGraphInstantiate(&entry.exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (e != cudaSuccess) return fail_cuda(ctx, "cudaGraphInstantiate", e);
+    entry.sorted_keys = ctx->sorted_keys;
+    entry.sorted_ids = ctx->sorted_ids;
+    if (ctx->graphs.size() >= 8) {
+        cudaGraphExecDestroy(ctx->graphs.front().exec);
+        ctx->graphs.erase(ctx->graphs.begin());
+    }
+    ctx->graphs.push_back(entry);
+    P3M_CUDA(ctx, cudaGraphLaunch(entry.exec, ctx->stream));
+    return P3M_OK;
 }
 
 size_t buffer_bytes(const p3m_ctx* ctx, int which, void** dptr) {
@@ -417,9 +591,12 @@ int p3m_create(const p3m_config* config, p3m_ctx** out) {
     ALLOC(ctx->force, M);
     ALLOC(ctx->green, HALF);
     ALLOC(ctx->twiddles, p3m::kTwiddleLength);
+    ALLOC(ctx->diag, (size_t)p3m::conservation_blocks() * 6 + 8);
 #undef ALLOC
 
     auto init = [&]() -> int {
+        P3M_CUDA(ctx, p3m::configure_deposit());
+        P3M_CUDA(ctx, p3m::configure_fft());
         std::vector<float2> tw(p3m::kTwiddleLength);
         p3m::host_twiddles(tw.data());
         P3M_CUDA(ctx, cudaMemcpyAsync(ctx->twiddles, tw.data(), tw.size() * sizeof(float2),
@@ -473,6 +650,22 @@ int p3m_upload_state(p3m_ctx* ctx, const float* bodies4, const float* materials4
     if (acceleration2)
         P3M_CUDA(ctx, cudaMemcpyAsync(ctx->accel, acceleration2, (size_t)n * 8, cudaMemcpyHostToDevice, ctx->stream));
     // Host arrays belong to the caller: finish reading them before returning.
+    P3M_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    return P3M_OK;
+}
+
+int p3m_upload_range(p3m_ctx* ctx, int32_t first, int32_t count, const float* bodies4,
+                     const float* materials4, const float* acceleration2) {
+    if (!ctx) return P3M_ERR_INVALID_ARGUMENT;
+    if (first < 0 || count < 0) return fail(ctx, P3M_ERR_INVALID_ARGUMENT, "range must be non-negative");
+    if ((long long)first + count > ctx->cfg.capacity)
+        return fail(ctx, P3M_ERR_CAPACITY, "range exceeds capacity");
+    if (bodies4)
+        P3M_CUDA(ctx, cudaMemcpyAsync(ctx->bodies + first, bodies4, (size_t)count * 16, cudaMemcpyHostToDevice, ctx->stream));
+    if (materials4)
+        P3M_CUDA(ctx, cudaMemcpyAsync(ctx->materials + first, materials4, (size_t)count * 16, cudaMemcpyHostToDevice, ctx->stream));
+    if (acceleration2)
+        P3M_CUDA(ctx, cudaMemcpyAsync(ctx->accel + first, acceleration2, (size_t)count * 8, cudaMemcpyHostToDevice, ctx->stream));
     P3M_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
     return P3M_OK;
 }
@@ -604,6 +797,118 @@ int p3m_apply_kick(p3m_ctx* ctx, int32_t n, int32_t initial) {
 
 int p3m_synchronize(p3m_ctx* ctx) {
     if (!ctx) return P3M_ERR_INVALID_ARGUMENT;
+    P3M_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    return P3M_OK;
+}
+
+int p3m_set_graphs(p3m_ctx* ctx, int32_t enabled) {
+    if (!ctx) return P3M_ERR_INVALID_ARGUMENT;
+    P3M_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    drop_graphs(ctx);
+    ctx->use_graphs = enabled != 0;
+    return P3M_OK;
+}
+
+int p3m_profile_enable(p3m_ctx* ctx, int32_t enabled) {
+    if (!ctx) return P3M_ERR_INVALID_ARGUMENT;
+    fold_stages(ctx);
+    if (enabled) {
+        for (int i = 0; i < P3M_STAGE_COUNT_; ++i) {
+            ctx->stage_ms[i] = 0.0;
+            ctx->stage_intervals[i] = 0;
+        }
+    }
+    ctx->profiling = enabled != 0;
+    return P3M_OK;
+}
+
+int p3m_profile_read(p3m_ctx* ctx, double* total_ms, int64_t* intervals) {
+    if (!ctx) return P3M_ERR_INVALID_ARGUMENT;
+    P3M_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    fold_stages(ctx);
+    for (int i = 0; i < P3M_STAGE_COUNT_; ++i) {
+        if (total_ms) total_ms[i] = ctx->stage_ms[i];
+        if (intervals) intervals[i] = ctx->stage_intervals[i];
+    }
+    return P3M_OK;
+}
+
+int64_t p3m_kernel_launches(void) { return p3m::g_launches.load(); }
+
+int p3m_get_stream(p3m_ctx* ctx, void** stream) {
+    if (!ctx || !stream) return P3M_ERR_INVALID_ARGUMENT;
+    *stream = (void*)ctx->stream;
+    return P3M_OK;
+}
+
+int p3m_host_alloc(size_t bytes, void** host) {
+    if (!host) return P3M_ERR_INVALID_ARGUMENT;
+    cudaError_t e = cudaHostAlloc(host, std::max<size_t>(bytes, 1), cudaHostAllocDefault);
+    if (e != cudaSuccess) {
+        *host = nullptr;
+        return fail_cuda(nullptr, "cudaHostAlloc", e);
+    }
+    return P3M_OK;
+}
+
+int p3m_host_free(void* host) {
+    if (!host) return P3M_OK;
+    cudaError_t e = cudaFreeHost(host);
+    return e == cudaSuccess ? P3M_OK : fail_cuda(nullptr, "cudaFreeHost", e);
+}
+
+int p3m_nonfinite_count(p3m_ctx* ctx, int64_t* count) {
+    if (!ctx || !count) return P3M_ERR_INVALID_ARGUMENT;
+    unsigned int v = 0;
+    P3M_CUDA(ctx, cudaMemcpyAsync(&v, ctx->status, sizeof(v), cudaMemcpyDeviceToHost, ctx->stream));
+    P3M_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    *count = (int64_t)v;
+    return P3M_OK;
+}
+
+int p3m_direct_accel_f64(p3m_ctx* ctx, int32_t n, const int32_t* targets, int32_t n_targets,
+                         double* out) {
+    int st = check_n(ctx, n);
+    if (st != P3M_OK) return st;
+    if (n_targets < 0 || (n_targets > 0 && (!targets || !out)))
+        return fail(ctx, P3M_ERR_INVALID_ARGUMENT, "targets/out missing");
+    for (int i = 0; i < n_targets; ++i)
+        if (targets[i] < 0 || targets[i] >= n) return fail(ctx, P3M_ERR_INVALID_ARGUMENT, "target ID out of range");
+    if (n_targets == 0) return P3M_OK;
+    normalize_to(ctx, n);
+    int* dt = nullptr;
+    double2* dout = nullptr;
+    P3M_CUDA(ctx, cudaMallocAsync((void**)&dt, (size_t)n_targets * sizeof(int), ctx->stream));
+    P3M_CUDA(ctx, cudaMallocAsync((void**)&dout, (size_t)n_targets * sizeof(double2), ctx->stream));
+    cudaError_t e = cudaMemcpyAsync(dt, targets, (size_t)n_targets * sizeof(int), cudaMemcpyHostToDevice, ctx->stream);
+    const double aspect = (double)ctx->cfg.viewport_width / (double)ctx->cfg.viewport_height;
+    const double cw = aspect / ctx->cfg.grid_width, ch = 1.0 / ctx->cfg.grid_height;
+    const double md = (double)ctx->cfg.minimum_distance_cell_fraction * std::min(cw, ch);
+    if (e == cudaSuccess)
+        e = p3m::launch_direct_accel(ctx->bodies, ctx->materials, n, dt, n_targets, aspect,
+                                     (double)ctx->cfg.gravitational_constant,
+                                     (double)ctx->normalization_mass, md * md, ctx->bounded, dout,
+                                     ctx->stream);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(out, dout, (size_t)n_targets * sizeof(double2), cudaMemcpyDeviceToHost, ctx->stream);
+    cudaFreeAsync(dt, ctx->stream);
+    cudaFreeAsync(dout, ctx->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    if (e != cudaSuccess) return fail_cuda(ctx, "p3m_direct_accel_f64", e);
+    return P3M_OK;
+}
+
+int p3m_diagnostics_f64(p3m_ctx* ctx, int32_t n, double* out6) {
+    int st = check_n(ctx, n);
+    if (st != P3M_OK) return st;
+    if (!out6) return fail(ctx, P3M_ERR_INVALID_ARGUMENT, "out is NULL");
+    double* partial = ctx->diag;
+    double* result = ctx->diag + (size_t)p3m::conservation_blocks() * 6;
+    P3M_CUDA(ctx, p3m::launch_conservation(ctx->bodies, ctx->materials, n,
+                                           (double)ctx->cfg.viewport_width,
+                                           (double)ctx->cfg.viewport_height, partial, result,
+                                           ctx->stream));
+    P3M_CUDA(ctx, cudaMemcpyAsync(out6, result, 6 * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
     P3M_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
     return P3M_OK;
 }

@@ -100,6 +100,15 @@ __global__ void __launch_bounds__(kDepositThreads) deposit_kernel(
 
 }  // namespace
 
+cudaError_t configure_deposit() {
+    cudaError_t e = cudaFuncSetAttribute(deposit_kernel<unsigned long long>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         kDepositWindowBytes);
+    if (e != cudaSuccess) return e;
+    return cudaFuncSetAttribute(deposit_kernel<uint32_t>,
+                                cudaFuncAttributeMaxDynamicSharedMemorySize, kDepositWindowBytes);
+}
+
 cudaError_t launch_deposit(const float4* entries, const uint32_t* keys, int n, GridShape g,
                            int deposit_mode, float mass_scale, void* density,
                            cudaStream_t stream) {
@@ -108,22 +117,15 @@ cudaError_t launch_deposit(const float4* entries, const uint32_t* keys, int n, G
     if (deposit_mode == P3M_DEPOSIT_I64) {
         using T = unsigned long long;
         const int cap = kDepositWindowBytes / (int)sizeof(T);
-        cudaError_t e = cudaFuncSetAttribute(deposit_kernel<T>,
-                                             cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             kDepositWindowBytes);
-        if (e != cudaSuccess) return e;
         deposit_kernel<T><<<blocks, kDepositThreads, kDepositWindowBytes, stream>>>(
             entries, keys, n, g.W, g.H, g.MW, g.MH, 4294967296.0f, static_cast<T*>(density), cap);
     } else {
         using T = uint32_t;
         const int cap = kDepositWindowBytes / (int)sizeof(T);
-        cudaError_t e = cudaFuncSetAttribute(deposit_kernel<T>,
-                                             cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             kDepositWindowBytes);
-        if (e != cudaSuccess) return e;
         deposit_kernel<T><<<blocks, kDepositThreads, kDepositWindowBytes, stream>>>(
             entries, keys, n, g.W, g.H, g.MW, g.MH, mass_scale, static_cast<T*>(density), cap);
     }
+    count_launches(1);
     return cudaGetLastError();
 }
 

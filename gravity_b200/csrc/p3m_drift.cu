@@ -1,0 +1,67 @@
+// p3m_drift.cu — the leapfrog drift of the gravity step.
+//
+// Built with --fmad=false: every multiply and add rounds on its own, as in
+// the oracle, so positions and the cell keys derived from them are
+// bit-identical to it for the same accelerations.
+//
+// drift: collision_build.comp:40-51 (gravity-only, so only the half kick,
+//   drift and wall clamp / torus wrap of each collision substep), all S
+//   substeps in registers, then the home-cell key of the cell sort.
+
+#include "p3m_internal.cuh"
+
+namespace p3m {
+namespace {
+
+__device__ __forceinline__ float fractf(float v) { return v - floorf(v); }
+
+__global__ void drift_kernel(float4* __restrict__ bodies, const float2* __restrict__ accel, int n,
+                             float half_kick, float drift_dt, int substeps, int bounded, int W,
+                             int H, uint32_t* __restrict__ keys, uint32_t* __restrict__ vals,
+                             unsigned int* __restrict__ nonfinite) {
+    const int id = blockIdx.x * blockDim.x + threadIdx.x;
+    if (id >= n) return;
+    float4 b = bodies[id];
+    const float2 a = accel[id];
+    for (int s = 0; s < substeps; ++s) {
+        // Substeps after the first carry kickDt = 0 (GravityPipeline.kt:465-473),
+        // whose kick adds a * 0.
+        const float hk = s == 0 ? half_kick : 0.0f;
+        b.z = b.z + a.x * hk;
+        b.w = b.w + a.y * hk;
+        b.x = b.x + b.z * drift_dt;
+        b.y = b.y + b.w * drift_dt;
+        if (bounded) {
+            b.x = fminf(fmaxf(b.x, 0.0f), kMaximumUnit);
+            b.y = fminf(fmaxf(b.y, 0.0f), kMaximumUnit);
+        } else {
+            b.x = fractf(b.x);
+            b.y = fractf(b.y);
+        }
+    }
+    bodies[id] = b;
+    if (nonfinite && !(isfinite(b.x) && isfinite(b.y) && isfinite(b.z) && isfinite(b.w)))
+        atomicAdd(nonfinite, 1u);
+    if (keys) {
+        const int hx = wrap_index(float_to_int(floorf(b.x * (float)W)), W);
+        const int hy = wrap_index(float_to_int(floorf(b.y * (float)H)), H);
+        const int slot = n - 1 - id;  // descending ID order for the cell sort
+        keys[slot] = (uint32_t)hx + (uint32_t)hy * (uint32_t)W;
+        vals[slot] = (uint32_t)id;
+    }
+}
+
+}  // namespace
+
+cudaError_t launch_drift(float4* bodies, const float2* accel, int n, float half_kick, float drift_dt,
+                         int substeps, GridShape g, uint32_t* keys, uint32_t* vals,
+                         unsigned int* nonfinite, cudaStream_t stream) {
+    if (n <= 0) return cudaSuccess;
+    drift_kernel<<<(n + 255) / 256, 256, 0, stream>>>(bodies, accel, n, half_kick, drift_dt,
+                                                      substeps, g.bounded, g.W, g.H, keys, vals,
+                                                      nonfinite);
+    count_launches(1);
+    return cudaGetLastError();
+}
+
+}  // namespace p3m

@@ -356,19 +356,43 @@ cudaError_t set_smem(const void* fn, size_t bytes) {
     return cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
 }
 
-// Columns per CTA of the column kernels: enough CTAs to fill the GPU, at most
-// 16 and at most what 128 KB of shared memory holds.
-int column_group(int MW, int MH, int lines_factor) {
-    const int SW = MW / 2 + 1;
-    int g = SW / 296;
-    const int cap = (128 * 1024) / (lines_factor * MH * (int)sizeof(float2));
+// Lines per CTA: enough CTAs for two per SM (296) when there are that many
+// lines, at most `cap`; threads: one radix-8 butterfly per thread and pass,
+// 64..256.
+void line_shape(int lines_total, int L, int cap, int* per_cta, int* threads) {
+    int g = lines_total / 296;
     if (g > cap) g = cap;
-    if (g > 16) g = 16;
     if (g < 1) g = 1;
-    return g;
+    *per_cta = g;
+    int t = ((g * L / 8) + 31) / 32 * 32;
+    *threads = t < 64 ? 64 : (t > 256 ? 256 : t);
+}
+
+// Columns per CTA of the column kernels: at most 16 and at most what 128 KB
+// of shared memory holds.
+void column_shape(int MW, int MH, int lines_factor, int* G, int* threads) {
+    const int SW = MW / 2 + 1;
+    int cap = (128 * 1024) / (lines_factor * MH * (int)sizeof(float2));
+    if (cap > 16) cap = 16;
+    line_shape(SW, MH, cap, G, threads);
 }
 
 }  // namespace
+
+// Dynamic shared memory opt-in (above 48 KB) of every FFT kernel, once per
+// device at context creation (never inside a stream capture).
+cudaError_t configure_fft() {
+    const size_t big = 200 * 1024;
+    const void* fns[] = {(const void*)fft_rows_forward_kernel<long long>,
+                         (const void*)fft_rows_forward_kernel<uint32_t>,
+                         (const void*)fft_columns_kernel, (const void*)fft_columns_forward_kernel,
+                         (const void*)fft_rows_inverse_kernel, (const void*)fft64_line_kernel};
+    for (const void* f : fns) {
+        cudaError_t e = set_smem(f, big);
+        if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
+}
 
 void host_twiddles(float2* out) {
     for (int m = 0; m < kTwiddleLength; ++m) {
@@ -380,62 +404,59 @@ void host_twiddles(float2* out) {
 cudaError_t launch_fft_forward_rows(const void* density, int deposit_mode, float inv_scale,
                                     GridShape g, const float2* twiddles, float2* half,
                                     cudaStream_t stream) {
-    const int pairs_per_cta = g.MW >= 4096 ? 1 : 4096 / g.MW;
     const int pairs = g.MH / 2;
+    int pairs_per_cta, threads;
+    line_shape(pairs, g.MW, g.MW >= 4096 ? 1 : 4096 / g.MW, &pairs_per_cta, &threads);
     const int blocks = (pairs + pairs_per_cta - 1) / pairs_per_cta;
     const size_t smem = (size_t)2 * pairs_per_cta * g.MW * sizeof(float2);
-    cudaError_t e;
     if (deposit_mode == P3M_DEPOSIT_I64) {
-        e = set_smem((const void*)fft_rows_forward_kernel<long long>, smem);
-        if (e != cudaSuccess) return e;
-        fft_rows_forward_kernel<long long><<<blocks, 256, smem, stream>>>(
+        fft_rows_forward_kernel<long long><<<blocks, threads, smem, stream>>>(
             static_cast<const long long*>(density), inv_scale, g.MW, g.MH, pairs_per_cta, twiddles,
             half);
     } else {
-        e = set_smem((const void*)fft_rows_forward_kernel<uint32_t>, smem);
-        if (e != cudaSuccess) return e;
-        fft_rows_forward_kernel<uint32_t><<<blocks, 256, smem, stream>>>(
+        fft_rows_forward_kernel<uint32_t><<<blocks, threads, smem, stream>>>(
             static_cast<const uint32_t*>(density), inv_scale, g.MW, g.MH, pairs_per_cta, twiddles,
             half);
     }
+    count_launches(1);
     return cudaGetLastError();
 }
 
 cudaError_t launch_fft_columns(const float2* half, const float2* green, float inv_total,
                                GridShape g, const float2* twiddles, float4* cols,
                                cudaStream_t stream) {
-    const int G = column_group(g.MW, g.MH, 4);
+    int G, threads;
+    column_shape(g.MW, g.MH, 4, &G, &threads);
     const int SW = g.MW / 2 + 1;
     const int blocks = (SW + G - 1) / G;
     const size_t smem = (size_t)4 * G * g.MH * sizeof(float2);
-    cudaError_t e = set_smem((const void*)fft_columns_kernel, smem);
-    if (e != cudaSuccess) return e;
-    fft_columns_kernel<<<blocks, 256, smem, stream>>>(half, green, inv_total, g.MW, g.MH, G,
+    fft_columns_kernel<<<blocks, threads, smem, stream>>>(half, green, inv_total, g.MW, g.MH, G,
                                                       twiddles, cols);
+    count_launches(1);
     return cudaGetLastError();
 }
 
 cudaError_t launch_fft_forward_columns(float2* half, GridShape g, const float2* twiddles,
                                        cudaStream_t stream) {
-    const int G = column_group(g.MW, g.MH, 2);
+    int G, threads;
+    column_shape(g.MW, g.MH, 2, &G, &threads);
     const int SW = g.MW / 2 + 1;
     const int blocks = (SW + G - 1) / G;
     const size_t smem = (size_t)2 * G * g.MH * sizeof(float2);
-    cudaError_t e = set_smem((const void*)fft_columns_forward_kernel, smem);
-    if (e != cudaSuccess) return e;
-    fft_columns_forward_kernel<<<blocks, 256, smem, stream>>>(half, g.MW, g.MH, G, twiddles);
+    fft_columns_forward_kernel<<<blocks, threads, smem, stream>>>(half, g.MW, g.MH, G, twiddles);
+    count_launches(1);
     return cudaGetLastError();
 }
 
 cudaError_t launch_fft_inverse_rows(const float4* cols, GridShape g, const float2* twiddles,
                                     float2* force, cudaStream_t stream) {
-    const int rows_per_cta = g.MW >= 4096 ? 1 : 4096 / g.MW;
+    int rows_per_cta, threads;
+    line_shape(g.MH, g.MW, g.MW >= 4096 ? 1 : 4096 / g.MW, &rows_per_cta, &threads);
     const int blocks = (g.MH + rows_per_cta - 1) / rows_per_cta;
     const size_t smem = (size_t)2 * rows_per_cta * g.MW * sizeof(float2);
-    cudaError_t e = set_smem((const void*)fft_rows_inverse_kernel, smem);
-    if (e != cudaSuccess) return e;
-    fft_rows_inverse_kernel<<<blocks, 256, smem, stream>>>(cols, g.MW, g.MH, rows_per_cta,
+    fft_rows_inverse_kernel<<<blocks, threads, smem, stream>>>(cols, g.MW, g.MH, rows_per_cta,
                                                            twiddles, force);
+    count_launches(1);
     return cudaGetLastError();
 }
 
@@ -444,15 +465,13 @@ cudaError_t build_green(GridShape g, GreenParams p, double2* work, float2* green
     const long long M = (long long)g.MW * g.MH;
     green_real_kernel<<<(int)((M + 255) / 256), 256, 0, stream>>>(
         work, g.MW, g.MH, g.W, g.H, (double)p.aspect, (double)p.gravity, (double)p.sigma_cells);
-    cudaError_t e = set_smem((const void*)fft64_line_kernel,
-                             (size_t)std::max(g.MW, g.MH) * sizeof(double2));
-    if (e != cudaSuccess) return e;
     fft64_line_kernel<<<g.MH, 256, (size_t)g.MW * sizeof(double2), stream>>>(work, g.MW, g.MH, 0);
     fft64_line_kernel<<<g.MW, 256, (size_t)g.MH * sizeof(double2), stream>>>(work, g.MW, g.MH, 1);
     const long long SWH = (long long)(g.MW / 2 + 1) * g.MH;
     green_final_kernel<<<(int)((SWH + 255) / 256), 256, 0, stream>>>(
         work, g.MW, g.MH, (double)p.window_floor, green);
     (void)ilog2_host;
+    count_launches(4);
     return cudaGetLastError();
 }
 

@@ -151,10 +151,49 @@ cudaError_t launch_kick(float4* bodies, float2* accel, const float2* force, cons
                         const int* cell_count, const uint32_t* cell_mass, const float4* entries,
                         KickParams p, cudaStream_t stream);
 
+// Shared-memory opt-ins, once per device (p3m_create), never during capture.
+cudaError_t configure_deposit();
+cudaError_t configure_fft();
+
 // Host-side twiddle table: e^{-2 pi i m / 4096}, computed in double.
 void host_twiddles(float2* out);
 
+// FP64 diagnostics (p3m_diag.cu).
+cudaError_t launch_direct_accel(const float4* bodies, const float4* materials, int n,
+                                const int* targets, int n_targets, double aspect, double gravity,
+                                double total_mass, double min_dist2, int bounded, double2* out,
+                                cudaStream_t stream);
+int conservation_blocks();
+cudaError_t launch_conservation(const float4* bodies, const float4* materials, int n, double w,
+                                double h, double* partial, double* out, cudaStream_t stream);
+
+// Process-wide count of kernels launched by this library (p3m_kernel_launches).
+void count_launches(int kernels);
+
 }  // namespace p3m
+
+#include <vector>
+
+// Stage timing: CUDA event pairs recorded on the context's stream.
+struct p3m_stage_events {
+    int stage;
+    cudaEvent_t start, stop;
+};
+
+// One captured step. Everything a replay bakes in is part of the key: the
+// body count, whether the step starts with a Morton reorder, which of the
+// ping-pong body buffers is current, and the scalar uniforms.
+struct p3m_step_graph {
+    int n;
+    bool sort;
+    const void* bodies;
+    int mutual, bounded, mass_scale;
+    float field_x, field_y, total_mass;
+    cudaGraphExec_t exec;
+    long long kernels;
+    uint32_t* sorted_keys;
+    uint32_t* sorted_ids;
+};
 
 // ------------------------------------------------------------------ context
 struct p3m_ctx {
@@ -204,6 +243,20 @@ struct p3m_ctx {
     float2* green = nullptr;
     float2* twiddles = nullptr;
     size_t mesh_capacity = 0;  // cells the mesh buffers hold
+
+    // diagnostics scratch
+    double* diag = nullptr;  // conservation partials + result
+
+    // captured steps (CUDA graphs)
+    bool use_graphs = true;
+    std::vector<p3m_step_graph> graphs;
+
+    // stage profiler
+    bool profiling = false;
+    std::vector<p3m_stage_events> pending;  // recorded, not yet folded
+    std::vector<cudaEvent_t> free_events;
+    double stage_ms[P3M_STAGE_COUNT_] = {};
+    long long stage_intervals[P3M_STAGE_COUNT_] = {};
 
     std::string last_error;
 };

@@ -1,80 +1,53 @@
-// p3m_kick.cu — leapfrog drift and the interpolation + short-range + kick.
+// p3m_kick.cu — CIC force interpolation + short-range correction + half kick.
 //
-// Built with --fmad=false: every multiply and add rounds on its own, as in
-// the oracle, so positions, keys and deposit weights derived from them are
-// bit-identical to it.
+// Restates kick.comp:66-156: the mesh force is interpolated at the body with
+// the CIC weights (kick.comp:82-103), the uniform field is added, and the
+// short-range complement of the Gaussian split is summed over the
+// (2Rx+1)x(2Ry+1) cell stencil around the home cell (kick.comp:122-151):
+// cells holding more than `exact` bodies act as a monopole at the cell centre
+// with the fixed-point cell mass; other cells, and the home cell up to
+// `home_limit` list entries, are summed body by body in list order (the cell
+// lists run in descending ID). Then v += a * dt/2 unless initial, and a is
+// stored.
 //
-// drift: collision_build.comp:40-51 (gravity-only, so only the half kick,
-//   drift and wall clamp / torus wrap of each collision substep), all S
-//   substeps in registers, then the home-cell key of the cell sort.
-// kick:  kick.comp:66-156 — CIC interpolation of the mesh force, uniform
-//   field, and the short-range correction over the (2Rx+1)x(2Ry+1) cell
-//   stencil: exact pairs for cells with at most `exact` bodies (the home cell
-//   walks at most `home_limit` list entries), a cell monopole otherwise; then
-//   v += a * dt/2 unless initial, and a is stored.
+// The pair term G m exp(-r^2/2s^2) d / (M max(r^2, r_min^2)) is evaluated as
+// (G/M) m exp2(-r^2 log2(e)/2s^2) * rcp(max(r^2, r_min^2)) * d: the same
+// expression with fused multiply-adds, the hardware exp2 and a reciprocal
+// instead of three IEEE divisions. Forces agree with the oracle's literal
+// FP32 evaluation to ~1e-7 relative per term; the contract is 1e-5 relative
+// RMS.
+//
+// One thread per body in ID order: after the Morton reorder, IDs follow
+// screen tiles, so the stencils of a warp overlap and the cell tables and
+// neighbour entries are served from L1/L2.
 
 #include "p3m_internal.cuh"
 
 namespace p3m {
 namespace {
 
-__device__ __forceinline__ float fractf(float v) { return v - floorf(v); }
-
-__global__ void drift_kernel(float4* __restrict__ bodies, const float2* __restrict__ accel, int n,
-                             float half_kick, float drift_dt, int substeps, int bounded, int W,
-                             int H, uint32_t* __restrict__ keys, uint32_t* __restrict__ vals,
-                             unsigned int* __restrict__ nonfinite) {
-    const int id = blockIdx.x * blockDim.x + threadIdx.x;
-    if (id >= n) return;
-    float4 b = bodies[id];
-    const float2 a = accel[id];
-    for (int s = 0; s < substeps; ++s) {
-        // Substeps after the first carry kickDt = 0 (GravityPipeline.kt:465-473),
-        // whose kick adds a * 0.
-        const float hk = s == 0 ? half_kick : 0.0f;
-        b.z = b.z + a.x * hk;
-        b.w = b.w + a.y * hk;
-        b.x = b.x + b.z * drift_dt;
-        b.y = b.y + b.w * drift_dt;
-        if (bounded) {
-            b.x = fminf(fmaxf(b.x, 0.0f), kMaximumUnit);
-            b.y = fminf(fmaxf(b.y, 0.0f), kMaximumUnit);
-        } else {
-            b.x = fractf(b.x);
-            b.y = fractf(b.y);
-        }
-    }
-    bodies[id] = b;
-    if (nonfinite && !(isfinite(b.x) && isfinite(b.y) && isfinite(b.z) && isfinite(b.w)))
-        atomicAdd(nonfinite, 1u);
-    if (keys) {
-        const int hx = wrap_index(float_to_int(floorf(b.x * (float)W)), W);
-        const int hy = wrap_index(float_to_int(floorf(b.y * (float)H)), H);
-        const int slot = n - 1 - id;  // descending ID order for the cell sort
-        keys[slot] = (uint32_t)hx + (uint32_t)hy * (uint32_t)W;
-        vals[slot] = (uint32_t)id;
-    }
-}
-
 struct KickConst {
-    float sigma2x2;     // 2 sigma^2
-    float min_dist2;    // (min_frac * min(cell w, cell h))^2
+    float neg_log2e_over_2s2;  // -log2(e) / (2 sigma^2)
+    float min_dist2;           // (min_frac * min(cell w, cell h))^2
+    float g_over_m;            // G / M_tot
+    float inv_w, inv_h;
 };
 
-// kick.comp:66-80 localAcceleration.
-__device__ __forceinline__ float2 local_acceleration(const KickParams& p, const KickConst& k,
-                                                     float sx, float sy, float tx, float ty,
-                                                     float m) {
+__device__ __forceinline__ void pair_term(const KickParams& p, const KickConst& k, float sx,
+                                          float sy, float tx, float ty, float m, float& ax,
+                                          float& ay) {
     float dx = sx - tx, dy = sy - ty;
     if (p.bounded == 0) {
         dx -= floorf(dx + 0.5f);
         dy -= floorf(dy + 0.5f);
     }
-    const float px = dx * p.aspect, py = dy;
-    const float r2 = px * px + py * py;
-    const float w = expf(-r2 / k.sigma2x2);
-    const float phys = p.gravity * m * w / (p.total_mass * fmaxf(r2, k.min_dist2));
-    return make_float2(phys * px / p.aspect, phys * py);
+    const float px = dx * p.aspect;
+    const float r2 = fmaf(px, px, dy * dy);
+    const float w = exp2f(r2 * k.neg_log2e_over_2s2);
+    const float phys = __fdividef(k.g_over_m * m * w, fmaxf(r2, k.min_dist2));
+    // (phys * px) / aspect == phys * dx
+    ax = fmaf(phys, dx, ax);
+    ay = fmaf(phys, dy, ay);
 }
 
 __global__ void __launch_bounds__(256) kick_kernel(
@@ -85,9 +58,11 @@ __global__ void __launch_bounds__(256) kick_kernel(
     if (id >= p.n) return;
     float4 b = bodies[id];
     if (p.mutual == 0) {
+        // Field only: the same separately rounded multiply and add as the
+        // oracle (this file otherwise allows contraction).
         if (p.initial == 0) {
-            b.z = b.z + p.field_x * (0.5f * p.dt);
-            b.w = b.w + p.field_y * (0.5f * p.dt);
+            b.z = __fadd_rn(b.z, __fmul_rn(p.field_x, 0.5f * p.dt));
+            b.w = __fadd_rn(b.w, __fmul_rn(p.field_y, 0.5f * p.dt));
         }
         accel[id] = make_float2(p.field_x, p.field_y);
         bodies[id] = b;
@@ -96,10 +71,13 @@ __global__ void __launch_bounds__(256) kick_kernel(
     KickConst k;
     {
         const float sigma = p.sigma_cells / (float)p.H;
-        k.sigma2x2 = 2.0f * sigma * sigma;
+        k.neg_log2e_over_2s2 = -1.4426950408889634f / (2.0f * sigma * sigma);
         const float cw = p.aspect / (float)p.W, ch = 1.0f / (float)p.H;
         const float md = p.min_frac * fminf(cw, ch);
         k.min_dist2 = md * md;
+        k.g_over_m = p.gravity / p.total_mass;
+        k.inv_w = 1.0f / (float)p.W;
+        k.inv_h = 1.0f / (float)p.H;
     }
     // kick.comp:82-103 interpolateForce.
     float rx, ry;
@@ -118,11 +96,9 @@ __global__ void __launch_bounds__(256) kick_kernel(
         const float ay = v00.y * (1.0f - tx) + v10.y * tx;
         const float bx2 = v01.x * (1.0f - tx) + v11.x * tx;
         const float by2 = v01.y * (1.0f - tx) + v11.y * tx;
-        rx = ax * (1.0f - ty) + bx2 * ty;
-        ry = ay * (1.0f - ty) + by2 * ty;
+        rx = ax * (1.0f - ty) + bx2 * ty + p.field_x;
+        ry = ay * (1.0f - ty) + by2 * ty + p.field_y;
     }
-    rx = rx + p.field_x;
-    ry = ry + p.field_y;
 
     const int hx = guard_coord(float_to_int(floorf(b.x * (float)p.W)), p.W);
     const int hy = guard_coord(float_to_int(floorf(b.y * (float)p.H)), p.H);
@@ -130,39 +106,35 @@ __global__ void __launch_bounds__(256) kick_kernel(
         const int cy = hy + dy;
         if (p.bounded && (cy < 0 || cy >= p.H)) continue;
         const int wy = wrap_index(cy, p.H);
+        const int row = wy * p.W;
+        const float cyf = ((float)wy + 0.5f) * k.inv_h;
         for (int dx = -p.rx; dx <= p.rx; ++dx) {
             const int cx = hx + dx;
             if (p.bounded && (cx < 0 || cx >= p.W)) continue;
             const int wx = wrap_index(cx, p.W);
-            const int index = wx + wy * p.W;
+            const int index = wx + row;
             const int count = __ldg(&cell_count[index]);
             if (count == 0) continue;
             const bool home = dx == 0 && dy == 0;
             if (!home && count > p.exact) {
-                const float cxf = ((float)wx + 0.5f) / (float)p.W;
-                const float cyf = ((float)wy + 0.5f) / (float)p.H;
-                const float agg = (float)__ldg(&cell_mass[index]) / kCellMassUnits;
-                const float2 a = local_acceleration(p, k, cxf, cyf, b.x, b.y, agg);
-                rx = rx + a.x;
-                ry = ry + a.y;
+                const float cxf = ((float)wx + 0.5f) * k.inv_w;
+                const float agg = (float)__ldg(&cell_mass[index]) * (1.0f / kCellMassUnits);
+                pair_term(p, k, cxf, cyf, b.x, b.y, agg, rx, ry);
             } else {
                 const int limit = home ? p.home_limit : p.exact;
                 const int walk = count < limit ? count : limit;
                 const int start = __ldg(&cell_start[index]);
                 for (int e = 0; e < walk; ++e) {
                     const float4 o = __ldg(&entries[start + e]);
-                    if (__float_as_uint(o.w) != (uint32_t)id) {
-                        const float2 a = local_acceleration(p, k, o.x, o.y, b.x, b.y, o.z);
-                        rx = rx + a.x;
-                        ry = ry + a.y;
-                    }
+                    if (__float_as_uint(o.w) != (uint32_t)id)
+                        pair_term(p, k, o.x, o.y, b.x, b.y, o.z, rx, ry);
                 }
             }
         }
     }
     if (p.initial == 0) {
-        b.z = b.z + rx * (0.5f * p.dt);
-        b.w = b.w + ry * (0.5f * p.dt);
+        b.z = __fadd_rn(b.z, __fmul_rn(rx, 0.5f * p.dt));
+        b.w = __fadd_rn(b.w, __fmul_rn(ry, 0.5f * p.dt));
     }
     accel[id] = make_float2(rx, ry);
     bodies[id] = b;
@@ -170,22 +142,13 @@ __global__ void __launch_bounds__(256) kick_kernel(
 
 }  // namespace
 
-cudaError_t launch_drift(float4* bodies, const float2* accel, int n, float half_kick, float drift_dt,
-                         int substeps, GridShape g, uint32_t* keys, uint32_t* vals,
-                         unsigned int* nonfinite, cudaStream_t stream) {
-    if (n <= 0) return cudaSuccess;
-    drift_kernel<<<(n + 255) / 256, 256, 0, stream>>>(bodies, accel, n, half_kick, drift_dt,
-                                                      substeps, g.bounded, g.W, g.H, keys, vals,
-                                                      nonfinite);
-    return cudaGetLastError();
-}
-
 cudaError_t launch_kick(float4* bodies, float2* accel, const float2* force, const int* cell_start,
                         const int* cell_count, const uint32_t* cell_mass, const float4* entries,
                         KickParams p, cudaStream_t stream) {
     if (p.n <= 0) return cudaSuccess;
     kick_kernel<<<(p.n + 255) / 256, 256, 0, stream>>>(bodies, accel, force, cell_start,
                                                        cell_count, cell_mass, entries, p);
+    count_launches(1);
     return cudaGetLastError();
 }
 

@@ -64,7 +64,7 @@ __device__ uint32_t block_exclusive_scan(uint32_t v, uint32_t* warp_tot, uint32_
 
 // ----------------------------------------------------------------- scan
 constexpr int kScanThreads = 1024;
-constexpr int kScanItems = 4;
+constexpr int kScanItems = 8;
 constexpr int kScanBlock = kScanThreads * kScanItems;
 
 __global__ void __launch_bounds__(kScanThreads) scan_local_kernel(uint32_t* data, int n,
@@ -358,12 +358,14 @@ cudaError_t exclusive_scan_u32(uint32_t* data, int n, uint32_t* block_sums, cuda
     const int blocks = blocks_for(n, kScanBlock);
     if (blocks == 1) {
         scan_local_kernel<<<1, kScanThreads, 0, stream>>>(data, n, nullptr);
+        count_launches(1);
         return cudaGetLastError();
     }
     if (blocks > kScanBlock) return cudaErrorInvalidValue;
     scan_local_kernel<<<blocks, kScanThreads, 0, stream>>>(data, n, block_sums);
     scan_local_kernel<<<1, kScanThreads, 0, stream>>>(block_sums, blocks, nullptr);
     scan_add_kernel<<<blocks, kScanThreads, 0, stream>>>(data, n, block_sums);
+    count_launches(3);
     return cudaGetLastError();
 }
 
@@ -389,6 +391,7 @@ cudaError_t radix_sort_pairs(uint32_t* keys, uint32_t* vals, const SortScratch& 
         if (e != cudaSuccess) return e;
         radix_scatter_kernel<<<tiles, kSortThreads, 0, stream>>>(kin, vin, kout, vout, n, shift,
                                                                  pbits, tiles, s.hist);
+        count_launches(2);
         uint32_t* tk = kin; kin = kout; kout = tk;
         uint32_t* tv = vin; vin = vout; vout = tv;
     }
@@ -401,6 +404,7 @@ cudaError_t launch_cell_keys(const float4* bodies, int n, GridShape g, uint32_t*
                              uint32_t* vals, cudaStream_t stream) {
     if (n <= 0) return cudaSuccess;
     cell_keys_kernel<<<blocks_for(n, 256), 256, 0, stream>>>(bodies, n, g.W, g.H, keys, vals);
+    count_launches(1);
     return cudaGetLastError();
 }
 
@@ -408,6 +412,7 @@ cudaError_t launch_morton_keys(const float4* bodies, int n, int wbits, int hbits
                                uint32_t* vals, cudaStream_t stream) {
     if (n <= 0) return cudaSuccess;
     morton_keys_kernel<<<blocks_for(n, 256), 256, 0, stream>>>(bodies, n, wbits, hbits, keys, vals);
+    count_launches(1);
     return cudaGetLastError();
 }
 
@@ -418,6 +423,7 @@ cudaError_t launch_permute(const uint32_t* order, int n, const float4* bodies, c
     permute_kernel<<<blocks_for(n, 256), 256, 0, stream>>>(order, n, bodies, accel, materials,
                                                            bodies_out, accel_out, materials_out,
                                                            destinations);
+    count_launches(1);
     return cudaGetLastError();
 }
 
@@ -428,6 +434,7 @@ cudaError_t launch_cell_build(const uint32_t* keys, const uint32_t* ids, int n, 
     cell_build_kernel<<<blocks_for(n, 256), 256, 0, stream>>>(keys, ids, n, bodies, materials,
                                                               cell_start, cell_count, cell_mass,
                                                               entries);
+    count_launches(1);
     return cudaGetLastError();
 }
 

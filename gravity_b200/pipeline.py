@@ -138,6 +138,16 @@ class GravityPipeline:
         a = None if acceleration is None else np.ascontiguousarray(acceleration, dtype=np.float32).reshape(n, 2)
         self._check(self._lib.p3m_upload_state(self._ctx, _ptr(b), _ptr(m), _ptr(a), n))
 
+    def upload_range(self, first: int, bodies: np.ndarray, materials: np.ndarray | None = None,
+                     acceleration: np.ndarray | None = None) -> None:
+        """Write bodies into slots [first, first + len) (spawnProjectile's
+        glBufferSubData at an offset, GravityPipeline.kt:621-718)."""
+        b = np.ascontiguousarray(bodies, dtype=np.float32).reshape(-1, 4)
+        k = b.shape[0]
+        m = None if materials is None else np.ascontiguousarray(materials, dtype=np.float32).reshape(k, 4)
+        a = None if acceleration is None else np.ascontiguousarray(acceleration, dtype=np.float32).reshape(k, 2)
+        self._check(self._lib.p3m_upload_range(self._ctx, first, k, _ptr(b), _ptr(m), _ptr(a)))
+
     def download(self, n: int):
         """(bodies (n,4), materials (n,4), acceleration (n,2)) as float32."""
         b = np.empty((n, 4), np.float32)
@@ -145,6 +155,26 @@ class GravityPipeline:
         a = np.empty((n, 2), np.float32)
         self._check(self._lib.p3m_download_state(self._ctx, _ptr(b), _ptr(m), _ptr(a), n))
         return b, m, a
+
+    def download_into(self, n: int, bodies: np.ndarray | None = None,
+                      materials: np.ndarray | None = None,
+                      acceleration: np.ndarray | None = None) -> None:
+        """Read state into caller-owned (e.g. page-locked) float32 arrays."""
+        for a, w in ((bodies, 4), (materials, 4), (acceleration, 2)):
+            if a is not None and (a.dtype != np.float32 or a.size < n * w or not a.flags.c_contiguous):
+                raise ValueError("output arrays must be contiguous float32 with room for n rows")
+        self._check(self._lib.p3m_download_state(self._ctx, _ptr(bodies), _ptr(materials),
+                                                  _ptr(acceleration), n))
+
+    def upload_n(self, n: int, bodies: np.ndarray | None = None,
+                 materials: np.ndarray | None = None,
+                 acceleration: np.ndarray | None = None) -> None:
+        """Upload the first n rows of caller-owned float32 arrays as they are."""
+        for a, w in ((bodies, 4), (materials, 4), (acceleration, 2)):
+            if a is not None and (a.dtype != np.float32 or a.size < n * w or not a.flags.c_contiguous):
+                raise ValueError("input arrays must be contiguous float32 with n rows")
+        self._check(self._lib.p3m_upload_state(self._ctx, _ptr(bodies), _ptr(materials),
+                                                _ptr(acceleration), n))
 
     def bodies(self, n: int) -> np.ndarray:
         return self.download(n)[0]
@@ -182,6 +212,40 @@ class GravityPipeline:
     def build_cell_lists(self, active_bodies: int) -> None:
         self._check(self._lib.p3m_build_cell_lists(self._ctx, active_bodies))
 
+    # -------------------------------------------------- profiling, diagnostics
+    def profile_enable(self, enabled: bool = True) -> None:
+        self._check(self._lib.p3m_profile_enable(self._ctx, 1 if enabled else 0))
+
+    def profile_read(self) -> dict:
+        """{stage: (total device ms, intervals)} since profiling was enabled."""
+        ms = np.zeros(len(_abi.STAGES), np.float64)
+        cnt = np.zeros(len(_abi.STAGES), np.int64)
+        self._check(self._lib.p3m_profile_read(self._ctx, _ptr(ms), _ptr(cnt)))
+        return {name: (float(ms[i]), int(cnt[i])) for i, name in enumerate(_abi.STAGES)}
+
+    def stream_handle(self) -> int:
+        s = ctypes.c_void_p()
+        self._check(self._lib.p3m_get_stream(self._ctx, ctypes.byref(s)))
+        return s.value or 0
+
+    def nonfinite_count(self) -> int:
+        c = ctypes.c_int64()
+        self._check(self._lib.p3m_nonfinite_count(self._ctx, ctypes.byref(c)))
+        return c.value
+
+    def direct_accel_f64(self, n: int, targets) -> np.ndarray:
+        """FP64 direct-sum accelerations (unit/s^2) of the target bodies."""
+        t = np.ascontiguousarray(targets, np.int32)
+        out = np.empty((len(t), 2), np.float64)
+        self._check(self._lib.p3m_direct_accel_f64(self._ctx, n, _ptr(t), len(t), _ptr(out)))
+        return out
+
+    def diagnostics_f64(self, n: int) -> dict:
+        out = np.zeros(6, np.float64)
+        self._check(self._lib.p3m_diagnostics_f64(self._ctx, n, _ptr(out)))
+        return {"momentum": (out[0], out[1]), "kinetic_energy": out[2],
+                "center_of_mass": (out[3], out[4]), "mass": out[5]}
+
     # ------------------------------------------------------ intermediates
     @property
     def mesh_shape(self) -> tuple[int, int]:
@@ -216,3 +280,34 @@ class GravityPipeline:
     def green(self) -> np.ndarray:
         mw, mh = self.mesh_shape
         return self.debug_get(_abi.BUF_GREEN, np.float32, (mw // 2 + 1) * mh * 2).reshape(mh, mw // 2 + 1, 2)
+
+
+class PinnedArray:
+    """A float32 numpy array over page-locked host memory (p3m_host_alloc)."""
+
+    def __init__(self, shape):
+        self._lib = _abi.load()
+        count = int(np.prod(shape))
+        self._ptr = ctypes.c_void_p()
+        rc = self._lib.p3m_host_alloc(count * 4, ctypes.byref(self._ptr))
+        if rc != _abi.P3M_OK:
+            raise _abi.P3MError(rc, self._lib.p3m_last_error(None).decode())
+        buf = (ctypes.c_float * count).from_address(self._ptr.value)
+        self.array = np.ctypeslib.as_array(buf).reshape(shape)
+
+    def free(self) -> None:
+        if self._ptr:
+            self.array = None
+            self._lib.p3m_host_free(self._ptr)
+            self._ptr = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+
+def kernel_launches() -> int:
+    """Kernels the library has launched in this process."""
+    return int(_abi.load().p3m_kernel_launches())

@@ -129,6 +129,13 @@ const char* p3m_status_string(int status);
  * :1438-1481). Any pointer may be NULL to leave that buffer unchanged. */
 int p3m_upload_state(p3m_ctx* ctx, const float* bodies4, const float* materials4,
                      const float* acceleration2, int32_t n);
+/* Writes `count` bodies starting at slot `first` (first + count <= capacity),
+ * leaving the other slots as they are: spawnProjectile / spawnBlock write new
+ * bodies past the active ones with glBufferSubData at an offset
+ * (GravityPipeline.kt:621-718). Slots beyond the active count keep their
+ * contents across steps and reorders. */
+int p3m_upload_range(p3m_ctx* ctx, int32_t first, int32_t count, const float* bodies4,
+                     const float* materials4, const float* acceleration2);
 /* Readback (the reference maps the SSBOs: GravityPipeline.kt:378-443). */
 int p3m_download_state(p3m_ctx* ctx, float* bodies4, float* materials4,
                        float* acceleration2, int32_t n);
@@ -168,8 +175,63 @@ int p3m_apply_kick(p3m_ctx* ctx, int32_t n, int32_t initial);   /* applyKick, :1
  * build_grid.comp, as CSR lists). */
 int p3m_build_cell_lists(p3m_ctx* ctx, int32_t n);
 
+/* Steps run as CUDA graphs captured once per (body count, reorder step,
+ * current buffer, uniforms) and replayed (default on); 0 launches kernels one
+ * by one. Profiling (p3m_profile_enable) always launches one by one. */
+int p3m_set_graphs(p3m_ctx* ctx, int32_t enabled);
+
 /* Wait for the context's stream; returns the first pending device error. */
 int p3m_synchronize(p3m_ctx* ctx);
+
+/* ---- profiling and diagnostics ----------------------------------------- */
+
+/* Stages of the step, timed with CUDA events on the context's stream
+ * (the reference's GpuProfiler stages, GpuTimer.kt:17-40). */
+typedef enum p3m_stage {
+    P3M_STAGE_SPATIAL_SORT = 0, /* Morton reorder (SPATIAL_SORT) */
+    P3M_STAGE_DRIFT = 1,        /* half kick + drift substeps + cell keys */
+    P3M_STAGE_CELL_LISTS = 2,   /* cell-key radix sort + list build */
+    P3M_STAGE_DEPOSIT = 3,      /* CIC deposit (GRAVITY_GRID) */
+    P3M_STAGE_FORWARD_FFT = 4,  /* row transform (FORWARD_FFT) */
+    P3M_STAGE_SPECTRAL = 5,     /* column transforms + Green's multiply (CONVOLUTION) */
+    P3M_STAGE_INVERSE_FFT = 6,  /* row inverse (INVERSE_FFT_X/Y) */
+    P3M_STAGE_KICK = 7,         /* interpolation + short range + kick (GRAVITY_KICK) */
+    P3M_STAGE_COUNT_ = 8
+} p3m_stage;
+
+/* Start (enabled != 0, accumulators cleared) or stop recording stage events. */
+int p3m_profile_enable(p3m_ctx* ctx, int32_t enabled);
+/* Synchronises, then returns accumulated device milliseconds and the number
+ * of timed intervals per stage (arrays of P3M_STAGE_COUNT_ entries). */
+int p3m_profile_read(p3m_ctx* ctx, double* total_ms, int64_t* intervals);
+
+/* Kernels this library has launched in this process (all contexts). */
+int64_t p3m_kernel_launches(void);
+
+/* The context's CUDA stream (a cudaStream_t), for callers that order their
+ * own work or events after the library's. */
+int p3m_get_stream(p3m_ctx* ctx, void** stream);
+
+/* Page-locked host memory for fast hand-off (cudaHostAlloc / cudaFreeHost). */
+int p3m_host_alloc(size_t bytes, void** host);
+int p3m_host_free(void* host);
+
+/* Non-finite bodies the drift has seen since the context was created
+ * (the reference counts them in measureCluster, GravityPipeline.kt:817-819). */
+int p3m_nonfinite_count(p3m_ctx* ctx, int64_t* count);
+
+/* FP64 direct-sum acceleration (unit/s^2) of `n_targets` bodies (IDs in
+ * `targets`, host array) from all n bodies: the law the P3M split
+ * approximates, G*m*d / (M_tot * max(r^2, r_min^2)) with the minimum image on
+ * the torus and the open sum inside walls. Writes 2*n_targets doubles to host
+ * `out`. Diagnostic; no counterpart kernel in the reference. */
+int p3m_direct_accel_f64(p3m_ctx* ctx, int32_t n, const int32_t* targets, int32_t n_targets,
+                         double* out);
+
+/* FP64 conservation diagnostics of the first n bodies, in px units:
+ * out[0..1] momentum sum(m*v), out[2] kinetic energy sum(m*v^2/2),
+ * out[3..4] centre of mass, out[5] total mass. Deterministic reduction. */
+int p3m_diagnostics_f64(p3m_ctx* ctx, int32_t n, double* out6);
 
 #ifdef __cplusplus
 }
