@@ -107,7 +107,11 @@ SIGNATURES = {
     "p3m_nonfinite_count": (ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_int64)]),
     "p3m_direct_accel_f64": (ctypes.c_int, [_vp, _i32, _vp, _i32, _vp]),
     "p3m_diagnostics_f64": (ctypes.c_int, [_vp, _i32, _vp]),
+    "p3m_cell_lists_static": (ctypes.c_int, [_vp, _vp, _i32, _i32, _i32, _vp, _vp, _vp, _vp,
+                                             _vp, _vp, _vp]),
 }
+
+CELL_LISTS_STATIC_MAX_BODIES = 1 << 20
 
 STAGES = ("spatial_sort", "drift", "cell_lists", "deposit", "forward_fft", "spectral",
           "inverse_fft", "kick")

@@ -474,6 +474,10 @@ size_t buffer_bytes(const p3m_ctx* ctx, int which, void** dptr) {
 
 }  // namespace
 
+namespace p3m {
+void set_detached_error(const std::string& what) { g_create_error = what; }
+}  // namespace p3m
+
 extern "C" {
 
 int p3m_config_default(p3m_config* c) {

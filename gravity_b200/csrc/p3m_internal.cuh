@@ -170,6 +170,10 @@ cudaError_t launch_conservation(const float4* bodies, const float4* materials, i
 // Process-wide count of kernels launched by this library (p3m_kernel_launches).
 void count_launches(int kernels);
 
+// Sets the message p3m_last_error(NULL) returns on this thread (entry points
+// without a context).
+void set_detached_error(const std::string& what);
+
 }  // namespace p3m
 
 #include <vector>

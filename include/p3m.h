@@ -233,6 +233,38 @@ int p3m_direct_accel_f64(p3m_ctx* ctx, int32_t n, const int32_t* targets, int32_
  * out[3..4] centre of mass, out[5] total mass. Deterministic reduction. */
 int p3m_diagnostics_f64(p3m_ctx* ctx, int32_t n, double* out6);
 
+/* ---- cell lists without allocation ------------------------------------- */
+
+/* No counterpart in the reference. For callers that cannot allocate device
+ * memory when they need cell lists — code running where allocation is
+ * forbidden or would stall (inside a frame callback, a captured region), or a
+ * host whose device memory is handed out by another runtime (a JVM, an
+ * engine). Builds the same lists as p3m_build_cell_lists — keys of the home
+ * cells, the 64-bit-key radix sort, the CSR lists — from caller-owned device
+ * arrays into caller-owned device arrays, on `stream` (a cudaStream_t, NULL
+ * for the default stream), without calling cudaMalloc, cudaFree or any
+ * allocating routine.
+ *
+ * Inputs: bodies4 (float4[n]) and materials4 (float4[n]) on the current
+ * device. Outputs: sorted_keys[n] (home cell per entry), sorted_ids[n] (body
+ * IDs by cell ascending, ID descending), cell_start/cell_count/cell_mass of
+ * grid_width*grid_height cells (start valid where count > 0; the entry point
+ * zeroes all three first), entries4 (float4[n]: x, y, mass, ID bits).
+ *
+ * Limit: n <= P3M_CELL_LISTS_STATIC_MAX_BODIES; larger n returns
+ * P3M_ERR_CAPACITY with a message in p3m_last_error(NULL). The working memory
+ * is one array compiled into the library (about 16.3 MB held on every GPU that
+ * loads it, until exit). The first call on each device looks up that array's
+ * address (cudaGetSymbolAddress) with the device current; make that first call
+ * before any stream capture. All calls share the array and it keeps the last
+ * call's contents: calls whose work overlaps on the GPU race, so order them on
+ * one stream. */
+#define P3M_CELL_LISTS_STATIC_MAX_BODIES 1048576
+int p3m_cell_lists_static(const float* bodies4, const float* materials4, int32_t n,
+                          int32_t grid_width, int32_t grid_height, uint32_t* sorted_keys,
+                          int32_t* sorted_ids, int32_t* cell_start, int32_t* cell_count,
+                          uint32_t* cell_mass, float* entries4, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
