@@ -100,7 +100,9 @@ def stage_bytes(sc, stage: str, radix_passes: int) -> float:
     if stage == "inverse_fft":
         return 16.0 * M
     if stage == "kick":
-        return 56.0 * n + 20.0 * P
+        return 48.0 * n + 8.0 * P
+    if stage == "short_range":
+        return 24.0 * n + 12.0 * P
     if stage == "spatial_sort":
         return 16.0 * radix_passes * n + 88.0 * n
     return 0.0

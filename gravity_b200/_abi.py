@@ -114,7 +114,7 @@ SIGNATURES = {
 CELL_LISTS_STATIC_MAX_BODIES = 1 << 20
 
 STAGES = ("spatial_sort", "drift", "cell_lists", "deposit", "forward_fft", "spectral",
-          "inverse_fft", "kick")
+          "inverse_fft", "kick", "short_range")
 
 _lock = threading.Lock()
 _lib = None

@@ -15,6 +15,7 @@ Usage: ``python -m gravity_b200.build [--force] [--verbose]``.
 from __future__ import annotations
 
 import argparse
+from concurrent.futures import ThreadPoolExecutor
 import os
 import shutil
 import subprocess
@@ -69,7 +70,7 @@ def build(force: bool = False, verbose: bool = False, ptxas_verbose: bool = Fals
     LIB_DIR.mkdir(parents=True, exist_ok=True)
     cc = nvcc()
     hdrs = headers() + [Path(__file__)]
-    objs = []
+    objs, jobs = [], []
     for src in sources():
         obj = OBJ_DIR / (src.stem + ".o")
         objs.append(obj)
@@ -82,7 +83,12 @@ def build(force: bool = False, verbose: bool = False, ptxas_verbose: bool = Fals
             cmd += ["-Xptxas", "-v"]
         if verbose:
             print(" ".join(cmd), flush=True)
-        res = subprocess.run(cmd, capture_output=True, text=True)
+        jobs.append((src, cmd))
+    # Translation units compile independently: run them side by side.
+    with ThreadPoolExecutor(max_workers=max(1, min(len(jobs), os.cpu_count() or 1))) as pool:
+        results = list(pool.map(
+            lambda job: (job[0], subprocess.run(job[1], capture_output=True, text=True)), jobs))
+    for src, res in results:
         if verbose or ptxas_verbose:
             sys.stdout.write(res.stdout)
             sys.stderr.write(res.stderr)

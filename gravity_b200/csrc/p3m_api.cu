@@ -158,6 +158,14 @@ int validate(const p3m_config* c, std::string* why) {
     if (c->spatial_sort_interval < 0) { *why = "sort interval must be non-negative"; return P3M_ERR_INVALID_ARGUMENT; }
     if (c->capacity <= 0 || c->capacity > (1 << 28)) { *why = "capacity must be in 1..2^28"; return P3M_ERR_INVALID_ARGUMENT; }
     if (c->deposit_mode != P3M_DEPOSIT_U32 && c->deposit_mode != P3M_DEPOSIT_I64) { *why = "unknown deposit mode"; return P3M_ERR_INVALID_ARGUMENT; }
+    {
+        int rx = 1, ry = 1;
+        neighbor_radii(*c, &rx, &ry);
+        if (rx > 6 || ry > 6) {
+            *why = "neighbour radii above 6 cells are not supported";
+            return P3M_ERR_UNSUPPORTED;
+        }
+    }
     if (c->bounded && 2 * std::max(c->grid_width, c->grid_height) > p3m::kMaxMeshAxis) {
         *why = "walls need an FFT grid of at most 2048 cells per axis";
         return P3M_ERR_UNSUPPORTED;
@@ -197,7 +205,7 @@ void free_all(p3m_ctx* ctx) {
     void* ptrs[] = {ctx->diag, ctx->bodies, ctx->bodies_alt, ctx->accel, ctx->accel_alt, ctx->materials,
                     ctx->materials_alt, ctx->destinations, ctx->status, ctx->keys, ctx->vals,
                     ctx->sort.keys_alt, ctx->sort.vals_alt, ctx->sort.hist, ctx->sort.block_sums,
-                    ctx->cell_start, ctx->cell_count, ctx->cell_mass, ctx->entries, ctx->density,
+                    ctx->cell_start, ctx->cell_count, ctx->cell_mass, ctx->entries, ctx->a_short, ctx->density,
                     ctx->half, ctx->cols, ctx->force, ctx->green, ctx->twiddles};
     for (void* p : ptrs)
         if (p) cudaFree(p);
@@ -308,9 +316,15 @@ int apply_kick(p3m_ctx* ctx, int n, int initial) {
     p.sigma_cells = ctx->cfg.softening_cells; p.total_mass = ctx->normalization_mass;
     p.min_frac = ctx->cfg.minimum_distance_cell_fraction; p.dt = ctx->cfg.time_step;
     p.field_x = ctx->field_x; p.field_y = ctx->field_y;
+    if (ctx->mutual) {
+        StageScope scope(ctx, P3M_STAGE_SHORT_RANGE);
+        P3M_CUDA(ctx, p3m::launch_short_range(ctx->bodies, ctx->entries, ctx->cell_start,
+                                              ctx->cell_count, ctx->cell_mass, ctx->a_short, p,
+                                              ctx->stream));
+    }
     StageScope scope(ctx, P3M_STAGE_KICK);
-    P3M_CUDA(ctx, p3m::launch_kick(ctx->bodies, ctx->accel, ctx->force, ctx->cell_start,
-                                   ctx->cell_count, ctx->cell_mass, ctx->entries, p, ctx->stream));
+    P3M_CUDA(ctx, p3m::launch_interp_kick(ctx->bodies, ctx->accel, ctx->force, ctx->a_short, p,
+                                          ctx->stream));
     return P3M_OK;
 }
 
@@ -585,6 +599,7 @@ int p3m_create(const p3m_config* config, p3m_ctx** out) {
     ALLOC(ctx->cell_count, P);
     ALLOC(ctx->cell_mass, P);
     ALLOC(ctx->entries, cap);
+    ALLOC(ctx->a_short, cap);
     {
         unsigned long long* d = nullptr;
         ALLOC(d, M);  // 8 bytes per cell holds either deposit mode

@@ -32,10 +32,20 @@ constexpr int kTwiddleLength = 1 << kTwiddleLog2;
 // floor(x) converted to int the way the GPU's cvt.rzi.s32.f32 converts:
 // NaN -> 0, saturation at the int range (the value is already integral).
 __host__ __device__ __forceinline__ int float_to_int(float f) {
+#ifdef __CUDA_ARCH__
+    return __float2int_rz(f);  // cvt.rzi.s32.f32: the same NaN and saturation rules
+#else
     if (f != f) return 0;
     if (f >= 2147483647.0f) return 2147483647;
     if (f <= -2147483648.0f) return (int)0x80000000;
     return (int)f;
+#endif
+}
+
+// Out-of-line so that the common path below stays two compares.
+static __host__ __device__ __noinline__ int wrap_far(int v, int size) {
+    v %= size;
+    return v < 0 ? v + size : v;
 }
 
 // wrapCell / wrapMesh (build_grid.comp:21-37, kick.comp:38-59): one period
@@ -45,10 +55,7 @@ __host__ __device__ __forceinline__ int float_to_int(float f) {
 __host__ __device__ __forceinline__ int wrap_index(int v, int size) {
     if (v < 0) v += size;
     else if (v >= size) v -= size;
-    if ((unsigned)v >= (unsigned)size) {
-        v %= size;
-        if (v < 0) v += size;
-    }
+    if ((unsigned)v >= (unsigned)size) v = wrap_far(v, size);
     return v;
 }
 
@@ -147,9 +154,15 @@ struct KickParams {
     int n, W, H, MW, MH, bounded, rx, ry, exact, home_limit, initial, mutual;
     float aspect, gravity, sigma_cells, total_mass, min_frac, dt, field_x, field_y;
 };
-cudaError_t launch_kick(float4* bodies, float2* accel, const float2* force, const int* cell_start,
-                        const int* cell_count, const uint32_t* cell_mass, const float4* entries,
-                        KickParams p, cudaStream_t stream);
+// Short-range correction over the cell stencil (kick.comp:122-151), one
+// thread per body; writes a_short[id]. Radii 1..6.
+cudaError_t launch_short_range(const float4* bodies, const float4* entries, const int* cell_start,
+                               const int* cell_count, const uint32_t* cell_mass, float2* a_short,
+                               KickParams p, cudaStream_t stream);
+// CIC interpolation + field + a_short, then the half kick (kick.comp:82-103,
+// :153-154), one thread per body in ID order.
+cudaError_t launch_interp_kick(float4* bodies, float2* accel, const float2* force,
+                               const float2* a_short, KickParams p, cudaStream_t stream);
 
 // Shared-memory opt-ins, once per device (p3m_create), never during capture.
 cudaError_t configure_deposit();
@@ -238,6 +251,7 @@ struct p3m_ctx {
     int* cell_count = nullptr;
     uint32_t* cell_mass = nullptr;
     float4* entries = nullptr;
+    float2* a_short = nullptr;  // short-range accelerations, by body ID
 
     // mesh
     void* density = nullptr;

@@ -1,0 +1,197 @@
+// p3m_short_range.cuh — the short-range correction kernel (kick.comp:122-151).
+//
+// The short-range complement of the Gaussian split, summed over the
+// (2Rx+1)x(2Ry+1) cell stencil around each body's home cell: cells holding
+// more than `exact` bodies act as a monopole at the cell centre with the
+// fixed-point cell mass; other cells, and the home cell up to `home_limit`
+// list entries, are summed body by body in list order (descending ID), the
+// body itself skipped. The result goes to a_short[id]; the interpolation +
+// kick kernel adds it.
+//
+// One thread per body in ID order: after the Morton reorder IDs follow screen
+// tiles, so a warp's stencils overlap in 2D and the cell tables and
+// neighbour entries come from L1/L2. The stencil radii are template
+// parameters and the loops are unrolled; the wrapped column/row of every
+// stencil offset and its periodic image shift are computed once per target.
+//
+// EXACT = 2 (the reference's default exactNeighborBodyLimit) runs every
+// non-home stencil cell without branches: two source slots per cell, filled
+// by predicated loads of the cell's first two list entries, or the monopole
+// and an empty slot; a missing source has mass 0 and adds exactly 0, so every
+// lane of a warp does the same work whatever its cells hold. EXACT = 0 walks
+// the lists for any other limit.
+//
+// The pair term G m exp(-r^2/2s^2) d / (M max(r^2, r_min^2)) is evaluated as
+// (G/M) m exp2(-r^2 log2(e)/2s^2) * rcp(max(r^2, r_min^2)) * d with fused
+// multiply-adds. On the torus the reference takes the minimum image
+// (kick.comp:68); every stencil here spans at most 13 cells of a grid of at
+// least 16, so the image of a neighbour cell is fixed by how its column and
+// row wrapped, and the source position is shifted by that image instead of
+// rounding the displacement. Forces agree with the oracle's literal FP32
+// evaluation to ~1e-7 relative per term (another summation order and
+// rounding); the contract is 1e-5 relative RMS.
+//
+// Each p3m_short_range_rN.cu instantiates one Rx so the instantiations
+// compile in parallel.
+#pragma once
+
+#include "p3m_internal.cuh"
+
+namespace p3m {
+namespace sr {
+
+struct PairConst {
+    float aspect;
+    float neg_log2e_over_2s2;  // -log2(e) / (2 sigma^2)
+    float min_dist2;           // (min_frac * min(cell w, cell h))^2
+    float g_over_m;            // G / M_tot
+};
+
+__device__ __forceinline__ PairConst pair_const(const KickParams& p) {
+    PairConst k;
+    k.aspect = p.aspect;
+    const float sigma = p.sigma_cells / (float)p.H;
+    k.neg_log2e_over_2s2 = -1.4426950408889634f / (2.0f * sigma * sigma);
+    const float cw = p.aspect / (float)p.W, ch = 1.0f / (float)p.H;
+    const float md = p.min_frac * fminf(cw, ch);
+    k.min_dist2 = md * md;
+    k.g_over_m = p.gravity / p.total_mass;
+    return k;
+}
+
+// (dx, dy): source minus target in unit coordinates, already on the right
+// image. Adds G m exp(-r^2/2s^2) d / (M max(r^2, r_min^2)).
+__device__ __forceinline__ void pair_add(const PairConst& k, float dx, float dy, float m,
+                                         float& ax, float& ay) {
+    const float px = dx * k.aspect;
+    const float r2 = fmaf(px, px, dy * dy);
+    const float w = exp2f(r2 * k.neg_log2e_over_2s2);
+    const float phys = __fdividef(k.g_over_m * m * w, fmaxf(r2, k.min_dist2));
+    ax = fmaf(phys, dx, ax);  // (phys * px) / aspect == phys * dx
+    ay = fmaf(phys, dy, ay);
+}
+
+template <int RX, int RY, int EXACT>
+__global__ void __launch_bounds__(256) short_range_kernel(
+    const float4* __restrict__ bodies, const float4* __restrict__ entries,
+    const int* __restrict__ cell_start, const int* __restrict__ cell_count,
+    const uint32_t* __restrict__ cell_mass, float2* __restrict__ a_short, KickParams p) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= p.n) return;
+    const float4 t = bodies[i];
+    const uint32_t id = (uint32_t)i;
+    const PairConst k = pair_const(p);
+    const float inv_w = 1.0f / (float)p.W, inv_h = 1.0f / (float)p.H;
+    const int hx = guard_coord(float_to_int(floorf(t.x * (float)p.W)), p.W);
+    const int hy = guard_coord(float_to_int(floorf(t.y * (float)p.H)), p.H);
+
+    // Per stencil column: wrapped column, periodic image shift, validity.
+    int col[2 * RX + 1];
+    float shift_x[2 * RX + 1];
+    bool ok_x[2 * RX + 1];
+#pragma unroll
+    for (int a = 0; a < 2 * RX + 1; ++a) {
+        const int cx = hx + a - RX;
+        const int wx = wrap_index(cx, p.W);
+        col[a] = wx;
+        shift_x[a] = (float)(cx - wx) * inv_w;
+        ok_x[a] = !p.bounded || (cx >= 0 && cx < p.W);
+    }
+    float ax = 0.0f, ay = 0.0f;
+#pragma unroll
+    for (int b = 0; b < 2 * RY + 1; ++b) {
+        const int cy = hy + b - RY;
+        if (p.bounded && (cy < 0 || cy >= p.H)) continue;
+        const int wy = wrap_index(cy, p.H);
+        const int row = wy * p.W;
+        const float shift_y = (float)(cy - wy) * inv_h;
+        const float cyr = ((float)wy + 0.5f) * inv_h;  // wrapped row centre
+#pragma unroll
+        for (int a = 0; a < 2 * RX + 1; ++a) {
+            if (!ok_x[a]) continue;
+            const int index = row + col[a];
+            const int count = __ldg(&cell_count[index]);
+            const bool home = (a == RX) && (b == RY);
+            if (EXACT == 2 && !home) {
+                const float cxr = ((float)col[a] + 0.5f) * inv_w;  // wrapped column centre
+                float4 s0 = make_float4(cxr, cyr, 0.0f, 0.0f);
+                float4 s1 = s0;
+                if (count > 2) {
+                    s0.z = (float)__ldg(&cell_mass[index]) * (1.0f / kCellMassUnits);
+                } else if (count > 0) {
+                    const int start = __ldg(&cell_start[index]);
+                    s0 = __ldg(&entries[start]);
+                    if (count == 2) s1 = __ldg(&entries[start + 1]);
+                }
+                pair_add(k, (s0.x + shift_x[a]) - t.x, (s0.y + shift_y) - t.y, s0.z, ax, ay);
+                pair_add(k, (s1.x + shift_x[a]) - t.x, (s1.y + shift_y) - t.y, s1.z, ax, ay);
+                continue;
+            }
+            if (count == 0) continue;
+            if (!home && count > p.exact) {
+                const float mass = (float)__ldg(&cell_mass[index]) * (1.0f / kCellMassUnits);
+                const float dx = ((float)col[a] + 0.5f) * inv_w + shift_x[a] - t.x;
+                pair_add(k, dx, (cyr + shift_y) - t.y, mass, ax, ay);
+            } else {
+                const int limit = home ? p.home_limit : p.exact;
+                const int walk = count < limit ? count : limit;
+                const int start = __ldg(&cell_start[index]);
+                for (int e = 0; e < walk; ++e) {
+                    const float4 o = __ldg(&entries[start + e]);
+                    if (__float_as_uint(o.w) != id)
+                        pair_add(k, (o.x + shift_x[a]) - t.x, (o.y + shift_y) - t.y, o.z, ax, ay);
+                }
+            }
+        }
+    }
+    a_short[id] = make_float2(ax, ay);
+}
+
+}  // namespace sr
+
+// Launches short_range_kernel<RX, p.ry, 2 or 0>; defined (explicitly
+// instantiated) in p3m_short_range_rN.cu.
+template <int RX>
+cudaError_t launch_short_range_rx(const float4* bodies, const float4* entries,
+                                  const int* cell_start, const int* cell_count,
+                                  const uint32_t* cell_mass, float2* a_short, const KickParams& p,
+                                  cudaStream_t stream);
+#define P3M_DECLARE_SHORT_RANGE_RX(RX_)                                                       \
+    template <>                                                                                 \
+    cudaError_t launch_short_range_rx<RX_>(const float4*, const float4*, const int*, const int*, \
+                                           const uint32_t*, float2*, const KickParams&,         \
+                                           cudaStream_t);
+P3M_DECLARE_SHORT_RANGE_RX(1)
+P3M_DECLARE_SHORT_RANGE_RX(2)
+P3M_DECLARE_SHORT_RANGE_RX(3)
+P3M_DECLARE_SHORT_RANGE_RX(4)
+P3M_DECLARE_SHORT_RANGE_RX(5)
+P3M_DECLARE_SHORT_RANGE_RX(6)
+#undef P3M_DECLARE_SHORT_RANGE_RX
+
+#define P3M_DEFINE_SHORT_RANGE_RX(RX_)                                                          \
+    template <>                                                                                 \
+    cudaError_t launch_short_range_rx<RX_>(const float4* bodies, const float4* entries,         \
+                                           const int* cell_start, const int* cell_count,        \
+                                           const uint32_t* cell_mass, float2* a_short,          \
+                                           const KickParams& p, cudaStream_t stream) {          \
+        const dim3 grid((p.n + 255) / 256), block(256);                                         \
+        switch (p.ry * 2 + (p.exact == 2 ? 1 : 0)) {                                            \
+            case 3: sr::short_range_kernel<RX_, 1, 2><<<grid, block, 0, stream>>>(bodies, entries, cell_start, cell_count, cell_mass, a_short, p); break; \
+            case 2: sr::short_range_kernel<RX_, 1, 0><<<grid, block, 0, stream>>>(bodies, entries, cell_start, cell_count, cell_mass, a_short, p); break; \
+            case 5: sr::short_range_kernel<RX_, 2, 2><<<grid, block, 0, stream>>>(bodies, entries, cell_start, cell_count, cell_mass, a_short, p); break; \
+            case 4: sr::short_range_kernel<RX_, 2, 0><<<grid, block, 0, stream>>>(bodies, entries, cell_start, cell_count, cell_mass, a_short, p); break; \
+            case 7: sr::short_range_kernel<RX_, 3, 2><<<grid, block, 0, stream>>>(bodies, entries, cell_start, cell_count, cell_mass, a_short, p); break; \
+            case 6: sr::short_range_kernel<RX_, 3, 0><<<grid, block, 0, stream>>>(bodies, entries, cell_start, cell_count, cell_mass, a_short, p); break; \
+            case 9: sr::short_range_kernel<RX_, 4, 2><<<grid, block, 0, stream>>>(bodies, entries, cell_start, cell_count, cell_mass, a_short, p); break; \
+            case 8: sr::short_range_kernel<RX_, 4, 0><<<grid, block, 0, stream>>>(bodies, entries, cell_start, cell_count, cell_mass, a_short, p); break; \
+            case 11: sr::short_range_kernel<RX_, 5, 2><<<grid, block, 0, stream>>>(bodies, entries, cell_start, cell_count, cell_mass, a_short, p); break; \
+            case 10: sr::short_range_kernel<RX_, 5, 0><<<grid, block, 0, stream>>>(bodies, entries, cell_start, cell_count, cell_mass, a_short, p); break; \
+            case 13: sr::short_range_kernel<RX_, 6, 2><<<grid, block, 0, stream>>>(bodies, entries, cell_start, cell_count, cell_mass, a_short, p); break; \
+            case 12: sr::short_range_kernel<RX_, 6, 0><<<grid, block, 0, stream>>>(bodies, entries, cell_start, cell_count, cell_mass, a_short, p); break; \
+            default: return cudaErrorInvalidValue;                                              \
+        }                                                                                       \
+        return cudaGetLastError();                                                              \
+    }
+
+}  // namespace p3m

@@ -1,0 +1,7 @@
+// p3m_short_range_r3.cu — short-range kernels with a stencil half-width of
+// 3 cell(s) in x (see p3m_short_range.cuh).
+#include "p3m_short_range.cuh"
+
+namespace p3m {
+P3M_DEFINE_SHORT_RANGE_RX(3)
+}  // namespace p3m

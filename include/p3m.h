@@ -195,8 +195,9 @@ typedef enum p3m_stage {
     P3M_STAGE_FORWARD_FFT = 4,  /* row transform (FORWARD_FFT) */
     P3M_STAGE_SPECTRAL = 5,     /* column transforms + Green's multiply (CONVOLUTION) */
     P3M_STAGE_INVERSE_FFT = 6,  /* row inverse (INVERSE_FFT_X/Y) */
-    P3M_STAGE_KICK = 7,         /* interpolation + short range + kick (GRAVITY_KICK) */
-    P3M_STAGE_COUNT_ = 8
+    P3M_STAGE_KICK = 7,         /* interpolation + half kick (GRAVITY_KICK) */
+    P3M_STAGE_SHORT_RANGE = 8,  /* short-range correction (GRAVITY_KICK, near field) */
+    P3M_STAGE_COUNT_ = 9
 } p3m_stage;
 
 /* Start (enabled != 0, accumulators cleared) or stop recording stage events. */
