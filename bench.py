@@ -67,6 +67,8 @@ def make_workload(name: str):
         return scenarios.uniform_torus()
     if name == "lattice_scale":
         return scenarios.lattice_scale()
+    if name == "batch":
+        return scenarios.batch()
     if name == "lattice_scale_u32":
         from gravity_b200 import _abi
         return scenarios.lattice_scale(deposit_mode=_abi.P3M_DEPOSIT_U32)
@@ -261,6 +263,23 @@ def force_error_vs_fp64(pipe, sc) -> float:
 def run_reference(args, ws, rank):
     if rank != 0:
         return
+    if args.workload == "batch":
+        scs = make_workload("batch")
+        budget = max(5.0, min(90.0, float(args.steps) * 2.0))
+        rate, sims, el, used = cpu_oracle_batch_rate(scs, budget, threads=os.cpu_count())
+        sample = (f"the first {sims} of {len(scs)} simulations, 4 P3M steps each ({el:.1f} s) "
+                  f"after initialisation and 1 untimed step")
+        line = {
+            "impl": "reference", "metric": METRIC, "value": rate, "unit": UNIT, "n_gpus": ws,
+            "steps": 4, "warmup": 1, "ms_per_step": None, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": batch_config(scs, args),
+            "cpu_baseline": {"value": rate, "unit": UNIT, "cores": used, "kind": "port",
+                             "sample": sample},
+            "e2e": {"value": rate, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        }
+        print(json.dumps(line), flush=True)
+        return
     sc = make_workload(args.workload)
     threads = os.cpu_count() or 1
     budget = max(5.0, min(90.0, float(args.steps) * 2.0))
@@ -278,6 +297,51 @@ def run_reference(args, ws, rank):
         "e2e": {"value": rate, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
+
+
+def batch_config(scs, args):
+    from collections import Counter
+
+    grids = Counter(f"{sc.config.gravity.grid_width}x{sc.config.gravity.grid_height}" for sc in scs)
+    ns = [sc.n for sc in scs]
+    return {
+        "workload": "batch", "simulations": len(scs), "n_bodies": int(sum(ns)),
+        "n_min": int(min(ns)), "n_max": int(max(ns)), "grids": dict(sorted(grids.items())),
+        "boundary": "torus", "deposit": "uint32", "px_per_cell": 5,
+        "dt": scs[0].config.time_step, "drift_substeps": scs[0].config.drift_substeps,
+        "spatial_sort_interval": scs[0].config.spatial_sort_interval,
+        "l2": "flushed (256 MiB write) before every timed step",
+        "parallelism": "replicas" if args.gpus > 1 else "single",
+    }
+
+
+def cpu_oracle_batch_rate(scs, budget_s: float, threads: int | None = None):
+    """bodies*steps/s of the CPU oracle over the batch's simulations taken in
+    order, each initialised and stepped once untimed, then stepped 4 times
+    timed, until `budget_s` of timed work is spent."""
+    import oracle
+
+    if threads:
+        oracle.set_threads(threads)
+    used = oracle.max_threads()
+    work = 0
+    el = 0.0
+    sims = 0
+    for sc in scs:
+        sim = oracle.OracleSim(sc.config)
+        sim.upload(sc.bodies, sc.materials)
+        sim.initialize_acceleration(sc.n)
+        sim.step(sc.n)
+        t0 = time.perf_counter()
+        for _ in range(4):
+            sim.step(sc.n)
+        el += time.perf_counter() - t0
+        sim.close()
+        work += 4 * sc.n
+        sims += 1
+        if el >= budget_s:
+            break
+    return work / el, sims, el, used
 
 
 def workload_config(sc, args):
@@ -436,6 +500,185 @@ def run_b200(args, ws, rank, local):
         dist.destroy_process_group()
 
 
+def run_batch(args, ws, rank, local):
+    """256 simulations of uneven sizes stepped together (one graph launch per
+    batch step), after the autotuner has picked launch shapes per grid."""
+    import torch
+
+    from gravity_b200.batch import GravityBatch
+    from gravity_b200.pipeline import GravityPipeline, PinnedArray, kernel_launches
+
+    dist = init_dist(ws, local)
+    torch.cuda.set_device(local)
+    scs = make_workload("batch")
+    total_n = sum(sc.n for sc in scs)
+    flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device="cuda")
+    batch = GravityBatch([sc.config for sc in scs])
+    stream = torch.cuda.ExternalStream(batch.stream_handle())
+
+    def reset():
+        for i, sc in enumerate(scs):
+            batch.upload(i, sc.bodies, sc.materials)
+        batch.initialize_acceleration()
+
+    reset()
+    batch.step(2)
+    tuned = batch.autotune(trial_steps=3)
+    reset()
+    # Every captured graph (body counts x reorder phase x buffers) is built
+    # during the warm-up.
+    warmup = max(args.warmup, 4)
+    batch.step(warmup)
+    batch.synchronize()
+    if dist:
+        dist.barrier()
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    stops = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    clocks = ClockSampler(local)
+    clocks.start()
+    time.sleep(0.3)
+    launches0 = kernel_launches()
+    with torch.cuda.stream(stream):
+        for i in range(args.steps):
+            flush.zero_()
+            starts[i].record(stream)
+            batch.step(1)
+            stops[i].record(stream)
+    torch.cuda.synchronize()
+    batch.synchronize()
+    launches = kernel_launches() - launches0
+    clk = clocks.stop()
+    total_ms = allreduce_max(dist, sum(a.elapsed_time(b) for a, b in zip(starts, stops)))
+    value = ws * total_n * args.steps / (total_ms / 1000.0)
+
+    # ---- e2e: every step uploads every simulation's bodies and materials
+    # from page-locked memory, steps the batch and reads every simulation's
+    # bodies back.
+    e2e_steps = args.steps if args.e2e_steps is None else min(args.steps, args.e2e_steps)
+    hb = [PinnedArray((sc.n, 4)) for sc in scs]
+    hm = [PinnedArray((sc.n, 4)) for sc in scs]
+    out = [PinnedArray((sc.n, 4)) for sc in scs]
+    views = []
+    for i, sc in enumerate(scs):
+        hb[i].array[:] = sc.bodies
+        hm[i].array[:] = sc.materials
+        views.append(batch.simulation(i))
+    e2e_s = 0.0
+    for it in range(min(args.warmup, 3) + e2e_steps):
+        with torch.cuda.stream(stream):
+            flush.zero_()
+        batch.synchronize()
+        t0 = time.perf_counter()
+        for i in range(len(scs)):
+            batch.upload(i, hb[i].array, hm[i].array)
+        batch.step(1)
+        batch.synchronize()
+        for i, sc in enumerate(scs):
+            views[i].download_into(sc.n, out[i].array)
+        if it >= min(args.warmup, 3):
+            e2e_s += time.perf_counter() - t0
+    e2e_s = allreduce_max(dist, e2e_s)
+    e2e_value = ws * total_n * e2e_steps / e2e_s
+
+    # ---- per-stage device time: every simulation stepped on its own with
+    # stage events (no graphs), summed over simulations.
+    stage_rows = {}
+    for i, sc in enumerate(scs):
+        views[i].profile_enable(True)
+        for _ in range(2):
+            views[i].step(sc.n)
+        prof = views[i].profile_read()
+        views[i].profile_enable(False)
+        P, M = mesh_sizes(sc)
+        for name, (ms, cnt) in prof.items():
+            if cnt == 0:
+                continue
+            passes = radix_passes_for(P)
+            if name == "spatial_sort":
+                from gravity_b200.config import sort_axis_bits
+                passes = (sort_axis_bits(sc.config.viewport_width)
+                          + sort_axis_bits(sc.config.viewport_height) + 7) // 8
+            r = stage_rows.setdefault(name, {"ms": 0.0, "launches": 0, "bytes": 0.0})
+            r["ms"] += ms
+            r["launches"] += cnt
+            r["bytes"] += stage_bytes(sc, name, passes) * cnt
+    for v in views:
+        v.close()
+    batch.close()
+
+    # ---- the same simulations as serial runs of the plain path: one context
+    # each, run alone for its steps (graph-replayed) before the next starts
+    pipes = []
+    for sc in scs:
+        p = GravityPipeline(sc.config)
+        p.upload(sc.bodies, sc.materials)
+        p.initialize_acceleration(sc.n)
+        pipes.append(p)
+    for _ in range(warmup):
+        for p, sc in zip(pipes, scs):
+            p.step(sc.n)
+    for p in pipes:
+        p.synchronize()
+    indiv_steps = min(args.steps, 30)
+    t0 = time.perf_counter()
+    for p, sc in zip(pipes, scs):
+        p.step(sc.n, indiv_steps)
+        p.synchronize()
+    serial_value = total_n * indiv_steps / (time.perf_counter() - t0)
+    # ... and all contexts stepped in turn from the host without waiting
+    # (their streams overlap on the GPU).
+    t0 = time.perf_counter()
+    for _ in range(indiv_steps):
+        for p, sc in zip(pipes, scs):
+            p.step(sc.n)
+    for p in pipes:
+        p.synchronize()
+    overlapped_value = total_n * indiv_steps / (time.perf_counter() - t0)
+    for p in pipes:
+        p.close()
+    for a in hb + hm + out:
+        a.free()
+
+    if rank == 0:
+        peak, peak_kind = measured_peaks()
+        rows = {k: {"ms_per_launch": v["ms"] / v["launches"], "launches": v["launches"],
+                    "algorithmic_bytes": v["bytes"] / v["launches"],
+                    "gbs": v["bytes"] / (v["ms"] / 1000.0) / 1e9 if v["ms"] > 0 else None}
+                for k, v in stage_rows.items()}
+        dominant = max(rows, key=lambda k: stage_rows[k]["ms"])
+        achieved = rows[dominant]["gbs"]
+        cpu = None
+        if not args.no_cpu_baseline:
+            rate, sims, el, used = cpu_oracle_batch_rate(scs, args.cpu_seconds, threads=os.cpu_count())
+            cpu = {"value": rate, "unit": UNIT, "cores": used, "kind": "port",
+                   "sample": f"the first {sims} of {len(scs)} simulations, 4 P3M steps each "
+                             f"({el:.1f} s) after initialisation and 1 untimed step"}
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+            "warmup": warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": batch_config(scs, args),
+            "autotuned": [{"grid": f"{r[0]}x{r[1]}", "fft_lines_per_cta": r[2] or "auto",
+                           "short_range_threads": r[3]} for r in tuned],
+            "serial_runs_value": serial_value,
+            "overlapped_contexts_value": overlapped_value,
+            "roofline": {"bound": "hbm", "kernel": dominant, "achieved": achieved, "peak": peak,
+                         "unit": "GB/s", "frac": achieved / peak if achieved else None,
+                         "traffic": None, "peak_source": peak_kind,
+                         "note": "stage bytes and device time summed over the simulations"},
+            "stages": rows,
+            "cpu_baseline": cpu,
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 32 * total_n,
+                    "d2h_bytes_per_step": 16 * total_n, "steps": e2e_steps},
+            "gpu_launches": launches,
+            "clocks": clk,
+        }
+        print(json.dumps(line), flush=True)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
 def main():
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     ap.add_argument("--gpus", type=int, default=1)
@@ -443,7 +686,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
     ap.add_argument("--workload", default="plummer_walls",
-                    choices=["plummer_walls", "uniform_torus", "lattice_scale", "lattice_scale_u32"])
+                    choices=["plummer_walls", "uniform_torus", "lattice_scale", "lattice_scale_u32",
+                             "batch"])
     ap.add_argument("--e2e-steps", type=int, default=None)
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -453,6 +697,9 @@ def main():
     ws, rank, local = dist_env()
     if args.impl == "reference":
         run_reference(args, ws, rank)
+        return
+    if args.workload == "batch":
+        run_batch(args, ws, rank, local)
         return
     run_b200(args, ws, rank, local)
 

@@ -107,6 +107,17 @@ SIGNATURES = {
     "p3m_nonfinite_count": (ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_int64)]),
     "p3m_direct_accel_f64": (ctypes.c_int, [_vp, _i32, _vp, _i32, _vp]),
     "p3m_diagnostics_f64": (ctypes.c_int, [_vp, _i32, _vp]),
+    "p3m_batch_create": (ctypes.c_int, [ctypes.POINTER(P3MConfig), _i32, ctypes.POINTER(_vp)]),
+    "p3m_batch_destroy": (ctypes.c_int, [_vp]),
+    "p3m_batch_last_error": (ctypes.c_char_p, [_vp]),
+    "p3m_batch_size": (ctypes.c_int, [_vp, ctypes.POINTER(_i32)]),
+    "p3m_batch_context": (ctypes.c_int, [_vp, _i32, ctypes.POINTER(_vp)]),
+    "p3m_batch_upload": (ctypes.c_int, [_vp, _i32, _vp, _vp, _i32]),
+    "p3m_batch_initialize_acceleration": (ctypes.c_int, [_vp]),
+    "p3m_batch_step": (ctypes.c_int, [_vp, _i32]),
+    "p3m_batch_autotune": (ctypes.c_int, [_vp, _i32, _vp]),
+    "p3m_batch_synchronize": (ctypes.c_int, [_vp]),
+    "p3m_batch_get_stream": (ctypes.c_int, [_vp, ctypes.POINTER(_vp)]),
     "p3m_cell_lists_static": (ctypes.c_int, [_vp, _vp, _i32, _i32, _i32, _vp, _vp, _vp, _vp,
                                              _vp, _vp, _vp]),
 }

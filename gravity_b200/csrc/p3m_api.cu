@@ -180,6 +180,7 @@ p3m::GridShape grid_for(const p3m_ctx* ctx) {
     g.bounded = ctx->bounded;
     g.MW = ctx->bounded ? 2 * g.W : g.W;
     g.MH = ctx->bounded ? 2 * g.H : g.H;
+    g.fft_lines = ctx->tune_fft_lines;
     return g;
 }
 
@@ -316,6 +317,7 @@ int apply_kick(p3m_ctx* ctx, int n, int initial) {
     p.sigma_cells = ctx->cfg.softening_cells; p.total_mass = ctx->normalization_mass;
     p.min_frac = ctx->cfg.minimum_distance_cell_fraction; p.dt = ctx->cfg.time_step;
     p.field_x = ctx->field_x; p.field_y = ctx->field_y;
+    p.sr_threads = ctx->tune_sr_threads;
     if (ctx->mutual) {
         StageScope scope(ctx, P3M_STAGE_SHORT_RANGE);
         P3M_CUDA(ctx, p3m::launch_short_range(ctx->bodies, ctx->entries, ctx->cell_start,
@@ -929,6 +931,387 @@ int p3m_diagnostics_f64(p3m_ctx* ctx, int32_t n, double* out6) {
                                            ctx->stream));
     P3M_CUDA(ctx, cudaMemcpyAsync(out6, result, 6 * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
     P3M_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    return P3M_OK;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Batched form: many independent simulations of uneven sizes (the
+// application's trajectory previews and ensembles), stepped together.
+//
+// Every simulation keeps its own context, buffers and stream. A batch step is
+// captured once as one CUDA graph: an event on the batch stream forks to every
+// simulation's stream, each enqueues its whole step (reorder, drift, lists,
+// deposit, FFT, short range, kick), and the batch stream joins them all. The
+// graph is replayed with one cudaGraphLaunch per step for the whole batch,
+// and the GPU runs the simulations' chains side by side. A replay bakes in
+// every simulation's body count, reorder phase, current ping-pong buffer and
+// uniforms; the cache keys on all of them and captures a new graph when any
+// changes (with the default reorder interval of 2 a steady batch cycles
+// through four graphs).
+
+struct p3m_batch {
+    std::vector<p3m_ctx*> sims;
+    std::vector<int> n;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t fork = nullptr;
+    std::vector<cudaEvent_t> join;
+    struct Graph {
+        std::vector<uint64_t> key;
+        cudaGraphExec_t exec;
+        long long kernels;
+        std::vector<std::pair<uint32_t*, uint32_t*>> sorted;
+    };
+    std::vector<Graph> graphs;
+    std::string last_error;
+};
+
+namespace {
+
+int batch_fail(p3m_batch* b, int status, const std::string& what) {
+    if (b) b->last_error = what;
+    else g_create_error = what;
+    return status;
+}
+
+int batch_fail_ctx(p3m_batch* b, size_t sim, int status) {
+    return batch_fail(b, status, "simulation " + std::to_string(sim) + ": " + b->sims[sim]->last_error);
+}
+
+void batch_drop_graphs(p3m_batch* b) {
+    for (auto& g : b->graphs) cudaGraphExecDestroy(g.exec);
+    b->graphs.clear();
+}
+
+uint64_t bits_of(float f) {
+    uint32_t u;
+    std::memcpy(&u, &f, 4);
+    return u;
+}
+
+// Everything one captured batch step bakes in.
+std::vector<uint64_t> batch_key(const p3m_batch* b, const std::vector<char>& sort) {
+    std::vector<uint64_t> key;
+    key.reserve(b->sims.size() * 6);
+    for (size_t i = 0; i < b->sims.size(); ++i) {
+        const p3m_ctx* c = b->sims[i];
+        key.push_back((uint64_t)b->n[i] | ((uint64_t)sort[i] << 32) | ((uint64_t)c->mutual << 33) |
+                      ((uint64_t)c->bounded << 34));
+        key.push_back((uint64_t)(uintptr_t)c->bodies);
+        key.push_back((uint64_t)c->mass_scale | (bits_of(c->normalization_mass) << 32));
+        key.push_back(bits_of(c->field_x) | (bits_of(c->field_y) << 32));
+        key.push_back((uint64_t)c->tune_fft_lines | ((uint64_t)c->tune_sr_threads << 32));
+    }
+    return key;
+}
+
+int batch_enqueue(p3m_batch* b, const std::vector<char>& sort) {
+    cudaError_t e = cudaEventRecord(b->fork, b->stream);
+    if (e != cudaSuccess) return batch_fail(b, P3M_ERR_CUDA, cudaGetErrorString(e));
+    for (size_t i = 0; i < b->sims.size(); ++i) {
+        p3m_ctx* c = b->sims[i];
+        e = cudaStreamWaitEvent(c->stream, b->fork, 0);
+        if (e != cudaSuccess) return batch_fail(b, P3M_ERR_CUDA, cudaGetErrorString(e));
+        int st = enqueue_step(c, b->n[i], sort[i] != 0);
+        if (st != P3M_OK) return batch_fail_ctx(b, i, st);
+        e = cudaEventRecord(b->join[i], c->stream);
+        if (e == cudaSuccess) e = cudaStreamWaitEvent(b->stream, b->join[i], 0);
+        if (e != cudaSuccess) return batch_fail(b, P3M_ERR_CUDA, cudaGetErrorString(e));
+    }
+    return P3M_OK;
+}
+
+int batch_one_step(p3m_batch* b) {
+    std::vector<char> sort(b->sims.size(), 0);
+    for (size_t i = 0; i < b->sims.size(); ++i) {
+        p3m_ctx* c = b->sims[i];
+        normalize_to(c, b->n[i]);
+        int st = ensure_green(c);
+        if (st != P3M_OK) return batch_fail_ctx(b, i, st);
+        const int interval = c->cfg.spatial_sort_interval;
+        sort[i] = (interval > 0 && (c->physics_steps % interval) == 0) ? 1 : 0;
+        if (interval > 0) c->physics_steps++;
+    }
+    const std::vector<uint64_t> key = batch_key(b, sort);
+    for (const auto& g : b->graphs) {
+        if (g.key != key) continue;
+        cudaError_t e = cudaGraphLaunch(g.exec, b->stream);
+        if (e != cudaSuccess) return batch_fail(b, P3M_ERR_CUDA, cudaGetErrorString(e));
+        p3m::count_launches((int)g.kernels);
+        for (size_t i = 0; i < b->sims.size(); ++i) {
+            if (sort[i]) swap_body_buffers(b->sims[i]);
+            b->sims[i]->sorted_keys = g.sorted[i].first;
+            b->sims[i]->sorted_ids = g.sorted[i].second;
+        }
+        return P3M_OK;
+    }
+    struct Saved { float4 *b, *ba, *m, *ma; float2 *a, *aa; };
+    std::vector<Saved> saved;
+    for (p3m_ctx* c : b->sims)
+        saved.push_back({c->bodies, c->bodies_alt, c->materials, c->materials_alt, c->accel, c->accel_alt});
+    const long long k0 = p3m_kernel_launches();
+    cudaError_t e = cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal);
+    if (e != cudaSuccess) return batch_fail(b, P3M_ERR_CUDA, cudaGetErrorString(e));
+    int st = batch_enqueue(b, sort);
+    cudaGraph_t graph = nullptr;
+    e = cudaStreamEndCapture(b->stream, &graph);
+    if (st != P3M_OK || e != cudaSuccess) {
+        if (graph) cudaGraphDestroy(graph);
+        for (size_t i = 0; i < b->sims.size(); ++i) {  // nothing ran: restore buffer roles
+            p3m_ctx* c = b->sims[i];
+            c->bodies = saved[i].b; c->bodies_alt = saved[i].ba;
+            c->materials = saved[i].m; c->materials_alt = saved[i].ma;
+            c->accel = saved[i].a; c->accel_alt = saved[i].aa;
+        }
+        if (st != P3M_OK) return st;
+        return batch_fail(b, P3M_ERR_CUDA, std::string("capture: ") + cudaGetErrorString(e));
+    }
+    p3m_batch::Graph entry;
+    entry.key = key;
+    entry.kernels = p3m_kernel_launches() - k0;
+    e = cudaGraphInstantiate(&entry.exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (e != cudaSuccess) return batch_fail(b, P3M_ERR_CUDA, std::string("instantiate: ") + cudaGetErrorString(e));
+    for (p3m_ctx* c : b->sims) entry.sorted.push_back({c->sorted_keys, c->sorted_ids});
+    if (b->graphs.size() >= 8) {
+        cudaGraphExecDestroy(b->graphs.front().exec);
+        b->graphs.erase(b->graphs.begin());
+    }
+    b->graphs.push_back(std::move(entry));
+    e = cudaGraphLaunch(b->graphs.back().exec, b->stream);
+    if (e != cudaSuccess) return batch_fail(b, P3M_ERR_CUDA, cudaGetErrorString(e));
+    return P3M_OK;
+}
+
+// Device time of `steps` direct (not captured) steps of one simulation.
+int time_direct_steps(p3m_ctx* c, int n, int steps, float* ms) {
+    cudaEvent_t t0 = nullptr, t1 = nullptr;
+    P3M_CUDA(c, cudaEventCreate(&t0));
+    P3M_CUDA(c, cudaEventCreate(&t1));
+    P3M_CUDA(c, cudaEventRecord(t0, c->stream));
+    for (int s = 0; s < steps; ++s) {
+        normalize_to(c, n);
+        const int interval = c->cfg.spatial_sort_interval;
+        const bool sort = interval > 0 && (c->physics_steps % interval) == 0;
+        if (interval > 0) c->physics_steps++;
+        int st = enqueue_step(c, n, sort);
+        if (st != P3M_OK) return st;
+    }
+    P3M_CUDA(c, cudaEventRecord(t1, c->stream));
+    P3M_CUDA(c, cudaEventSynchronize(t1));
+    P3M_CUDA(c, cudaEventElapsedTime(ms, t0, t1));
+    cudaEventDestroy(t0);
+    cudaEventDestroy(t1);
+    return P3M_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int p3m_batch_create(const p3m_config* configs, int32_t count, p3m_batch** out) {
+    g_create_error.clear();
+    if (!out || !configs || count <= 0) return batch_fail(nullptr, P3M_ERR_INVALID_ARGUMENT, "configs, count and out are required");
+    *out = nullptr;
+    p3m_batch* b = new (std::nothrow) p3m_batch();
+    if (!b) return batch_fail(nullptr, P3M_ERR_OUT_OF_MEMORY, "host allocation failed");
+    auto undo = [&](int st) {
+        for (p3m_ctx* c : b->sims) p3m_destroy(c);
+        for (cudaEvent_t e : b->join) cudaEventDestroy(e);
+        if (b->fork) cudaEventDestroy(b->fork);
+        if (b->stream) cudaStreamDestroy(b->stream);
+        delete b;
+        return st;
+    };
+    cudaError_t e = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming);
+    if (e != cudaSuccess) return undo(fail_cuda(nullptr, "batch stream/event", e));
+    for (int32_t i = 0; i < count; ++i) {
+        p3m_ctx* c = nullptr;
+        int st = p3m_create(&configs[i], &c);
+        if (st != P3M_OK) {
+            g_create_error = "simulation " + std::to_string(i) + ": " + g_create_error;
+            return undo(st);
+        }
+        b->sims.push_back(c);
+        b->n.push_back(0);
+        cudaEvent_t j = nullptr;
+        e = cudaEventCreateWithFlags(&j, cudaEventDisableTiming);
+        if (e != cudaSuccess) return undo(fail_cuda(nullptr, "batch event", e));
+        b->join.push_back(j);
+    }
+    *out = b;
+    return P3M_OK;
+}
+
+int p3m_batch_destroy(p3m_batch* b) {
+    if (!b) return P3M_OK;
+    cudaStreamSynchronize(b->stream);
+    batch_drop_graphs(b);
+    for (p3m_ctx* c : b->sims) p3m_destroy(c);
+    for (cudaEvent_t e : b->join) cudaEventDestroy(e);
+    cudaEventDestroy(b->fork);
+    cudaStreamDestroy(b->stream);
+    delete b;
+    return P3M_OK;
+}
+
+const char* p3m_batch_last_error(const p3m_batch* b) {
+    return b ? b->last_error.c_str() : g_create_error.c_str();
+}
+
+int p3m_batch_size(const p3m_batch* b, int32_t* count) {
+    if (!b || !count) return P3M_ERR_INVALID_ARGUMENT;
+    *count = (int32_t)b->sims.size();
+    return P3M_OK;
+}
+
+int p3m_batch_context(p3m_batch* b, int32_t sim, p3m_ctx** ctx) {
+    if (!b || !ctx) return P3M_ERR_INVALID_ARGUMENT;
+    if (sim < 0 || sim >= (int32_t)b->sims.size()) return batch_fail(b, P3M_ERR_INVALID_ARGUMENT, "simulation index out of range");
+    *ctx = b->sims[sim];
+    return P3M_OK;
+}
+
+int p3m_batch_upload(p3m_batch* b, int32_t sim, const float* bodies4, const float* materials4,
+                     int32_t n) {
+    p3m_ctx* c = nullptr;
+    int st = p3m_batch_context(b, sim, &c);
+    if (st != P3M_OK) return st;
+    cudaError_t e = cudaStreamSynchronize(b->stream);
+    if (e != cudaSuccess) return batch_fail(b, P3M_ERR_CUDA, cudaGetErrorString(e));
+    st = p3m_upload_state(c, bodies4, materials4, nullptr, n);
+    if (st != P3M_OK) return batch_fail_ctx(b, (size_t)sim, st);
+    b->n[sim] = n;
+    return P3M_OK;
+}
+
+int p3m_batch_initialize_acceleration(p3m_batch* b) {
+    if (!b) return P3M_ERR_INVALID_ARGUMENT;
+    cudaError_t e = cudaStreamSynchronize(b->stream);
+    if (e != cudaSuccess) return batch_fail(b, P3M_ERR_CUDA, cudaGetErrorString(e));
+    for (size_t i = 0; i < b->sims.size(); ++i) {
+        int st = p3m_initialize_acceleration(b->sims[i], b->n[i]);
+        if (st != P3M_OK) return batch_fail_ctx(b, i, st);
+    }
+    for (size_t i = 0; i < b->sims.size(); ++i) {
+        int st = p3m_synchronize(b->sims[i]);
+        if (st != P3M_OK) return batch_fail_ctx(b, i, st);
+    }
+    return P3M_OK;
+}
+
+int p3m_batch_step(p3m_batch* b, int32_t steps) {
+    if (!b) return P3M_ERR_INVALID_ARGUMENT;
+    if (steps < 0) return batch_fail(b, P3M_ERR_INVALID_ARGUMENT, "steps must be >= 0");
+    for (int32_t s = 0; s < steps; ++s) {
+        int st = batch_one_step(b);
+        if (st != P3M_OK) return st;
+    }
+    return P3M_OK;
+}
+
+int p3m_batch_autotune(p3m_batch* b, int32_t trial_steps, int32_t* chosen) {
+    if (!b) return P3M_ERR_INVALID_ARGUMENT;
+    if (trial_steps <= 0) return batch_fail(b, P3M_ERR_INVALID_ARGUMENT, "trial_steps must be > 0");
+    cudaError_t e = cudaStreamSynchronize(b->stream);
+    if (e != cudaSuccess) return batch_fail(b, P3M_ERR_CUDA, cudaGetErrorString(e));
+    batch_drop_graphs(b);
+    // One probe per distinct grid: the simulation with the most bodies.
+    std::vector<size_t> probes;
+    for (size_t i = 0; i < b->sims.size(); ++i) {
+        const p3m_ctx* c = b->sims[i];
+        bool placed = false;
+        for (size_t& p : probes) {
+            const p3m_ctx* q = b->sims[p];
+            if (q->grid.W == c->grid.W && q->grid.H == c->grid.H && q->bounded == c->bounded) {
+                if (b->n[i] > b->n[p]) p = i;
+                placed = true;
+                break;
+            }
+        }
+        if (!placed) probes.push_back(i);
+    }
+    const int fft_choices[] = {0, 1, 2, 4, 8};
+    const int sr_choices[] = {64, 128, 256};
+    int tuned = 0;
+    for (size_t p : probes) {
+        p3m_ctx* c = b->sims[p];
+        const int n = b->n[p];
+        const size_t cap = (size_t)c->cfg.capacity;
+        // The trials step the probe; its state is put back afterwards.
+        float4 *sb = nullptr, *sm = nullptr;
+        float2* sa = nullptr;
+        const long long steps_before = c->physics_steps;
+        P3M_CUDA(c, cudaMallocAsync((void**)&sb, cap * sizeof(float4), c->stream));
+        P3M_CUDA(c, cudaMallocAsync((void**)&sm, cap * sizeof(float4), c->stream));
+        P3M_CUDA(c, cudaMallocAsync((void**)&sa, cap * sizeof(float2), c->stream));
+        P3M_CUDA(c, cudaMemcpyAsync(sb, c->bodies, cap * sizeof(float4), cudaMemcpyDeviceToDevice, c->stream));
+        P3M_CUDA(c, cudaMemcpyAsync(sm, c->materials, cap * sizeof(float4), cudaMemcpyDeviceToDevice, c->stream));
+        P3M_CUDA(c, cudaMemcpyAsync(sa, c->accel, cap * sizeof(float2), cudaMemcpyDeviceToDevice, c->stream));
+        auto trial = [&](float* ms) -> int {
+            c->grid = grid_for(c);
+            int st = time_direct_steps(c, n, 1, ms);  // warm-up
+            if (st == P3M_OK) st = time_direct_steps(c, n, trial_steps, ms);
+            return st;
+        };
+        int best_fft = 0, best_sr = 256;
+        float best = 3.4e38f, ms = 0.0f;
+        c->tune_sr_threads = 256;
+        for (int f : fft_choices) {
+            c->tune_fft_lines = f;
+            int st = trial(&ms);
+            if (st != P3M_OK) return batch_fail_ctx(b, p, st);
+            if (ms < best) { best = ms; best_fft = f; }
+        }
+        c->tune_fft_lines = best_fft;
+        best = 3.4e38f;
+        for (int t : sr_choices) {
+            c->tune_sr_threads = t;
+            int st = trial(&ms);
+            if (st != P3M_OK) return batch_fail_ctx(b, p, st);
+            if (ms < best) { best = ms; best_sr = t; }
+        }
+        // Put the probe's state back (the buffer roles may have swapped).
+        P3M_CUDA(c, cudaMemcpyAsync(c->bodies, sb, cap * sizeof(float4), cudaMemcpyDeviceToDevice, c->stream));
+        P3M_CUDA(c, cudaMemcpyAsync(c->materials, sm, cap * sizeof(float4), cudaMemcpyDeviceToDevice, c->stream));
+        P3M_CUDA(c, cudaMemcpyAsync(c->accel, sa, cap * sizeof(float2), cudaMemcpyDeviceToDevice, c->stream));
+        cudaFreeAsync(sb, c->stream);
+        cudaFreeAsync(sm, c->stream);
+        cudaFreeAsync(sa, c->stream);
+        P3M_CUDA(c, cudaStreamSynchronize(c->stream));
+        c->physics_steps = steps_before;
+        for (size_t i = 0; i < b->sims.size(); ++i) {
+            p3m_ctx* o = b->sims[i];
+            if (o->grid.W == c->grid.W && o->grid.H == c->grid.H && o->bounded == c->bounded) {
+                o->tune_fft_lines = best_fft;
+                o->tune_sr_threads = best_sr;
+                o->grid = grid_for(o);
+                drop_graphs(o);
+            }
+        }
+        if (chosen && tuned < 64) {
+            chosen[4 * tuned + 0] = c->grid.W;
+            chosen[4 * tuned + 1] = c->grid.H;
+            chosen[4 * tuned + 2] = best_fft;
+            chosen[4 * tuned + 3] = best_sr;
+        }
+        ++tuned;
+    }
+    return P3M_OK;
+}
+
+int p3m_batch_synchronize(p3m_batch* b) {
+    if (!b) return P3M_ERR_INVALID_ARGUMENT;
+    cudaError_t e = cudaStreamSynchronize(b->stream);
+    if (e != cudaSuccess) return batch_fail(b, P3M_ERR_CUDA, cudaGetErrorString(e));
+    return P3M_OK;
+}
+
+int p3m_batch_get_stream(p3m_batch* b, void** stream) {
+    if (!b || !stream) return P3M_ERR_INVALID_ARGUMENT;
+    *stream = (void*)b->stream;
     return P3M_OK;
 }
 

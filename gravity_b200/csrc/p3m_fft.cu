@@ -359,8 +359,8 @@ cudaError_t set_smem(const void* fn, size_t bytes) {
 // Lines per CTA: enough CTAs for two per SM (296) when there are that many
 // lines, at most `cap`; threads: one radix-8 butterfly per thread and pass,
 // 64..256.
-void line_shape(int lines_total, int L, int cap, int* per_cta, int* threads) {
-    int g = lines_total / 296;
+void line_shape(int lines_total, int L, int cap, int* per_cta, int* threads, int fixed = 0) {
+    int g = fixed > 0 ? fixed : lines_total / 296;
     if (g > cap) g = cap;
     if (g < 1) g = 1;
     *per_cta = g;
@@ -370,11 +370,11 @@ void line_shape(int lines_total, int L, int cap, int* per_cta, int* threads) {
 
 // Columns per CTA of the column kernels: at most 16 and at most what 128 KB
 // of shared memory holds.
-void column_shape(int MW, int MH, int lines_factor, int* G, int* threads) {
+void column_shape(int MW, int MH, int lines_factor, int* G, int* threads, int fixed) {
     const int SW = MW / 2 + 1;
     int cap = (128 * 1024) / (lines_factor * MH * (int)sizeof(float2));
     if (cap > 16) cap = 16;
-    line_shape(SW, MH, cap, G, threads);
+    line_shape(SW, MH, cap, G, threads, fixed);
 }
 
 }  // namespace
@@ -406,7 +406,7 @@ cudaError_t launch_fft_forward_rows(const void* density, int deposit_mode, float
                                     cudaStream_t stream) {
     const int pairs = g.MH / 2;
     int pairs_per_cta, threads;
-    line_shape(pairs, g.MW, g.MW >= 4096 ? 1 : 4096 / g.MW, &pairs_per_cta, &threads);
+    line_shape(pairs, g.MW, g.MW >= 4096 ? 1 : 4096 / g.MW, &pairs_per_cta, &threads, g.fft_lines);
     const int blocks = (pairs + pairs_per_cta - 1) / pairs_per_cta;
     const size_t smem = (size_t)2 * pairs_per_cta * g.MW * sizeof(float2);
     if (deposit_mode == P3M_DEPOSIT_I64) {
@@ -426,7 +426,7 @@ cudaError_t launch_fft_columns(const float2* half, const float2* green, float in
                                GridShape g, const float2* twiddles, float4* cols,
                                cudaStream_t stream) {
     int G, threads;
-    column_shape(g.MW, g.MH, 4, &G, &threads);
+    column_shape(g.MW, g.MH, 4, &G, &threads, g.fft_lines);
     const int SW = g.MW / 2 + 1;
     const int blocks = (SW + G - 1) / G;
     const size_t smem = (size_t)4 * G * g.MH * sizeof(float2);
@@ -439,7 +439,7 @@ cudaError_t launch_fft_columns(const float2* half, const float2* green, float in
 cudaError_t launch_fft_forward_columns(float2* half, GridShape g, const float2* twiddles,
                                        cudaStream_t stream) {
     int G, threads;
-    column_shape(g.MW, g.MH, 2, &G, &threads);
+    column_shape(g.MW, g.MH, 2, &G, &threads, g.fft_lines);
     const int SW = g.MW / 2 + 1;
     const int blocks = (SW + G - 1) / G;
     const size_t smem = (size_t)2 * G * g.MH * sizeof(float2);
@@ -451,7 +451,7 @@ cudaError_t launch_fft_forward_columns(float2* half, GridShape g, const float2* 
 cudaError_t launch_fft_inverse_rows(const float4* cols, GridShape g, const float2* twiddles,
                                     float2* force, cudaStream_t stream) {
     int rows_per_cta, threads;
-    line_shape(g.MH, g.MW, g.MW >= 4096 ? 1 : 4096 / g.MW, &rows_per_cta, &threads);
+    line_shape(g.MH, g.MW, g.MW >= 4096 ? 1 : 4096 / g.MW, &rows_per_cta, &threads, g.fft_lines);
     const int blocks = (g.MH + rows_per_cta - 1) / rows_per_cta;
     const size_t smem = (size_t)2 * rows_per_cta * g.MW * sizeof(float2);
     fft_rows_inverse_kernel<<<blocks, threads, smem, stream>>>(cols, g.MW, g.MH, rows_per_cta,

@@ -100,6 +100,7 @@ struct GridShape {
     int W, H;     // physical grid
     int MW, MH;   // mesh (= physical on the torus, 2x on walls)
     int bounded;
+    int fft_lines = 0;  // lines per CTA of the FFT kernels; 0 = automatic
 };
 
 // Half kick + drift substeps (collision_build.comp:40-51), then the home-cell
@@ -152,6 +153,7 @@ cudaError_t build_green(GridShape g, GreenParams p, double2* work, float2* green
 // Interpolation + short range + half kick (kick.comp:66-156).
 struct KickParams {
     int n, W, H, MW, MH, bounded, rx, ry, exact, home_limit, initial, mutual;
+    int sr_threads;  // block size of the short-range kernel (64..256)
     float aspect, gravity, sigma_cells, total_mass, min_frac, dt, field_x, field_y;
 };
 // Short-range correction over the cell stencil (kick.comp:122-151), one
@@ -230,6 +232,8 @@ struct p3m_ctx {
     int mass_scale = 1;
     long long physics_steps = 0;
     int green_bounded = -1;  // which mesh the Green's table was built for
+    int tune_fft_lines = 0;  // launch shapes chosen by the batch autotuner
+    int tune_sr_threads = 256;
 
     // body state
     float4* bodies = nullptr;

@@ -175,7 +175,8 @@ P3M_DECLARE_SHORT_RANGE_RX(6)
                                            const int* cell_start, const int* cell_count,        \
                                            const uint32_t* cell_mass, float2* a_short,          \
                                            const KickParams& p, cudaStream_t stream) {          \
-        const dim3 grid((p.n + 255) / 256), block(256);                                         \
+        const int threads_ = p.sr_threads > 0 ? p.sr_threads : 256;                               \
+        const dim3 grid((p.n + threads_ - 1) / threads_), block(threads_);                      \
         switch (p.ry * 2 + (p.exact == 2 ? 1 : 0)) {                                            \
             case 3: sr::short_range_kernel<RX_, 1, 2><<<grid, block, 0, stream>>>(bodies, entries, cell_start, cell_count, cell_mass, a_short, p); break; \
             case 2: sr::short_range_kernel<RX_, 1, 0><<<grid, block, 0, stream>>>(bodies, entries, cell_start, cell_count, cell_mass, a_short, p); break; \

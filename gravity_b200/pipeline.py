@@ -51,6 +51,22 @@ class GravityPipeline:
         self._mutual = bool(self.config.mutual_gravity)
         self._field = (0.0, 0.0)
         self._mass_excess = 0.0
+        self._owned = True
+
+    @classmethod
+    def borrow(cls, handle: ctypes.c_void_p, config: P3MConfig) -> "GravityPipeline":
+        """A view of a context owned elsewhere (a simulation of a batch);
+        closing the view leaves the context alive."""
+        self = cls.__new__(cls)
+        self.config = config
+        self._lib = _abi.load()
+        self._ctx = handle
+        self._bounded = bool(config.bounded)
+        self._mutual = bool(config.mutual_gravity)
+        self._field = (0.0, 0.0)
+        self._mass_excess = 0.0
+        self._owned = False
+        return self
 
     # ------------------------------------------------------------ plumbing
     def _check(self, rc: int) -> None:
@@ -63,9 +79,9 @@ class GravityPipeline:
         return self._ctx
 
     def close(self) -> None:
-        if self._ctx:
+        if self._ctx and getattr(self, "_owned", True):
             self._lib.p3m_destroy(self._ctx)
-            self._ctx = ctypes.c_void_p()
+        self._ctx = ctypes.c_void_p()
 
     def __enter__(self) -> "GravityPipeline":
         return self

@@ -234,6 +234,44 @@ int p3m_direct_accel_f64(p3m_ctx* ctx, int32_t n, const int32_t* targets, int32_
  * out[3..4] centre of mass, out[5] total mass. Deterministic reduction. */
 int p3m_diagnostics_f64(p3m_ctx* ctx, int32_t n, double* out6);
 
+/* ---- batched form ------------------------------------------------------- */
+
+/* Many independent simulations of uneven body counts and grid sizes — the
+ * application's trajectory previews (trajectory.comp, GravityPipeline.kt:
+ * 514-600) and ensembles — stepped together: each simulation is a full
+ * context, and one batch step is one CUDA graph that forks to every
+ * simulation's stream, runs its step and joins (captured once per set of body
+ * counts, reorder phases, buffers and uniforms, then replayed). The
+ * reference runs one simulation per GravityPipeline. */
+typedef struct p3m_batch p3m_batch;
+
+/* count configurations, one per simulation. */
+int p3m_batch_create(const p3m_config* configs, int32_t count, p3m_batch** out);
+int p3m_batch_destroy(p3m_batch* batch);
+/* Message of the last failing batch call (or of p3m_batch_create when NULL). */
+const char* p3m_batch_last_error(const p3m_batch* batch);
+int p3m_batch_size(const p3m_batch* batch, int32_t* count);
+/* The context of one simulation (for downloads, diagnostics, debug reads;
+ * its stream is ordered after the batch's only through p3m_batch_synchronize). */
+int p3m_batch_context(p3m_batch* batch, int32_t sim, p3m_ctx** ctx);
+/* Upload n bodies (and materials, may be NULL) and make them simulation
+ * sim's active bodies. */
+int p3m_batch_upload(p3m_batch* batch, int32_t sim, const float* bodies4,
+                     const float* materials4, int32_t n);
+/* initializeAcceleration of every simulation. */
+int p3m_batch_initialize_acceleration(p3m_batch* batch);
+/* `steps` steps of every simulation, one graph launch per step. */
+int p3m_batch_step(p3m_batch* batch, int32_t steps);
+/* Autotuner: for each distinct grid, times `trial_steps` steps of its largest
+ * simulation under each candidate launch shape (FFT lines per CTA: automatic,
+ * 1, 2, 4, 8; short-range block: 64, 128, 256 threads), keeps the fastest for
+ * every simulation on that grid and restores the probe's state. Writes up to
+ * 64 rows of (grid_width, grid_height, fft_lines, short_range_threads) to
+ * `chosen` when it is not NULL. Results do not depend on the shapes. */
+int p3m_batch_autotune(p3m_batch* batch, int32_t trial_steps, int32_t* chosen);
+int p3m_batch_synchronize(p3m_batch* batch);
+int p3m_batch_get_stream(p3m_batch* batch, void** stream);
+
 /* ---- cell lists without allocation ------------------------------------- */
 
 /* No counterpart in the reference. For callers that cannot allocate device

@@ -1,0 +1,94 @@
+"""The batched form (p3m_batch_*) against simulations stepped one by one.
+
+A batch step is one CUDA graph over every simulation's stream; each
+simulation must come out bit for bit as the same simulation stepped alone in
+its own context, before and after the autotuner changes launch shapes, and
+across the reorder phases (a batch cycles through several captured graphs).
+"""
+
+from dataclasses import replace
+
+import numpy as np
+import pytest
+
+from gravity_b200 import scenarios
+from gravity_b200.batch import GravityBatch
+from gravity_b200.pipeline import GravityPipeline
+
+pytestmark = pytest.mark.gpu
+
+
+def mixed_batch():
+    scs = scenarios.batch(sims=7, seed=21, nmin=300, nmax=9000)
+    # One simulation with walls, one with a field, one without mutual gravity.
+    scs[1] = replace(scs[1], config=scs[1].config.with_(bounded=True))
+    scs[3] = replace(scs[3], config=scs[3].config.with_(mutual_gravity=False))
+    return scs
+
+
+def step_alone(sc, steps, field=(0.0, 0.0)):
+    with GravityPipeline(sc.config) as p:
+        p.upload(sc.bodies, sc.materials)
+        if field != (0.0, 0.0):
+            p.set_field_acceleration(*field)
+        p.initialize_acceleration(sc.n)
+        p.step(sc.n, steps)
+        return p.download(sc.n)
+
+
+def assert_same(got, want, what):
+    for g, w, name in zip(got, want, ("bodies", "materials", "acceleration")):
+        np.testing.assert_array_equal(g, w, err_msg=f"{what}: {name}")
+
+
+def test_batch_matches_individual_steps(cuda_device):
+    scs = mixed_batch()
+    field = (0.0, 3.5)
+    with GravityBatch([sc.config for sc in scs]) as batch:
+        for i, sc in enumerate(scs):
+            batch.upload(i, sc.bodies, sc.materials)
+        batch.simulation(5).set_field_acceleration(*field)
+        batch.initialize_acceleration()
+        batch.step(5)
+        for i, sc in enumerate(scs):
+            want = step_alone(sc, 5, field if i == 5 else (0.0, 0.0))
+            assert_same(batch.download(i), want, f"simulation {i}")
+
+
+def test_batch_after_autotune_is_unchanged(cuda_device):
+    scs = mixed_batch()
+    with GravityBatch([sc.config for sc in scs]) as batch:
+        for i, sc in enumerate(scs):
+            batch.upload(i, sc.bodies, sc.materials)
+        batch.initialize_acceleration()
+        batch.step(3)
+        rows = batch.autotune(trial_steps=2)
+        grids = {(sc.config.gravity.grid_width, sc.config.gravity.grid_height) for sc in scs}
+        assert {(r[0], r[1]) for r in rows} == grids
+        assert all(r[2] in (0, 1, 2, 4, 8) and r[3] in (64, 128, 256) for r in rows)
+        batch.step(4)
+        for i, sc in enumerate(scs):
+            assert_same(batch.download(i), step_alone(sc, 7), f"simulation {i}")
+
+
+def test_batch_with_an_empty_simulation(cuda_device):
+    scs = scenarios.batch(sims=3, seed=5, nmin=200, nmax=2000)
+    with GravityBatch([sc.config for sc in scs]) as batch:
+        for i, sc in enumerate(scs):
+            if i != 1:
+                batch.upload(i, sc.bodies, sc.materials)
+        batch.initialize_acceleration()
+        batch.step(3)
+        for i in (0, 2):
+            assert_same(batch.download(i), step_alone(scs[i], 3), f"simulation {i}")
+
+
+def test_batch_rejects_bad_arguments(cuda_device):
+    scs = scenarios.batch(sims=2, seed=6, nmin=100, nmax=200)
+    with GravityBatch([sc.config for sc in scs]) as batch:
+        with pytest.raises(ValueError):
+            batch.upload(2, scs[0].bodies)
+        with pytest.raises(ValueError):
+            batch.step(-1)
+        with pytest.raises(ValueError):
+            batch.upload(0, np.zeros((scs[0].config.capacity + 1, 4), np.float32))
