@@ -69,6 +69,8 @@ def make_workload(name: str):
         return scenarios.lattice_scale()
     if name == "batch":
         return scenarios.batch()
+    if name == "adjoint":
+        return scenarios.adjoint_cluster()
     if name == "lattice_scale_u32":
         from gravity_b200 import _abi
         return scenarios.lattice_scale(deposit_mode=_abi.P3M_DEPOSIT_U32)
@@ -679,6 +681,198 @@ def run_batch(args, ws, rank, local):
         dist.destroy_process_group()
 
 
+ADJOINT_GROUP = slice(99_000, 100_000)   # the projectile disc
+ADJOINT_V0_PX = (-60.0, 45.0)             # launch velocity, px/s
+ADJOINT_TARGET_PX = (1900.0, 760.0)       # target of the disc's centroid, px
+ADJOINT_INTERVAL = 16
+ADJOINT_FD_H = 1e-2                       # px/s
+
+
+def run_adjoint(args, ws, rank, local):
+    """Forward (checkpointed) + backward of the T-step rollout; value =
+    differentiated bodies*steps/s. Also the plain forward's rate, the
+    backward/forward cost ratio, the launch-velocity gradient against central
+    differences, and (with --fp64-check) against the FP64 reference."""
+    import torch
+
+    from gravity_b200.adjoint import Rollout, launch_velocity_objective
+    from gravity_b200.pipeline import GravityPipeline, PinnedArray, kernel_launches
+
+    dist = init_dist(ws, local)
+    torch.cuda.set_device(local)
+    sc = make_workload("adjoint")
+    n, T = sc.n, sc.steps
+    group = np.arange(n)[ADJOINT_GROUP]
+    base = sc.bodies.copy()
+    base[group, 2] = ADJOINT_V0_PX[0] / sc.config.viewport_width
+    base[group, 3] = ADJOINT_V0_PX[1] / sc.config.viewport_height
+    pipe = GravityPipeline(sc.config)
+    pipe.upload(base, sc.materials)
+    stream = torch.cuda.ExternalStream(pipe.stream_handle())
+    roll = Rollout(pipe, n, T, checkpoint_interval=ADJOINT_INTERVAL)
+    x0 = torch.tensor(base, device="cuda")
+    seed = torch.zeros((n, 4), dtype=torch.float32, device="cuda")
+    seed[group, 0] = 1.0
+    grad = torch.empty_like(seed)
+    final = torch.empty_like(seed)
+    flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device="cuda")
+
+    def plain_forward():
+        pipe.initialize_acceleration(n)
+        pipe.step(n, T)
+
+    # ---- plain forward: initializeAcceleration + T steps, device-timed
+    for _ in range(args.warmup):
+        pipe.upload(base)
+        plain_forward()
+    pipe.synchronize()
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+    fwd_ms = []
+    for _ in range(max(3, min(args.steps, 10))):
+        pipe.upload(base)
+        with torch.cuda.stream(stream):
+            flush.zero_()
+            ev[0].record(stream)
+        plain_forward()
+        with torch.cuda.stream(stream):
+            ev[1].record(stream)
+        torch.cuda.synchronize()
+        fwd_ms.append(ev[0].elapsed_time(ev[1]))
+    plain_ms = statistics.median(fwd_ms)
+
+    # ---- value: forward with checkpoints + backward, device-resident
+    for _ in range(args.warmup):
+        roll.forward(x0, final)
+        roll.backward(seed, out=grad)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    clocks = ClockSampler(local)
+    clocks.start()
+    time.sleep(0.3)
+    launches0 = kernel_launches()
+    f_ms, b_ms = [], []
+    for _ in range(args.steps):
+        with torch.cuda.stream(stream):
+            flush.zero_()
+            ev[0].record(stream)
+        roll.forward(x0, final)
+        with torch.cuda.stream(stream):
+            ev[1].record(stream)
+        roll.backward(seed, out=grad)
+        with torch.cuda.stream(stream):
+            ev[2].record(stream)
+        torch.cuda.synchronize()
+        f_ms.append(ev[0].elapsed_time(ev[1]))
+        b_ms.append(ev[1].elapsed_time(ev[2]))
+    launches = kernel_launches() - launches0
+    clk = clocks.stop()
+    total_ms = allreduce_max(dist, sum(f_ms) + sum(b_ms))
+    value = ws * n * T * args.steps / (total_ms / 1000.0)
+
+    # ---- e2e: host initial state in, host gradient out
+    hb = PinnedArray((n, 4))
+    hs = PinnedArray((n, 4))
+    hg = PinnedArray((n, 4))
+    hf = PinnedArray((n, 4))
+    hb.array[:] = base
+    hs.array[:] = seed.cpu().numpy()
+    e2e_steps = max(1, min(args.steps, args.e2e_steps or args.steps))
+    e2e_s = 0.0
+    for it in range(1 + e2e_steps):
+        t0 = time.perf_counter()
+        roll.forward(hb.array, hf.array)
+        roll.backward(hs.array, out=hg.array)
+        if it > 0:
+            e2e_s += time.perf_counter() - t0
+    e2e_s = allreduce_max(dist, e2e_s)
+    e2e_value = ws * n * T * e2e_steps / e2e_s
+
+    # ---- gradient checks on the launch velocity
+    v0 = np.array(ADJOINT_V0_PX)
+    obj = launch_velocity_objective(roll, sc.bodies, group, v0, ADJOINT_TARGET_PX)
+    def central(h):
+        out = []
+        for k in range(2):
+            e = np.zeros(2)
+            e[k] = h
+            lp = launch_velocity_objective(roll, sc.bodies, group, v0 + e, ADJOINT_TARGET_PX, False).loss
+            lm = launch_velocity_objective(roll, sc.bodies, group, v0 - e, ADJOINT_TARGET_PX, False).loss
+            out.append((lp - lm) / (2 * h))
+        return np.array(out)
+
+    fd = central(ADJOINT_FD_H)
+    fd_err = float(np.linalg.norm(obj.grad_velocity_px - fd) / np.linalg.norm(fd))
+    # The quotient at neighbouring steps: where they disagree with each
+    # other the loss is not smooth at that scale.
+    fd_spread = {str(h): central(h).tolist() for h in (1e-1, 1e-3)}
+    fp64 = None
+    if args.fp64_check and rank == 0:
+        import oracle
+
+        ref = oracle.Adjoint64(sc.config, sc.materials)
+        b = sc.bodies.astype(np.float64)
+        b[group, 2] = v0[0] / sc.config.viewport_width
+        b[group, 3] = v0[1] / sc.config.viewport_height
+        t0 = time.perf_counter()
+        fin, _ = ref.forward(b, T)
+        scale = np.array([sc.config.viewport_width, sc.config.viewport_height], np.float64)
+        d = fin[group, :2] - b[group, :2]
+        d -= np.round(d)
+        c = (b[group, :2] + d).mean(axis=0) * scale
+        s64 = np.zeros((n, 4))
+        s64[group, 0] = 2 * (c[0] - ADJOINT_TARGET_PX[0]) * scale[0] / len(group)
+        s64[group, 1] = 2 * (c[1] - ADJOINT_TARGET_PX[1]) * scale[1] / len(group)
+        g64, _ = ref.backward(s64)
+        gv64 = np.array([g64[group, 2].sum() / scale[0], g64[group, 3].sum() / scale[1]])
+        g = obj.grad_bodies.astype(np.float64)
+        fp64 = {"launch_velocity_rel_err": float(np.linalg.norm(obj.grad_velocity_px - gv64) / np.linalg.norm(gv64)),
+                "all_bodies_rel_err": float(np.linalg.norm(g - g64) / np.linalg.norm(g64)),
+                "grad_velocity_px_fp64": gv64.tolist(), "host_seconds": time.perf_counter() - t0}
+    for a in (hb, hs, hg, hf):
+        a.free()
+
+    if rank == 0:
+        peak, peak_kind = measured_peaks()
+        f_avg, b_avg = statistics.mean(f_ms), statistics.mean(b_ms)
+        cpu = None
+        if not args.no_cpu_baseline:
+            rate, steps, el, used = cpu_oracle_rate(sc, args.cpu_seconds, threads=os.cpu_count())
+            cpu = {"value": rate, "unit": UNIT, "cores": used, "kind": "port",
+                   "sample": f"{steps} plain P3M steps of the {n}-body adjoint workload ({el:.1f} s); "
+                             f"the reference has no adjoint"}
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": (sum(f_ms) + sum(b_ms)) / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic",
+            "config": {"workload": "adjoint", "n_bodies": n, "rollout_steps": T,
+                       "checkpoint_interval": ADJOINT_INTERVAL, "grid": "1024x512",
+                       "boundary": "torus", "viewport_px": "2560x1440",
+                       "step": "one forward rollout with checkpoints + its backward",
+                       "l2": "flushed (256 MiB write) before every timed step",
+                       "parallelism": "replicas" if args.gpus > 1 else "single"},
+            "adjoint": {"plain_forward_ms": plain_ms, "checkpointed_forward_ms": f_avg,
+                        "backward_ms": b_avg, "backward_over_plain_forward": b_avg / plain_ms,
+                        "launch_velocity_px": list(ADJOINT_V0_PX), "target_px": list(ADJOINT_TARGET_PX),
+                        "loss_px2": obj.loss, "grad_velocity_px": obj.grad_velocity_px.tolist(),
+                        "fd_grad_velocity_px": fd.tolist(), "fd_h_px_per_s": ADJOINT_FD_H,
+                        "fd_rel_err": fd_err, "fd_grad_other_h": fd_spread,
+                        "fp64_reference": fp64},
+            "roofline": None,
+            "cpu_baseline": cpu,
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 32 * n,
+                    "d2h_bytes_per_step": 32 * n, "steps": e2e_steps},
+            "gpu_launches": launches,
+            "clocks": clk,
+        }
+        print(json.dumps(line), flush=True)
+    pipe.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
 def main():
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     ap.add_argument("--gpus", type=int, default=1)
@@ -687,7 +881,9 @@ def main():
     ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
     ap.add_argument("--workload", default="plummer_walls",
                     choices=["plummer_walls", "uniform_torus", "lattice_scale", "lattice_scale_u32",
-                             "batch"])
+                             "batch", "adjoint"])
+    ap.add_argument("--fp64-check", action="store_true",
+                    help="adjoint workload: also run the FP64 reference adjoint on the host")
     ap.add_argument("--e2e-steps", type=int, default=None)
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -700,6 +896,9 @@ def main():
         return
     if args.workload == "batch":
         run_batch(args, ws, rank, local)
+        return
+    if args.workload == "adjoint":
+        run_adjoint(args, ws, rank, local)
         return
     run_b200(args, ws, rank, local)
 

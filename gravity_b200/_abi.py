@@ -24,6 +24,8 @@ P3M_ERR_CAPACITY = -6
 P3M_ERR_UNSUPPORTED = -7
 P3M_ERR_STATE = -8
 
+P3M_ADJOINT_INITIAL_ACCELERATION = 1
+
 P3M_DEPOSIT_U32 = 0
 P3M_DEPOSIT_I64 = 1
 
@@ -118,6 +120,9 @@ SIGNATURES = {
     "p3m_batch_autotune": (ctypes.c_int, [_vp, _i32, _vp]),
     "p3m_batch_synchronize": (ctypes.c_int, [_vp]),
     "p3m_batch_get_stream": (ctypes.c_int, [_vp, ctypes.POINTER(_vp)]),
+    "p3m_adjoint_forward": (ctypes.c_int, [_vp, _i32, _i32, _i32, _i32]),
+    "p3m_adjoint_backward": (ctypes.c_int, [_vp, _vp, _vp, _vp, _vp]),
+    "p3m_adjoint_release": (ctypes.c_int, [_vp]),
     "p3m_cell_lists_static": (ctypes.c_int, [_vp, _vp, _i32, _i32, _i32, _vp, _vp, _vp, _vp,
                                              _vp, _vp, _vp]),
 }

@@ -197,7 +197,10 @@ int dalloc(p3m_ctx* ctx, T** p, size_t count, const char* what) {
     return P3M_OK;
 }
 
+void adjoint_free(p3m_ctx* ctx);
+
 void free_all(p3m_ctx* ctx) {
+    adjoint_free(ctx);
     fold_stages(ctx);
     for (auto& g : ctx->graphs) cudaGraphExecDestroy(g.exec);
     ctx->graphs.clear();
@@ -665,11 +668,11 @@ int p3m_upload_state(p3m_ctx* ctx, const float* bodies4, const float* materials4
     int st = check_n(ctx, n);
     if (st != P3M_OK) return st;
     if (bodies4)
-        P3M_CUDA(ctx, cudaMemcpyAsync(ctx->bodies, bodies4, (size_t)n * 16, cudaMemcpyHostToDevice, ctx->stream));
+        P3M_CUDA(ctx, cudaMemcpyAsync(ctx->bodies, bodies4, (size_t)n * 16, cudaMemcpyDefault, ctx->stream));
     if (materials4)
-        P3M_CUDA(ctx, cudaMemcpyAsync(ctx->materials, materials4, (size_t)n * 16, cudaMemcpyHostToDevice, ctx->stream));
+        P3M_CUDA(ctx, cudaMemcpyAsync(ctx->materials, materials4, (size_t)n * 16, cudaMemcpyDefault, ctx->stream));
     if (acceleration2)
-        P3M_CUDA(ctx, cudaMemcpyAsync(ctx->accel, acceleration2, (size_t)n * 8, cudaMemcpyHostToDevice, ctx->stream));
+        P3M_CUDA(ctx, cudaMemcpyAsync(ctx->accel, acceleration2, (size_t)n * 8, cudaMemcpyDefault, ctx->stream));
     // Host arrays belong to the caller: finish reading them before returning.
     P3M_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
     return P3M_OK;
@@ -682,11 +685,11 @@ int p3m_upload_range(p3m_ctx* ctx, int32_t first, int32_t count, const float* bo
     if ((long long)first + count > ctx->cfg.capacity)
         return fail(ctx, P3M_ERR_CAPACITY, "range exceeds capacity");
     if (bodies4)
-        P3M_CUDA(ctx, cudaMemcpyAsync(ctx->bodies + first, bodies4, (size_t)count * 16, cudaMemcpyHostToDevice, ctx->stream));
+        P3M_CUDA(ctx, cudaMemcpyAsync(ctx->bodies + first, bodies4, (size_t)count * 16, cudaMemcpyDefault, ctx->stream));
     if (materials4)
-        P3M_CUDA(ctx, cudaMemcpyAsync(ctx->materials + first, materials4, (size_t)count * 16, cudaMemcpyHostToDevice, ctx->stream));
+        P3M_CUDA(ctx, cudaMemcpyAsync(ctx->materials + first, materials4, (size_t)count * 16, cudaMemcpyDefault, ctx->stream));
     if (acceleration2)
-        P3M_CUDA(ctx, cudaMemcpyAsync(ctx->accel + first, acceleration2, (size_t)count * 8, cudaMemcpyHostToDevice, ctx->stream));
+        P3M_CUDA(ctx, cudaMemcpyAsync(ctx->accel + first, acceleration2, (size_t)count * 8, cudaMemcpyDefault, ctx->stream));
     P3M_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
     return P3M_OK;
 }
@@ -696,11 +699,11 @@ int p3m_download_state(p3m_ctx* ctx, float* bodies4, float* materials4, float* a
     int st = check_n(ctx, n);
     if (st != P3M_OK) return st;
     if (bodies4)
-        P3M_CUDA(ctx, cudaMemcpyAsync(bodies4, ctx->bodies, (size_t)n * 16, cudaMemcpyDeviceToHost, ctx->stream));
+        P3M_CUDA(ctx, cudaMemcpyAsync(bodies4, ctx->bodies, (size_t)n * 16, cudaMemcpyDefault, ctx->stream));
     if (materials4)
-        P3M_CUDA(ctx, cudaMemcpyAsync(materials4, ctx->materials, (size_t)n * 16, cudaMemcpyDeviceToHost, ctx->stream));
+        P3M_CUDA(ctx, cudaMemcpyAsync(materials4, ctx->materials, (size_t)n * 16, cudaMemcpyDefault, ctx->stream));
     if (acceleration2)
-        P3M_CUDA(ctx, cudaMemcpyAsync(acceleration2, ctx->accel, (size_t)n * 8, cudaMemcpyDeviceToHost, ctx->stream));
+        P3M_CUDA(ctx, cudaMemcpyAsync(acceleration2, ctx->accel, (size_t)n * 8, cudaMemcpyDefault, ctx->stream));
     P3M_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
     return P3M_OK;
 }
@@ -1312,6 +1315,270 @@ int p3m_batch_synchronize(p3m_batch* b) {
 int p3m_batch_get_stream(p3m_batch* b, void** stream) {
     if (!b || !stream) return P3M_ERR_INVALID_ARGUMENT;
     *stream = (void*)b->stream;
+    return P3M_OK;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Differentiated rollout: the gravity-only step (GravityPipeline.kt:445-494
+// without collisions) run forward with checkpoints, then reversed with the
+// hand-written adjoint of p3m_adjoint.cu. The reference has no adjoint.
+//
+// Forward: `steps` plain steps (graph-replayed like p3m_step), with the
+// bodies and accelerations saved every `interval` steps. Backward: for each
+// segment from the last, the segment's checkpoint is restored and its steps
+// recomputed, keeping for every step the positions, cell lists and mesh
+// force the reverse step needs (the memory of one segment), then the steps
+// are reversed. The context's state is put back to the forward's end.
+// Memory: (steps/interval + 2) x 24 B per body of checkpoints, plus
+// (interval + 1) x (32 B per body + 12 B per cell + 8 B per mesh cell) of
+// recompute slots, plus the cotangents.
+
+struct p3m_adjoint_store {
+    int n = 0, steps = 0, interval = 0, initial = 0, slots = 0;
+    size_t P = 0, M = 0;
+    bool recorded = false;
+    std::vector<void*> blocks;
+    float4* ck_bodies = nullptr;  // [checkpoints + 1][n], the last: the final state
+    float2* ck_accel = nullptr;
+    float4* slot_bodies = nullptr;  // [slots][n]
+    float4* slot_entries = nullptr;
+    int* slot_start = nullptr;      // [slots][P]
+    int* slot_count = nullptr;
+    uint32_t* slot_mass = nullptr;
+    float2* slot_force = nullptr;   // [slots][M]
+    float4* lam = nullptr;          // cotangents of (x, y, vx, vy)
+    float2* lam_a = nullptr;        // cotangents of a
+    float2* wa = nullptr;
+    float2* g_short = nullptr;
+    float* cot = nullptr;           // 2*MH x MW
+    float2* half2 = nullptr;        // 2*MH x (MW/2+1)
+    float2* mu2 = nullptr;          // MH/2 x MW
+};
+
+namespace {
+
+void adjoint_free(p3m_ctx* ctx) {
+    if (!ctx->adjoint) return;
+    for (void* b : ctx->adjoint->blocks) cudaFree(b);
+    delete ctx->adjoint;
+    ctx->adjoint = nullptr;
+}
+
+int checkpoints_for(int steps, int interval) { return (steps + interval - 1) / interval; }
+
+template <typename T>
+int adjoint_alloc(p3m_ctx* ctx, p3m_adjoint_store* a, T** out, size_t count) {
+    void* p = nullptr;
+    cudaError_t e = cudaMalloc(&p, std::max<size_t>(count, 1) * sizeof(T));
+    if (e != cudaSuccess) return fail_cuda(ctx, "adjoint storage", e);
+    a->blocks.push_back(p);
+    *out = static_cast<T*>(p);
+    return P3M_OK;
+}
+
+int adjoint_prepare(p3m_ctx* ctx, int n, int steps, int interval) {
+    p3m_adjoint_store* a = ctx->adjoint;
+    const size_t P = phys_cells(ctx), M = mesh_cells(ctx);
+    if (a && a->n == n && a->steps == steps && a->interval == interval && a->P == P && a->M == M)
+        return P3M_OK;
+    adjoint_free(ctx);
+    a = new (std::nothrow) p3m_adjoint_store();
+    if (!a) return fail(ctx, P3M_ERR_OUT_OF_MEMORY, "host allocation failed");
+    ctx->adjoint = a;
+    a->n = n;
+    a->steps = steps;
+    a->interval = interval;
+    a->P = P;
+    a->M = M;
+    a->slots = interval + 1;
+    const size_t nn = (size_t)n, ck = (size_t)checkpoints_for(steps, interval) + 1;
+    const size_t S = (size_t)a->slots;
+    const size_t SW = (size_t)ctx->grid.MW / 2 + 1, MH = (size_t)ctx->grid.MH, MW = (size_t)ctx->grid.MW;
+    int st = P3M_OK;
+    if (st == P3M_OK) st = adjoint_alloc(ctx, a, &a->ck_bodies, ck * nn);
+    if (st == P3M_OK) st = adjoint_alloc(ctx, a, &a->ck_accel, ck * nn);
+    if (st == P3M_OK) st = adjoint_alloc(ctx, a, &a->slot_bodies, S * nn);
+    if (st == P3M_OK) st = adjoint_alloc(ctx, a, &a->slot_entries, S * nn);
+    if (st == P3M_OK) st = adjoint_alloc(ctx, a, &a->slot_start, S * P);
+    if (st == P3M_OK) st = adjoint_alloc(ctx, a, &a->slot_count, S * P);
+    if (st == P3M_OK) st = adjoint_alloc(ctx, a, &a->slot_mass, S * P);
+    if (st == P3M_OK) st = adjoint_alloc(ctx, a, &a->slot_force, S * M);
+    if (st == P3M_OK) st = adjoint_alloc(ctx, a, &a->lam, nn);
+    if (st == P3M_OK) st = adjoint_alloc(ctx, a, &a->lam_a, nn);
+    if (st == P3M_OK) st = adjoint_alloc(ctx, a, &a->wa, nn);
+    if (st == P3M_OK) st = adjoint_alloc(ctx, a, &a->g_short, nn);
+    if (st == P3M_OK) st = adjoint_alloc(ctx, a, &a->cot, 2 * MH * MW);
+    if (st == P3M_OK) st = adjoint_alloc(ctx, a, &a->half2, 2 * MH * SW);
+    if (st == P3M_OK) st = adjoint_alloc(ctx, a, &a->mu2, MH / 2 * MW);
+    if (st != P3M_OK) adjoint_free(ctx);
+    return st;
+}
+
+#define P3M_COPY(ctx, dst, src, bytes) \
+    P3M_CUDA(ctx, cudaMemcpyAsync((dst), (src), (bytes), cudaMemcpyDeviceToDevice, (ctx)->stream))
+
+// Keeps what the reverse step at the current state needs.
+int adjoint_save_slot(p3m_ctx* ctx, int slot) {
+    p3m_adjoint_store* a = ctx->adjoint;
+    const size_t n = (size_t)a->n, P = a->P, M = a->M, s = (size_t)slot;
+    P3M_COPY(ctx, a->slot_bodies + s * n, ctx->bodies, n * sizeof(float4));
+    P3M_COPY(ctx, a->slot_entries + s * n, ctx->entries, n * sizeof(float4));
+    P3M_COPY(ctx, a->slot_start + s * P, ctx->cell_start, P * sizeof(int));
+    P3M_COPY(ctx, a->slot_count + s * P, ctx->cell_count, P * sizeof(int));
+    P3M_COPY(ctx, a->slot_mass + s * P, ctx->cell_mass, P * sizeof(uint32_t));
+    P3M_COPY(ctx, a->slot_force + s * M, ctx->force, M * sizeof(float2));
+    return P3M_OK;
+}
+
+int adjoint_checkpoint(p3m_ctx* ctx, int index, bool restore) {
+    p3m_adjoint_store* a = ctx->adjoint;
+    const size_t n = (size_t)a->n, k = (size_t)index;
+    if (restore) {
+        P3M_COPY(ctx, ctx->bodies, a->ck_bodies + k * n, n * sizeof(float4));
+        P3M_COPY(ctx, ctx->accel, a->ck_accel + k * n, n * sizeof(float2));
+    } else {
+        P3M_COPY(ctx, a->ck_bodies + k * n, ctx->bodies, n * sizeof(float4));
+        P3M_COPY(ctx, a->ck_accel + k * n, ctx->accel, n * sizeof(float2));
+    }
+    return P3M_OK;
+}
+
+p3m::AdjointParams adjoint_params(const p3m_ctx* ctx, int n) {
+    p3m::AdjointParams p;
+    p.n = n;
+    p.W = ctx->grid.W; p.H = ctx->grid.H; p.MW = ctx->grid.MW; p.MH = ctx->grid.MH;
+    p.bounded = ctx->bounded; p.rx = ctx->rx; p.ry = ctx->ry;
+    p.exact = ctx->cfg.exact_neighbor_body_limit;
+    p.home_limit = ctx->cfg.maximum_home_body_interactions;
+    p.mutual = ctx->mutual;
+    p.fold = 0;
+    p.aspect = ctx->aspect; p.gravity = ctx->cfg.gravitational_constant;
+    p.sigma_cells = ctx->cfg.softening_cells; p.total_mass = ctx->normalization_mass;
+    p.min_frac = ctx->cfg.minimum_distance_cell_fraction; p.dt = ctx->cfg.time_step;
+    p.cv = 0.5f * ctx->cfg.time_step;
+    return p;
+}
+
+// One reverse step against recompute slot `slot`.
+int adjoint_reverse(p3m_ctx* ctx, int slot, const p3m::AdjointParams& p) {
+    p3m_adjoint_store* a = ctx->adjoint;
+    const size_t n = (size_t)a->n, P = a->P, M = a->M, s = (size_t)slot;
+    const float4* bodies = a->slot_bodies + s * n;
+    P3M_CUDA(ctx, cudaMemsetAsync(a->cot, 0, 2 * M * sizeof(float), ctx->stream));
+    P3M_CUDA(ctx, cudaMemsetAsync(a->g_short, 0, n * sizeof(float2), ctx->stream));
+    P3M_CUDA(ctx, p3m::launch_adjoint_spread(bodies, a->lam, a->lam_a, a->wa, a->cot, p, ctx->stream));
+    P3M_CUDA(ctx, p3m::launch_adjoint_short_range(bodies, a->slot_entries + s * n,
+                                                  a->slot_start + s * P, a->slot_count + s * P,
+                                                  a->slot_mass + s * P, a->wa, a->g_short, p,
+                                                  ctx->stream));
+    if (p.mutual)
+        P3M_CUDA(ctx, p3m::launch_fft_adjoint(a->cot, ctx->green, 1.0f / ctx->normalization_mass,
+                                              ctx->grid, ctx->twiddles, a->half2, ctx->cols,
+                                              a->mu2, ctx->stream));
+    P3M_CUDA(ctx, p3m::launch_adjoint_gather(bodies, ctx->materials, a->wa, a->mu2,
+                                             a->slot_force + s * M, a->g_short, a->lam, a->lam_a,
+                                             p, ctx->stream));
+    return P3M_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int p3m_adjoint_forward(p3m_ctx* ctx, int32_t n, int32_t steps, int32_t interval, int32_t flags) {
+    int st = check_n(ctx, n);
+    if (st != P3M_OK) return st;
+    if (steps < 1 || interval < 1) return fail(ctx, P3M_ERR_INVALID_ARGUMENT, "steps and interval must be >= 1");
+    if (n < 1) return fail(ctx, P3M_ERR_INVALID_ARGUMENT, "the rollout needs at least one body");
+    if (flags & ~P3M_ADJOINT_INITIAL_ACCELERATION) return fail(ctx, P3M_ERR_INVALID_ARGUMENT, "unknown flags");
+    if (ctx->bounded) return fail(ctx, P3M_ERR_UNSUPPORTED, "the differentiated rollout covers the torus only");
+    if (ctx->cfg.spatial_sort_interval != 0)
+        return fail(ctx, P3M_ERR_UNSUPPORTED, "the differentiated rollout keeps body order: spatial_sort_interval must be 0");
+    normalize_to(ctx, n);
+    st = ensure_green(ctx);
+    if (st != P3M_OK) return st;
+    st = adjoint_prepare(ctx, n, steps, interval);
+    if (st != P3M_OK) return st;
+    p3m_adjoint_store* a = ctx->adjoint;
+    a->recorded = false;
+    a->initial = (flags & P3M_ADJOINT_INITIAL_ACCELERATION) ? 1 : 0;
+    if (a->initial) {
+        st = p3m_initialize_acceleration(ctx, n);
+        if (st != P3M_OK) return st;
+    }
+    for (int k = 0; k < steps; ++k) {
+        if (k % interval == 0) {
+            st = adjoint_checkpoint(ctx, k / interval, false);
+            if (st != P3M_OK) return st;
+        }
+        st = one_step(ctx, n);
+        if (st != P3M_OK) return st;
+    }
+    st = adjoint_checkpoint(ctx, checkpoints_for(steps, interval), false);
+    if (st != P3M_OK) return st;
+    a->recorded = true;
+    return P3M_OK;
+}
+
+int p3m_adjoint_backward(p3m_ctx* ctx, const float* seed_bodies4, const float* seed_accel2,
+                         float* grad_bodies4, float* grad_accel2) {
+    if (!ctx || !seed_bodies4 || !grad_bodies4) return P3M_ERR_INVALID_ARGUMENT;
+    p3m_adjoint_store* a = ctx->adjoint;
+    if (!a || !a->recorded) return fail(ctx, P3M_ERR_STATE, "no recorded rollout: call p3m_adjoint_forward first");
+    const int n = a->n;
+    normalize_to(ctx, n);
+    P3M_CUDA(ctx, cudaMemcpyAsync(a->lam, seed_bodies4, (size_t)n * sizeof(float4), cudaMemcpyDefault, ctx->stream));
+    if (seed_accel2)
+        P3M_CUDA(ctx, cudaMemcpyAsync(a->lam_a, seed_accel2, (size_t)n * sizeof(float2), cudaMemcpyDefault, ctx->stream));
+    else
+        P3M_CUDA(ctx, cudaMemsetAsync(a->lam_a, 0, (size_t)n * sizeof(float2), ctx->stream));
+    const p3m::AdjointParams p = adjoint_params(ctx, n);
+    const int init_slot = a->slots - 1;
+    int st = P3M_OK;
+    for (int seg = checkpoints_for(a->steps, a->interval) - 1; seg >= 0; --seg) {
+        const int first = seg * a->interval;
+        const int count = std::min(a->interval, a->steps - first);
+        st = adjoint_checkpoint(ctx, seg, true);
+        if (st != P3M_OK) return st;
+        if (seg == 0 && a->initial && ctx->mutual) {
+            st = build_force(ctx, n);
+            if (st == P3M_OK) st = adjoint_save_slot(ctx, init_slot);
+            if (st != P3M_OK) return st;
+        }
+        for (int s = 0; s < count; ++s) {
+            st = one_step(ctx, n);
+            if (st == P3M_OK) st = adjoint_save_slot(ctx, s);
+            if (st != P3M_OK) return st;
+        }
+        for (int s = count - 1; s >= 0; --s) {
+            st = adjoint_reverse(ctx, s, p);
+            if (st != P3M_OK) return st;
+        }
+    }
+    if (a->initial && ctx->mutual) {
+        p3m::AdjointParams q = p;
+        q.cv = 0.0f;
+        q.fold = 1;
+        st = adjoint_reverse(ctx, init_slot, q);
+        if (st != P3M_OK) return st;
+    } else if (a->initial) {
+        P3M_CUDA(ctx, cudaMemsetAsync(a->lam_a, 0, (size_t)n * sizeof(float2), ctx->stream));
+    }
+    st = adjoint_checkpoint(ctx, checkpoints_for(a->steps, a->interval), true);
+    if (st != P3M_OK) return st;
+    P3M_CUDA(ctx, cudaMemcpyAsync(grad_bodies4, a->lam, (size_t)n * sizeof(float4), cudaMemcpyDefault, ctx->stream));
+    if (grad_accel2)
+        P3M_CUDA(ctx, cudaMemcpyAsync(grad_accel2, a->lam_a, (size_t)n * sizeof(float2), cudaMemcpyDefault, ctx->stream));
+    P3M_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    return P3M_OK;
+}
+
+int p3m_adjoint_release(p3m_ctx* ctx) {
+    if (!ctx) return P3M_ERR_INVALID_ARGUMENT;
+    P3M_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    adjoint_free(ctx);
     return P3M_OK;
 }
 

@@ -217,6 +217,51 @@ __global__ void __launch_bounds__(256) fft_columns_kernel(const float2* __restri
     }
 }
 
+// 2'. columns of the adjoint (transposed) mesh operator. `half` holds the
+// row spectra of the two cotangent fields interleaved by row (row 2y: X, row
+// 2y+1: Y, as fft_rows_forward_kernel leaves a field of 2*MH rows). Each
+// column of X and Y is transformed along y, combined as
+//   mu^ = Kx^T X^ + Ky^T Y^ = -(i gx X^ + i gy Y^) / M
+// (the gradient kernels are real and odd, so each transpose is the negated
+// operator), and transformed back; row y of mu^ goes to component (y & 1) of
+// the complex pair at cols[(y >> 1) * SW + kx], the layout
+// fft_rows_inverse_kernel turns into two real rows per float2.
+__global__ void __launch_bounds__(256) fft_columns_adjoint_kernel(const float2* __restrict__ half,
+                                                                  const float2* __restrict__ green,
+                                                                  float inv_total, int MW, int MH,
+                                                                  int G,
+                                                                  const float2* __restrict__ tw,
+                                                                  float2* __restrict__ cols) {
+    extern __shared__ __align__(16) float2 sm[];
+    const int SW = MW / 2 + 1;
+    const int kx0 = blockIdx.x * G;
+    const int ncols = min(G, SW - kx0);
+    const int logH = ilog2(MH);
+    float2* A = sm;               // 2G lines: X columns, then Y columns
+    float2* B = sm + 2 * G * MH;  // 2G lines
+    for (int t = threadIdx.x; t < 2 * ncols * MH; t += blockDim.x) {
+        const int row = t / ncols, c = t - row * ncols;  // row = 2y + component
+        const int y = row >> 1, comp = row & 1;
+        A[(comp * ncols + c) * MH + y] = half[(size_t)row * SW + kx0 + c];
+    }
+    __syncthreads();
+    float2* R = line_fft(A, B, MH, logH, 2 * ncols, MH, false, tw);
+    float2* C = R == A ? B : A;
+    for (int t = threadIdx.x; t < ncols * MH; t += blockDim.x) {
+        const int y = t / ncols, c = t - y * ncols;
+        const float2 X = R[c * MH + y], Y = R[(ncols + c) * MH + y];
+        const float2 g = __ldg(&green[(size_t)y * SW + kx0 + c]);
+        const float sx = X.x * g.x + Y.x * g.y, sy = X.y * g.x + Y.y * g.y;
+        C[c * MH + y] = make_float2(sy * inv_total, -sx * inv_total);  // -i (gx X + gy Y) / M
+    }
+    __syncthreads();
+    const float2* F = line_fft(C, R, MH, logH, ncols, MH, true, tw);
+    for (int t = threadIdx.x; t < ncols * MH; t += blockDim.x) {
+        const int y = t / ncols, c = t - y * ncols;
+        cols[((size_t)(y >> 1) * SW + kx0 + c) * 2 + (y & 1)] = F[c * MH + y];
+    }
+}
+
 // Forward column transform only (the density spectrum, for diagnostics).
 __global__ void __launch_bounds__(256) fft_columns_forward_kernel(float2* half, int MW, int MH,
                                                                   int G,
@@ -385,6 +430,8 @@ cudaError_t configure_fft() {
     const size_t big = 200 * 1024;
     const void* fns[] = {(const void*)fft_rows_forward_kernel<long long>,
                          (const void*)fft_rows_forward_kernel<uint32_t>,
+                         (const void*)fft_rows_forward_kernel<float>,
+                         (const void*)fft_columns_adjoint_kernel,
                          (const void*)fft_columns_kernel, (const void*)fft_columns_forward_kernel,
                          (const void*)fft_rows_inverse_kernel, (const void*)fft64_line_kernel};
     for (const void* f : fns) {
@@ -433,6 +480,44 @@ cudaError_t launch_fft_columns(const float2* half, const float2* green, float in
     fft_columns_kernel<<<blocks, threads, smem, stream>>>(half, green, inv_total, g.MW, g.MH, G,
                                                       twiddles, cols);
     count_launches(1);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_fft_adjoint(const float* cotangent, const float2* green, float inv_total,
+                               GridShape g, const float2* twiddles, float2* half2, float4* cols,
+                               float2* mu2, cudaStream_t stream) {
+    // Rows: the 2*MH-row field (X and Y rows interleaved), two rows per line.
+    {
+        const int pairs = g.MH;
+        int pairs_per_cta, threads;
+        line_shape(pairs, g.MW, g.MW >= 4096 ? 1 : 4096 / g.MW, &pairs_per_cta, &threads, g.fft_lines);
+        const int blocks = (pairs + pairs_per_cta - 1) / pairs_per_cta;
+        const size_t smem = (size_t)2 * pairs_per_cta * g.MW * sizeof(float2);
+        fft_rows_forward_kernel<float><<<blocks, threads, smem, stream>>>(
+            cotangent, 1.0f, g.MW, 2 * g.MH, pairs_per_cta, twiddles, half2);
+        count_launches(1);
+    }
+    {
+        int G, threads;
+        column_shape(g.MW, g.MH, 4, &G, &threads, g.fft_lines);
+        const int SW = g.MW / 2 + 1;
+        const int blocks = (SW + G - 1) / G;
+        const size_t smem = (size_t)4 * G * g.MH * sizeof(float2);
+        fft_columns_adjoint_kernel<<<blocks, threads, smem, stream>>>(
+            half2, green, inv_total, g.MW, g.MH, G, twiddles, reinterpret_cast<float2*>(cols));
+        count_launches(1);
+    }
+    // Inverse rows: pairs of mu rows as the real and imaginary parts.
+    {
+        const int rows = g.MH / 2;
+        int rows_per_cta, threads;
+        line_shape(rows, g.MW, g.MW >= 4096 ? 1 : 4096 / g.MW, &rows_per_cta, &threads, g.fft_lines);
+        const int blocks = (rows + rows_per_cta - 1) / rows_per_cta;
+        const size_t smem = (size_t)2 * rows_per_cta * g.MW * sizeof(float2);
+        fft_rows_inverse_kernel<<<blocks, threads, smem, stream>>>(cols, g.MW, rows, rows_per_cta,
+                                                               twiddles, mu2);
+        count_launches(1);
+    }
     return cudaGetLastError();
 }
 

@@ -166,6 +166,39 @@ cudaError_t launch_short_range(const float4* bodies, const float4* entries, cons
 cudaError_t launch_interp_kick(float4* bodies, float2* accel, const float2* force,
                                const float2* a_short, KickParams p, cudaStream_t stream);
 
+// Reverse pass of one gravity-only step (p3m_adjoint.cu). cv: coefficient of
+// the velocity cotangent in the acceleration cotangent (dt/2 for a step, 0
+// when folding the initial acceleration a0 = F(x0) into x0); fold: update
+// only the position cotangent and clear the acceleration cotangent.
+struct AdjointParams {
+    int n, W, H, MW, MH, bounded, rx, ry, exact, home_limit, mutual, fold;
+    float aspect, gravity, sigma_cells, total_mass, min_frac, dt, cv;
+};
+// wa = la + cv lv per body, and its CIC spread into `cotangent`, a field of
+// 2*MH rows of MW floats (row 2y: x component of row y, row 2y+1: y).
+cudaError_t launch_adjoint_spread(const float4* bodies, const float4* lam, const float2* lam_a,
+                                  float2* wa, float* cotangent, const AdjointParams& p,
+                                  cudaStream_t stream);
+// Short-range pair and monopole terms, accumulated into g_short (zeroed).
+cudaError_t launch_adjoint_short_range(const float4* bodies, const float4* entries,
+                                       const int* cell_start, const int* cell_count,
+                                       const uint32_t* cell_mass, const float2* wa,
+                                       float2* g_short, const AdjointParams& p,
+                                       cudaStream_t stream);
+// CIC-gradient gather of m mu + wa . E, plus g_short; then the step's
+// cotangent update (or the fold).
+cudaError_t launch_adjoint_gather(const float4* bodies, const float4* materials, const float2* wa,
+                                  const float2* mu2, const float2* force, const float2* g_short,
+                                  float4* lam, float2* lam_a, const AdjointParams& p,
+                                  cudaStream_t stream);
+// Transposed mesh operator: mu = Kx^T X + Ky^T Y for the interleaved
+// cotangent field; mu2[(y >> 1) * MW + x] holds rows 2q and 2q+1 as (x, y).
+// half2: 2*MH*(MW/2+1) float2; cols: MH*(MW/2+1) float2 (may alias the
+// forward's float4 column buffer).
+cudaError_t launch_fft_adjoint(const float* cotangent, const float2* green, float inv_total,
+                               GridShape g, const float2* twiddles, float2* half2, float4* cols,
+                               float2* mu2, cudaStream_t stream);
+
 // Shared-memory opt-ins, once per device (p3m_create), never during capture.
 cudaError_t configure_deposit();
 cudaError_t configure_fft();
@@ -268,6 +301,9 @@ struct p3m_ctx {
 
     // diagnostics scratch
     double* diag = nullptr;  // conservation partials + result
+
+    // differentiated rollout (checkpoints, recompute slots, cotangents)
+    struct p3m_adjoint_store* adjoint = nullptr;
 
     // captured steps (CUDA graphs)
     bool use_graphs = true;

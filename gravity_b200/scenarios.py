@@ -167,14 +167,17 @@ def batch(sims: int = 256, seed: int = 11, steps: int = 60, nmin: int = 1000,
 
 
 def adjoint_cluster(n_cluster: int = 99_000, n_disc: int = 1_000, seed: int = 5,
-                    steps: int = 200) -> Scenario:
-    w, h = 2560, 1440
+                    steps: int = 200, viewport=(2560, 1440), grid=(1024, 512)) -> Scenario:
+    """The projectile disc is bodies n_cluster .. n-1. A smaller viewport
+    scales the cluster, the disc and the offset with its width."""
+    w, h = viewport
+    k = w / 2560.0
     rng = np.random.default_rng(seed)
     cx, cy = w / 2.0, h / 2.0
-    xc, yc = _plummer_2d(rng, n_cluster, 100.0, cx, cy, 0.45 * h)
-    r = 20.0 * np.sqrt(rng.uniform(0, 1, n_disc))
+    xc, yc = _plummer_2d(rng, n_cluster, 100.0 * k, cx, cy, 0.45 * h)
+    r = 20.0 * k * np.sqrt(rng.uniform(0, 1, n_disc))
     t = rng.uniform(0, 2 * np.pi, n_disc)
-    xd = (cx + 800.0 + r * np.cos(t)) % w
+    xd = (cx + 800.0 * k + r * np.cos(t)) % w
     yd = cy + r * np.sin(t)
     x = np.concatenate([xc, xd]) % w
     y = np.concatenate([yc, yd]) % h
@@ -182,6 +185,6 @@ def adjoint_cluster(n_cluster: int = 99_000, n_disc: int = 1_000, seed: int = 5,
     b = _to_unit(x, y, np.zeros(n), np.zeros(n), w, h)
     b[:, :2] = np.minimum(b[:, :2], np.float32(0.99999994))
     cfg = P3MConfig(viewport_width=w, viewport_height=h,
-                    gravity=GravityFieldConfig(grid_width=1024, grid_height=512),
+                    gravity=GravityFieldConfig(grid_width=grid[0], grid_height=grid[1]),
                     capacity=n, bounded=False, spatial_sort_interval=0)
     return Scenario("adjoint_cluster", cfg, b, unit_materials(n), steps)

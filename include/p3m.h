@@ -126,7 +126,9 @@ const char* p3m_status_string(int status);
 /* ---- state hand-off ----------------------------------------------------- */
 
 /* Replaces seedBodies / glBufferSubData uploads (GravityPipeline.kt:724-770,
- * :1438-1481). Any pointer may be NULL to leave that buffer unchanged. */
+ * :1438-1481). Any pointer may be NULL to leave that buffer unchanged. State
+ * pointers of these three calls may be host memory (pageable or page-locked)
+ * or device memory of the context's device. */
 int p3m_upload_state(p3m_ctx* ctx, const float* bodies4, const float* materials4,
                      const float* acceleration2, int32_t n);
 /* Writes `count` bodies starting at slot `first` (first + count <= capacity),
@@ -139,7 +141,7 @@ int p3m_upload_range(p3m_ctx* ctx, int32_t first, int32_t count, const float* bo
 /* Readback (the reference maps the SSBOs: GravityPipeline.kt:378-443). */
 int p3m_download_state(p3m_ctx* ctx, float* bodies4, float* materials4,
                        float* acceleration2, int32_t n);
-/* Copy a whole buffer to host memory; bytes must equal the buffer's size. */
+/* Copy the first `bytes` of a buffer to host memory (at most its size). */
 int p3m_debug_get(p3m_ctx* ctx, int32_t which, void* host, size_t bytes);
 /* Device address and size of a buffer (for callers that share device memory,
  * e.g. a renderer); the pointer stays valid until p3m_destroy. */
@@ -271,6 +273,34 @@ int p3m_batch_step(p3m_batch* batch, int32_t steps);
 int p3m_batch_autotune(p3m_batch* batch, int32_t trial_steps, int32_t* chosen);
 int p3m_batch_synchronize(p3m_batch* batch);
 int p3m_batch_get_stream(p3m_batch* batch, void** stream);
+
+/* ---- differentiated rollout ---------------------------------------------- */
+
+/* A hand-written adjoint of the gravity-only step (GravityPipeline.kt:445-494
+ * without collisions; the reference has no adjoint), as a forward/backward
+ * pair: p3m_adjoint_forward runs `steps` plain steps from the current state,
+ * saving bodies and accelerations every `interval` steps;
+ * p3m_adjoint_backward takes the cotangents of the final state and returns
+ * those of the initial state, recomputing each segment from its checkpoint.
+ * The cell topology (monopole cells, summed list entries) is held fixed
+ * where the positions are differentiated, and the fixed-point deposit is
+ * taken as its real value. Torus only (walls: P3M_ERR_UNSUPPORTED), and the
+ * context's spatial_sort_interval must be 0 (the rollout keeps body order).
+ * State pointers may be host memory or device memory of the context's
+ * device. Changing the state, the uniforms or the body count between the
+ * two calls gives meaningless gradients. */
+#define P3M_ADJOINT_INITIAL_ACCELERATION 1 /* a0 = initializeAcceleration(x0):
+                                              the backward folds da0 into dx0 */
+int p3m_adjoint_forward(p3m_ctx* ctx, int32_t n, int32_t steps, int32_t interval, int32_t flags);
+/* seed_bodies4: dL/d(x, y, vx, vy) of the final state (unit coordinates);
+ * seed_accel2: dL/d(final a), may be NULL (zero). Writes dL/d(initial
+ * x, y, vx, vy) and, if grad_accel2 is not NULL, dL/d(initial a) (zero when
+ * the forward computed a0 itself). Synchronous. Leaves the context in the
+ * forward's final state. */
+int p3m_adjoint_backward(p3m_ctx* ctx, const float* seed_bodies4, const float* seed_accel2,
+                         float* grad_bodies4, float* grad_accel2);
+/* Frees the checkpoints and recompute storage. */
+int p3m_adjoint_release(p3m_ctx* ctx);
 
 /* ---- cell lists without allocation ------------------------------------- */
 

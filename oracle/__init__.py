@@ -46,8 +46,8 @@ def load() -> ctypes.CDLL:
     with _lock:
         if _lib is not None:
             return _lib
-        src = HERE / "p3m_oracle.cpp"
-        if not LIB.exists() or LIB.stat().st_mtime < src.stat().st_mtime:
+        newest = max((HERE / f).stat().st_mtime for f in ("p3m_oracle.cpp", "p3m_adjoint_f64.cpp"))
+        if not LIB.exists() or LIB.stat().st_mtime < newest:
             build()
         lib = ctypes.CDLL(str(LIB))
         vp, i, f = ctypes.c_void_p, ctypes.c_int, ctypes.c_float
@@ -87,6 +87,13 @@ def load() -> ctypes.CDLL:
             "oracle_kernel_spectra": (None, [vp, vp, vp]),
             "oracle_destinations": (None, [vp, vp, i]),
             "oracle_direct_sum_f64": (None, [vp, vp, i, vp, i, vp, f, i, vp]),
+            "oracle_adj_create": (vp, [vp, vp, i, ctypes.c_double, ctypes.c_double]),
+            "oracle_adj_destroy": (None, [vp]),
+            "oracle_adj_force": (None, [vp, vp, vp]),
+            "oracle_adj_mesh_force": (None, [vp, vp, vp, vp]),
+            "oracle_adj_set_positions": (None, [vp, i, vp]),
+            "oracle_adj_forward": (None, [vp, vp, vp, i, i, vp, vp]),
+            "oracle_adj_backward": (None, [vp, vp, vp, vp, vp]),
         }
         for name, (res, args) in sigs.items():
             fn = getattr(lib, name)
@@ -291,3 +298,73 @@ class OracleSim:
         out = np.empty(n, np.uint32)
         self._lib.oracle_destinations(self._s, _p(out), n)
         return out
+
+
+class Adjoint64:
+    """FP64 reference of the differentiated gravity-only rollout on the torus
+    (p3m_adjoint_f64.cpp): forward, then the hand-written reverse pass.
+
+    field_px: uniform field in px/s^2, converted to unit/s^2 like the library.
+    """
+
+    def __init__(self, config, materials, field_px=(0.0, 0.0)):
+        self._lib = load()
+        self._abi_cfg = config.to_abi()
+        m = np.ascontiguousarray(materials, np.float64).reshape(-1, 4)
+        self.n = m.shape[0]
+        fx = field_px[0] / config.viewport_width
+        fy = field_px[1] / config.viewport_height
+        self._s = self._lib.oracle_adj_create(ctypes.byref(self._abi_cfg), _p(m), self.n, fx, fy)
+        if not self._s:
+            raise ValueError("the FP64 adjoint covers the torus only, with n > 0")
+
+    def close(self):
+        if self._s:
+            self._lib.oracle_adj_destroy(self._s)
+            self._s = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def force(self, positions):
+        x = np.ascontiguousarray(positions, np.float64).reshape(-1, 2)
+        out = np.empty_like(x)
+        self._lib.oracle_adj_force(self._s, _p(x), _p(out))
+        return out
+
+    def mesh_force(self, positions):
+        """The FP64 mesh force (H, W, 2) at `positions` (n, 2)."""
+        x = np.ascontiguousarray(positions, np.float64).reshape(-1, 2)
+        w, h = self._abi_cfg.grid_width, self._abi_cfg.grid_height
+        ex = np.empty((h, w), np.float64)
+        ey = np.empty((h, w), np.float64)
+        self._lib.oracle_adj_mesh_force(self._s, _p(x), _p(ex), _p(ey))
+        return np.stack([ex, ey], axis=-1)
+
+    def forward(self, bodies, steps, acceleration=None):
+        """Final (bodies (n,4), acceleration (n,2)) in float64. Without
+        `acceleration`, a0 is the force at the initial positions."""
+        b = np.ascontiguousarray(bodies, np.float64).reshape(-1, 4)
+        a = None if acceleration is None else np.ascontiguousarray(acceleration, np.float64).reshape(-1, 2)
+        out = np.empty_like(b)
+        acc = np.empty((self.n, 2), np.float64)
+        self._lib.oracle_adj_forward(self._s, _p(b), _p(a), 1 if a is None else 0, steps,
+                                     _p(out), _p(acc))
+        return out, acc
+
+    def set_positions(self, k, positions):
+        """Replace the recorded positions of step k (0 = initial)."""
+        x = np.ascontiguousarray(positions, np.float64).reshape(self.n, 2)
+        self._lib.oracle_adj_set_positions(self._s, int(k), _p(x))
+
+    def backward(self, seed, seed_accel=None):
+        """dL/d(initial bodies) (n,4) and dL/d(initial acceleration) (n,2)."""
+        s4 = np.ascontiguousarray(seed, np.float64).reshape(-1, 4)
+        sa = None if seed_accel is None else np.ascontiguousarray(seed_accel, np.float64).reshape(-1, 2)
+        g = np.empty_like(s4)
+        ga = np.empty((self.n, 2), np.float64)
+        self._lib.oracle_adj_backward(self._s, _p(s4), _p(sa), _p(g), _p(ga))
+        return g, ga
