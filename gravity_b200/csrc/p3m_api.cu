@@ -209,7 +209,8 @@ void free_all(p3m_ctx* ctx) {
     void* ptrs[] = {ctx->diag, ctx->bodies, ctx->bodies_alt, ctx->accel, ctx->accel_alt, ctx->materials,
                     ctx->materials_alt, ctx->destinations, ctx->status, ctx->keys, ctx->vals,
                     ctx->sort.keys_alt, ctx->sort.vals_alt, ctx->sort.hist, ctx->sort.block_sums,
-                    ctx->cell_start, ctx->cell_count, ctx->cell_mass, ctx->entries, ctx->a_short, ctx->density,
+                    ctx->cell_start, ctx->cell_count, ctx->cell_mass, ctx->entries, ctx->a_short,
+                    ctx->deposit_work, ctx->density,
                     ctx->half, ctx->cols, ctx->force, ctx->green, ctx->twiddles};
     for (void* p : ptrs)
         if (p) cudaFree(p);
@@ -260,7 +261,7 @@ int lists_from_keys(p3m_ctx* ctx, int n) {
     P3M_CUDA(ctx, cudaMemsetAsync(ctx->cell_count, 0, P * sizeof(int), ctx->stream));
     P3M_CUDA(ctx, cudaMemsetAsync(ctx->cell_mass, 0, P * sizeof(uint32_t), ctx->stream));
     P3M_CUDA(ctx, p3m::launch_cell_build(sk, sv, n, ctx->bodies, ctx->materials, ctx->cell_start,
-                                         ctx->cell_count, ctx->cell_mass, ctx->entries,
+                                         ctx->cell_count, ctx->cell_mass, ctx->entries, (int)P,
                                          ctx->stream));
     return P3M_OK;
 }
@@ -271,13 +272,14 @@ int mesh_force(p3m_ctx* ctx, int n) {
     int st = ensure_green(ctx);
     if (st != P3M_OK) return st;
     const bool i64 = ctx->cfg.deposit_mode == P3M_DEPOSIT_I64;
-    const size_t M = mesh_cells(ctx);
     {
         StageScope scope(ctx, P3M_STAGE_DEPOSIT);
-        P3M_CUDA(ctx, cudaMemsetAsync(ctx->density, 0, M * (i64 ? 8 : 4), ctx->stream));
-        P3M_CUDA(ctx, p3m::launch_deposit(ctx->entries, ctx->sorted_keys, n, ctx->grid,
+        P3M_CUDA(ctx, p3m::launch_deposit(ctx->entries, ctx->sorted_keys, ctx->cell_start, n, ctx->grid,
                                           ctx->cfg.deposit_mode, (float)ctx->mass_scale,
-                                          ctx->density, ctx->stream));
+                                          ctx->density, ctx->deposit_work,
+                                          reinterpret_cast<int*>(ctx->deposit_work +
+                                                                 ctx->deposit_work_capacity),
+                                          (int)ctx->deposit_work_capacity, ctx->stream));
     }
     // fft_init.comp's uInverseMassScale = 1f / massScale (GravityPipeline.kt:942).
     const float inv_scale = i64 ? 1.0f / 4294967296.0f : 1.0f / (float)ctx->mass_scale;
@@ -600,11 +602,13 @@ int p3m_create(const p3m_config* config, p3m_ctx** out) {
     ALLOC(ctx->sort.vals_alt, cap);
     ALLOC(ctx->sort.hist, p3m::sort_hist_entries((int)cap));
     ALLOC(ctx->sort.block_sums, p3m::sort_block_sum_entries((int)cap));
-    ALLOC(ctx->cell_start, P);
+    ALLOC(ctx->cell_start, P + 1);
     ALLOC(ctx->cell_count, P);
     ALLOC(ctx->cell_mass, P);
     ALLOC(ctx->entries, cap);
     ALLOC(ctx->a_short, cap);
+    ctx->deposit_work_capacity = p3m::deposit_work_entries((int)cap, mw_max, mh_max);
+    ALLOC(ctx->deposit_work, ctx->deposit_work_capacity + 1);  // + the counter
     {
         unsigned long long* d = nullptr;
         ALLOC(d, M);  // 8 bytes per cell holds either deposit mode
@@ -634,7 +638,7 @@ int p3m_create(const p3m_config* config, p3m_ctx** out) {
         P3M_CUDA(ctx, cudaMemsetAsync(ctx->destinations, 0, cap * sizeof(uint32_t), ctx->stream));
         P3M_CUDA(ctx, cudaMemsetAsync(ctx->status, 0, 4 * sizeof(unsigned), ctx->stream));
         P3M_CUDA(ctx, cudaMemsetAsync(ctx->cell_count, 0, P * sizeof(int), ctx->stream));
-        P3M_CUDA(ctx, cudaMemsetAsync(ctx->cell_start, 0, P * sizeof(int), ctx->stream));
+        P3M_CUDA(ctx, cudaMemsetAsync(ctx->cell_start, 0, (P + 1) * sizeof(int), ctx->stream));
         P3M_CUDA(ctx, cudaMemsetAsync(ctx->cell_mass, 0, P * sizeof(uint32_t), ctx->stream));
         int s = ensure_green(ctx);
         if (s != P3M_OK) return s;

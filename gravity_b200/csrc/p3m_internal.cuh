@@ -118,16 +118,22 @@ cudaError_t launch_morton_keys(const float4* bodies, int n, int wbits, int hbits
 cudaError_t launch_permute(const uint32_t* order, int n, const float4* bodies, const float2* accel,
                            const float4* materials, float4* bodies_out, float2* accel_out,
                            float4* materials_out, uint32_t* destinations, cudaStream_t stream);
-// Cell lists from sorted keys: start, count, mass; gathers entries.
+// Cell lists from sorted keys: start, count, mass; gathers entries. With
+// fill_cells = P > 0, cell_start (P + 1 entries) becomes a full CSR: an empty
+// cell starts where the next occupied one does and cell_start[P] = n;
+// otherwise only occupied cells are written.
 cudaError_t launch_cell_build(const uint32_t* keys, const uint32_t* ids, int n,
                               const float4* bodies, const float4* materials, int* cell_start,
                               int* cell_count, uint32_t* cell_mass, float4* entries,
-                              cudaStream_t stream);
+                              int fill_cells, cudaStream_t stream);
 
-// Tile-reduced CIC deposit (build_grid.comp:53-69) over cell-ordered entries.
-cudaError_t launch_deposit(const float4* entries, const uint32_t* keys, int n, GridShape g,
-                           int deposit_mode, float mass_scale, void* density,
-                           cudaStream_t stream);
+// CIC deposit (build_grid.comp:53-69) over cell-ordered entries (keys: their
+// sorted cells; cell_start: the full CSR). Writes every mesh cell.
+// work: deposit_work_entries(capacity, MW, MH) int4 + 1 counter.
+size_t deposit_work_entries(int capacity, int MW, int MH);
+cudaError_t launch_deposit(const float4* entries, const uint32_t* keys, const int* cell_start,
+                           int n, GridShape g, int deposit_mode, float mass_scale, void* density,
+                           int4* work, int* work_count, int work_capacity, cudaStream_t stream);
 
 // Real 2D FFT, spectral multiply and inverse (fft_shared.comp, convolve.comp).
 cudaError_t launch_fft_forward_rows(const void* density, int deposit_mode, float inv_scale,
@@ -289,6 +295,8 @@ struct p3m_ctx {
     uint32_t* cell_mass = nullptr;
     float4* entries = nullptr;
     float2* a_short = nullptr;  // short-range accelerations, by body ID
+    int4* deposit_work = nullptr;  // pieces of heavy mesh tiles (+1 counter)
+    size_t deposit_work_capacity = 0;
 
     // mesh
     void* density = nullptr;

@@ -297,10 +297,26 @@ __global__ void permute_kernel(const uint32_t* __restrict__ order, int n,
 // the fixed-point cell masses (build_grid.comp:74-75) are reduced over each
 // warp's segment of equal keys, then added with one atomic per segment
 // (integer sums, so the result does not depend on the order).
+// The whole warp stores value v into cell_start[f0, f1) for every lane's
+// range, one lane's range after another (gaps can be long when cells far
+// outnumber bodies).
+__device__ __forceinline__ void fill_ranges(int* cell_start, uint32_t f0, uint32_t f1, int v) {
+    const int lane = threadIdx.x & 31;
+    unsigned pending = __ballot_sync(kFull, f1 > f0);
+    while (pending) {
+        const int src = __ffs(pending) - 1;
+        pending &= pending - 1;
+        const uint32_t a = __shfl_sync(kFull, f0, src), b = __shfl_sync(kFull, f1, src);
+        const int value = __shfl_sync(kFull, v, src);
+        for (uint32_t c = a + lane; c < b; c += 32) cell_start[c] = value;
+    }
+}
+
 __global__ void cell_build_kernel(const uint32_t* __restrict__ keys, const uint32_t* __restrict__ ids,
                                   int n, const float4* __restrict__ bodies,
                                   const float4* __restrict__ materials, int* cell_start,
-                                  int* cell_count, uint32_t* cell_mass, float4* entries) {
+                                  int* cell_count, uint32_t* cell_mass, float4* entries,
+                                  int fill_cells) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const int lane = threadIdx.x & 31;
     const bool valid = i < n;
@@ -336,6 +352,16 @@ __global__ void cell_build_kernel(const uint32_t* __restrict__ keys, const uint3
     if (tail) {
         atomicAdd(&cell_count[c], (int)cnt);
         atomicAdd(&cell_mass[c], mq);
+    }
+    if (fill_cells > 0) {
+        // Full CSR: an empty cell starts where the next occupied cell does,
+        // and cell_start[fill_cells] = n. The head of each run fills the
+        // empty cells before it; the last entry fills the cells after it.
+        const bool head = valid && (i == 0 || prev != c);
+        const uint32_t g0 = (i == 0) ? 0u : prev + 1u;
+        fill_ranges(cell_start, head ? g0 : 0u, head ? c : 0u, i);
+        const bool last = valid && i == n - 1;
+        fill_ranges(cell_start, last ? c + 1u : 0u, last ? (uint32_t)fill_cells + 1u : 0u, n);
     }
 }
 
@@ -429,11 +455,16 @@ cudaError_t launch_permute(const uint32_t* order, int n, const float4* bodies, c
 
 cudaError_t launch_cell_build(const uint32_t* keys, const uint32_t* ids, int n, const float4* bodies,
                               const float4* materials, int* cell_start, int* cell_count,
-                              uint32_t* cell_mass, float4* entries, cudaStream_t stream) {
-    if (n <= 0) return cudaSuccess;
+                              uint32_t* cell_mass, float4* entries, int fill_cells,
+                              cudaStream_t stream) {
+    if (n <= 0) {
+        if (fill_cells > 0)
+            return cudaMemsetAsync(cell_start, 0, ((size_t)fill_cells + 1) * sizeof(int), stream);
+        return cudaSuccess;
+    }
     cell_build_kernel<<<blocks_for(n, 256), 256, 0, stream>>>(keys, ids, n, bodies, materials,
                                                               cell_start, cell_count, cell_mass,
-                                                              entries);
+                                                              entries, fill_cells);
     count_launches(1);
     return cudaGetLastError();
 }

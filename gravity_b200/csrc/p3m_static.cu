@@ -129,7 +129,8 @@ extern "C" int p3m_cell_lists_static(const float* bodies4, const float* material
     if (e == cudaSuccess && n > 0)
         e = p3m::launch_cell_build(sk, sv, n, reinterpret_cast<const float4*>(bodies4),
                                    reinterpret_cast<const float4*>(materials4), cell_start,
-                                   cell_count, cell_mass, reinterpret_cast<float4*>(entries4), s);
+                                   cell_count, cell_mass, reinterpret_cast<float4*>(entries4), 0,
+                                   s);
     if (e == cudaSuccess && n > 0)
         e = cudaMemcpyAsync(sorted_keys, sk, (size_t)n * sizeof(uint32_t), cudaMemcpyDeviceToDevice, s);
     if (e == cudaSuccess && n > 0)
