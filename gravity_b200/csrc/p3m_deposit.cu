@@ -63,6 +63,7 @@ __device__ __forceinline__ unsigned long long quantize<unsigned long long>(float
 
 struct TileGeom {
     int W, H, MW, MH, TX, TY, tiles_x;
+    int tx_log2;  // TX is a power of two
 };
 
 // The runs of entries whose bodies can reach tile `tile`, in shared memory;
@@ -186,18 +187,6 @@ __device__ __forceinline__ void add_node(TileAcc<T>& acc, const TileGeom& g, int
     if ((unsigned)tx < (unsigned)g.TX && (unsigned)ty < (unsigned)g.TY) acc.add(ty * g.TX + tx, v);
 }
 
-// Entry index of position k of the tile's runs taken end to end: the last
-// run starting at or before k (an empty run starts where the next one does).
-__device__ __forceinline__ int flat_entry(int k, const int* run_begin, const int* run_prefix) {
-    int lo = 0, hi = kMaxRuns - 1;
-    while (lo < hi) {
-        const int mid = (lo + hi + 1) >> 1;
-        if (run_prefix[mid] <= k) lo = mid;
-        else hi = mid - 1;
-    }
-    return run_begin[lo] + (k - run_prefix[lo]);
-}
-
 template <typename T>
 __device__ __forceinline__ void add_corners(const Corners<T>& c, const TileGeom& g, int c0, int r0,
                                             TileAcc<T>& acc) {
@@ -214,25 +203,42 @@ __device__ __forceinline__ void add_corners(const Corners<T>& c, const TileGeom&
     }
 }
 
-// Sparse tiles: the CTA's threads take positions t, t + threads, ... of the
-// runs (coalesced), four loads in flight per thread, and add each body's
-// corners one by one.
+// Sparse tiles: warp w takes the w-th share of the runs' positions, its
+// lanes consecutive positions (coalesced within a run), four loads in flight
+// per lane; each lane walks the runs forward from one search, so finding an
+// entry costs O(1). Each body's corners are added one by one.
 template <typename T>
 __device__ void tile_direct(const float4* __restrict__ entries, int total, const int* run_begin,
                             const int* run_prefix, const TileGeom& g, int c0, int r0, float scale,
                             TileAcc<T>& acc) {
     constexpr int U = 4;
-    const int step = blockDim.x;
-    for (int k0 = threadIdx.x; k0 < total; k0 += U * step) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, warps = blockDim.x >> 5;
+    const int share = (total + warps - 1) / warps;
+    const int kb = min(total, warp * share), ke = min(total, kb + share);
+    int r = 0;
+    {
+        int lo = 0, hi = kMaxRuns - 1;
+        const int k = kb + lane;
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (run_prefix[mid] <= k) lo = mid;
+            else hi = mid - 1;
+        }
+        r = lo;
+    }
+    for (int p0 = kb + lane; p0 < ke; p0 += 32 * U) {
         float4 e[U];
 #pragma unroll
         for (int u = 0; u < U; ++u) {
-            const int k = k0 + u * step;
-            if (k < total) e[u] = __ldg(&entries[flat_entry(k, run_begin, run_prefix)]);
+            const int p = p0 + 32 * u;
+            if (p < ke) {
+                while (r + 1 < kMaxRuns && run_prefix[r + 1] <= p) ++r;
+                e[u] = __ldg(&entries[run_begin[r] + (p - run_prefix[r])]);
+            }
         }
 #pragma unroll
         for (int u = 0; u < U; ++u)
-            if (k0 + u * step < total) add_corners<T>(corners<T>(e[u], g, scale), g, c0, r0, acc);
+            if (p0 + 32 * u < ke) add_corners<T>(corners<T>(e[u], g, scale), g, c0, r0, acc);
     }
 }
 
@@ -368,7 +374,7 @@ __global__ void __launch_bounds__(kThreads) deposit_tiles_kernel(
     }
     __syncthreads();
     for (int i = threadIdx.x; i < cells; i += blockDim.x) {
-        const int y = i / g.TX, x = i - y * g.TX;
+        const int y = i >> g.tx_log2, x = i & (g.TX - 1);
         density[(size_t)(r0 + y) * g.MW + c0 + x] = acc.get(i);
     }
 }
@@ -395,7 +401,7 @@ __global__ void __launch_bounds__(kThreads) deposit_heavy_kernel(
         __syncthreads();
         for (int i = threadIdx.x; i < cells; i += blockDim.x) {
             const T v = acc.get(i);
-            const int y = i / g.TX, x = i - y * g.TX;
+            const int y = i >> g.tx_log2, x = i & (g.TX - 1);
             if (v != T(0)) atomicAdd(&density[(size_t)(r0 + y) * g.MW + c0 + x], v);
         }
         __syncthreads();  // acc is reused by the next item
@@ -478,6 +484,8 @@ TileGeom tile_geom(const GridShape& g) {
     t.TX = g.MW < kTileX ? g.MW : kTileX;
     t.TY = g.MH < kTileY ? g.MH : kTileY;
     t.tiles_x = g.MW / t.TX;
+    t.tx_log2 = 0;
+    while ((1 << t.tx_log2) < t.TX) ++t.tx_log2;
     return t;
 }
 
