@@ -476,9 +476,13 @@ def run_b200(args, ws, rank, local):
         cpu = None
         if not args.no_cpu_baseline:
             rate, steps, el, used = cpu_oracle_rate(sc, args.cpu_seconds, threads=os.cpu_count())
+            rate1, steps1, el1, _ = cpu_oracle_rate(sc, min(args.cpu_seconds, 10.0), threads=1,
+                                                    max_steps=steps)
             cpu = {"value": rate, "unit": UNIT, "cores": used, "kind": "port",
                    "sample": f"{steps} P3M steps of the {n}-body {args.workload} workload "
-                             f"({el:.1f} s) after initialisation and 1 untimed step"}
+                             f"({el:.1f} s) after initialisation and 1 untimed step",
+                   "value_1_thread": rate1,
+                   "sample_1_thread": f"{steps1} steps ({el1:.1f} s) on one thread"}
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True,
