@@ -118,6 +118,7 @@ SIGNATURES = {
     "p3m_batch_initialize_acceleration": (ctypes.c_int, [_vp]),
     "p3m_batch_step": (ctypes.c_int, [_vp, _i32]),
     "p3m_batch_autotune": (ctypes.c_int, [_vp, _i32, _vp]),
+    "p3m_batch_set_fused": (ctypes.c_int, [_vp, _i32]),
     "p3m_batch_synchronize": (ctypes.c_int, [_vp]),
     "p3m_batch_get_stream": (ctypes.c_int, [_vp, ctypes.POINTER(_vp)]),
     "p3m_adjoint_forward": (ctypes.c_int, [_vp, _i32, _i32, _i32, _i32]),

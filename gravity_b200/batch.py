@@ -70,6 +70,11 @@ class GravityBatch:
     def step(self, steps: int = 1) -> None:
         self._check(self._lib.p3m_batch_step(self._b, steps))
 
+    def set_fused(self, enabled: bool) -> None:
+        """One launch per stage for all simulations (default) or one step
+        per simulation inside one graph; the results are the same bits."""
+        self._check(self._lib.p3m_batch_set_fused(self._b, 1 if enabled else 0))
+
     def synchronize(self) -> None:
         self._check(self._lib.p3m_batch_synchronize(self._b))
 

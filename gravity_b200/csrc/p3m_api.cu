@@ -11,6 +11,8 @@
 #include <cstring>
 #include <new>
 #include <string>
+#include <functional>
+#include <map>
 #include <vector>
 
 namespace p3m {
@@ -261,7 +263,8 @@ int lists_from_keys(p3m_ctx* ctx, int n) {
     P3M_CUDA(ctx, cudaMemsetAsync(ctx->cell_count, 0, P * sizeof(int), ctx->stream));
     P3M_CUDA(ctx, cudaMemsetAsync(ctx->cell_mass, 0, P * sizeof(uint32_t), ctx->stream));
     P3M_CUDA(ctx, p3m::launch_cell_build(sk, sv, n, ctx->bodies, ctx->materials, ctx->cell_start,
-                                         ctx->cell_count, ctx->cell_mass, ctx->entries, (int)P,
+                                         ctx->cell_count, ctx->cell_mass, ctx->entries,
+                                         p3m::deposit_uses_cell_starts(n) ? (int)P : 0,
                                          ctx->stream));
     return P3M_OK;
 }
@@ -310,7 +313,7 @@ int build_force(p3m_ctx* ctx, int n) {
     return mesh_force(ctx, n);
 }
 
-int apply_kick(p3m_ctx* ctx, int n, int initial) {
+p3m::KickParams kick_params(const p3m_ctx* ctx, int n, int initial) {
     p3m::KickParams p;
     p.n = n;
     p.W = ctx->grid.W; p.H = ctx->grid.H; p.MW = ctx->grid.MW; p.MH = ctx->grid.MH;
@@ -323,6 +326,11 @@ int apply_kick(p3m_ctx* ctx, int n, int initial) {
     p.min_frac = ctx->cfg.minimum_distance_cell_fraction; p.dt = ctx->cfg.time_step;
     p.field_x = ctx->field_x; p.field_y = ctx->field_y;
     p.sr_threads = ctx->tune_sr_threads;
+    return p;
+}
+
+int apply_kick(p3m_ctx* ctx, int n, int initial) {
+    const p3m::KickParams p = kick_params(ctx, n, initial);
     if (ctx->mutual) {
         StageScope scope(ctx, P3M_STAGE_SHORT_RANGE);
         P3M_CUDA(ctx, p3m::launch_short_range(ctx->bodies, ctx->entries, ctx->cell_start,
@@ -971,6 +979,17 @@ struct p3m_batch {
         std::vector<std::pair<uint32_t*, uint32_t*>> sorted;
     };
     std::vector<Graph> graphs;
+    // Fused form: one launch per stage for every simulation (see batch_plan).
+    bool fused = true;
+    struct Plan {
+        std::vector<uint64_t> key;
+        void* blob = nullptr;  // per-simulation arguments and block prefixes
+        cudaGraphExec_t exec = nullptr;
+        long long kernels = 0;
+        std::vector<char> swap;  // simulations whose buffers the reorder swapped
+        std::vector<std::pair<uint32_t*, uint32_t*>> sorted;
+    };
+    std::vector<Plan> plans;
     std::string last_error;
 };
 
@@ -989,6 +1008,11 @@ int batch_fail_ctx(p3m_batch* b, size_t sim, int status) {
 void batch_drop_graphs(p3m_batch* b) {
     for (auto& g : b->graphs) cudaGraphExecDestroy(g.exec);
     b->graphs.clear();
+    for (auto& p : b->plans) {
+        if (p.exec) cudaGraphExecDestroy(p.exec);
+        if (p.blob) cudaFree(p.blob);
+    }
+    b->plans.clear();
 }
 
 uint64_t bits_of(float f) {
@@ -1029,6 +1053,9 @@ int batch_enqueue(p3m_batch* b, const std::vector<char>& sort) {
     return P3M_OK;
 }
 
+bool fused_supported(const p3m_batch* b);
+int batch_fused_step(p3m_batch* b, const std::vector<char>& sort, const std::vector<uint64_t>& key);
+
 int batch_one_step(p3m_batch* b) {
     std::vector<char> sort(b->sims.size(), 0);
     for (size_t i = 0; i < b->sims.size(); ++i) {
@@ -1041,6 +1068,7 @@ int batch_one_step(p3m_batch* b) {
         if (interval > 0) c->physics_steps++;
     }
     const std::vector<uint64_t> key = batch_key(b, sort);
+    if (b->fused && fused_supported(b)) return batch_fused_step(b, sort, key);
     for (const auto& g : b->graphs) {
         if (g.key != key) continue;
         cudaError_t e = cudaGraphLaunch(g.exec, b->stream);
@@ -1088,6 +1116,371 @@ int batch_one_step(p3m_batch* b) {
     b->graphs.push_back(std::move(entry));
     e = cudaGraphLaunch(b->graphs.back().exec, b->stream);
     if (e != cudaSuccess) return batch_fail(b, P3M_ERR_CUDA, cudaGetErrorString(e));
+    return P3M_OK;
+}
+
+// ---- fused batch step ------------------------------------------------------
+// Every stage of the step runs as one launch over all simulations (CTA b
+// takes local block b - first[s] of simulation s; see p3m_internal.cuh), so a
+// batch step costs ~25 launches whatever the number of simulations. The
+// per-simulation arguments of every launch and the block prefixes live in one
+// device blob, written once per plan; the launches are captured in a graph.
+// A plan holds for one set of body counts, reorder flags, buffer roles and
+// uniforms, like the graphs of the other form.
+
+struct BlobBuilder {
+    std::vector<unsigned char> host;
+    size_t add(const void* data, size_t bytes) {
+        const size_t off = (host.size() + 15) & ~(size_t)15;
+        host.resize(off + bytes);
+        if (bytes) std::memcpy(host.data() + off, data, bytes);
+        return off;
+    }
+};
+
+struct FusedBuilder {
+    BlobBuilder blob;
+    std::vector<std::function<cudaError_t(unsigned char*, cudaStream_t)>> launches;
+
+    template <typename Args, typename Fn>
+    void stage(const std::vector<Args>& args, const std::vector<int>& blocks, Fn fn) {
+        if (args.empty()) return;
+        std::vector<int> first(args.size() + 1, 0);
+        for (size_t i = 0; i < args.size(); ++i) first[i + 1] = first[i] + blocks[i];
+        if (first.back() == 0) return;
+        const size_t a_off = blob.add(args.data(), args.size() * sizeof(Args));
+        const size_t f_off = blob.add(first.data(), first.size() * sizeof(int));
+        const int sims = (int)args.size(), total = first.back();
+        launches.push_back([=](unsigned char* dev, cudaStream_t st) {
+            p3m::BatchGrid g{reinterpret_cast<const int*>(dev + f_off), sims, total};
+            return fn(reinterpret_cast<const Args*>(dev + a_off), g, st);
+        });
+    }
+    void raw(std::function<cudaError_t(unsigned char*, cudaStream_t)> fn) { launches.push_back(fn); }
+};
+
+// Whether the fused form covers this batch: every histogram of a radix pass
+// fits one scan CTA.
+bool fused_supported(const p3m_batch* b) {
+    for (size_t i = 0; i < b->sims.size(); ++i)
+        if ((long long)p3m::radix_tiles(b->n[i]) * 256 > p3m::radix_scan_limit()) return false;
+    return true;
+}
+
+struct SimRoles {
+    float4 *bodies, *materials;
+    float2* accel;
+    uint32_t *sk, *sv;  // the cell sort's result
+};
+
+// Radix passes over the simulations listed in `who` (key bits each), with
+// keys/vals ping-ponging between (keys, vals) and the sort scratch.
+void fused_radix(FusedBuilder& fb, const p3m_batch* b, const std::vector<int>& who,
+                 const std::vector<int>& key_bits, std::vector<uint32_t*>& kin,
+                 std::vector<uint32_t*>& vin) {
+    int max_passes = 0;
+    std::vector<int> passes(who.size()), bits(who.size());
+    for (size_t j = 0; j < who.size(); ++j) {
+        passes[j] = (key_bits[j] + 7) / 8;
+        bits[j] = (key_bits[j] + passes[j] - 1) / passes[j];
+        if (b->n[who[j]] <= 1) passes[j] = 0;
+        max_passes = std::max(max_passes, passes[j]);
+    }
+    std::vector<uint32_t*> kout(who.size()), vout(who.size());
+    for (size_t j = 0; j < who.size(); ++j) {
+        const p3m_ctx* c = b->sims[who[j]];
+        kout[j] = c->sort.keys_alt;
+        vout[j] = c->sort.vals_alt;
+    }
+    for (int pass = 0; pass < max_passes; ++pass) {
+        std::vector<p3m::RadixArgs> ra;
+        std::vector<p3m::ScanArgs> sa;
+        std::vector<int> tiles, ones;
+        for (size_t j = 0; j < who.size(); ++j) {
+            if (pass >= passes[j]) continue;
+            const p3m_ctx* c = b->sims[who[j]];
+            const int n = b->n[who[j]];
+            const int shift = pass * bits[j];
+            const int pbits = std::min(bits[j], key_bits[j] - shift);
+            const int t = p3m::radix_tiles(n);
+            ra.push_back({kin[j], vin[j], kout[j], vout[j], c->sort.hist, n, shift, pbits, t});
+            sa.push_back({c->sort.hist, (1 << pbits) * t});
+            tiles.push_back(t);
+            ones.push_back(1);
+            std::swap(kin[j], kout[j]);
+            std::swap(vin[j], vout[j]);
+        }
+        fb.stage(ra, tiles, p3m::batched_radix_hist);
+        fb.stage(sa, ones, p3m::batched_scan);
+        fb.stage(ra, tiles, p3m::batched_radix_scatter);
+    }
+}
+
+int build_fused(p3m_batch* b, const std::vector<char>& sort, p3m_batch::Plan& plan) {
+    const size_t S = b->sims.size();
+    FusedBuilder fb;
+    std::vector<SimRoles> role(S);
+    plan.swap.assign(S, 0);
+    for (size_t i = 0; i < S; ++i) {
+        p3m_ctx* c = b->sims[i];
+        role[i] = {c->bodies, c->materials, c->accel, c->keys, c->vals};
+    }
+    // 1. Morton reorder (simulations whose reorder step this is).
+    {
+        std::vector<int> who, bits;
+        std::vector<p3m::MortonArgs> ma;
+        std::vector<int> blocks;
+        for (size_t i = 0; i < S; ++i) {
+            if (!sort[i] || b->n[i] <= 0) continue;
+            p3m_ctx* c = b->sims[i];
+            who.push_back((int)i);
+            bits.push_back(c->sort_wbits + c->sort_hbits);
+            ma.push_back({c->bodies, c->keys, c->vals, b->n[i], c->sort_wbits, c->sort_hbits});
+            blocks.push_back((b->n[i] + 255) / 256);
+        }
+        fb.stage(ma, blocks, p3m::batched_morton_keys);
+        std::vector<uint32_t*> kin(who.size()), vin(who.size());
+        for (size_t j = 0; j < who.size(); ++j) {
+            kin[j] = b->sims[who[j]]->keys;
+            vin[j] = b->sims[who[j]]->vals;
+        }
+        fused_radix(fb, b, who, bits, kin, vin);
+        std::vector<p3m::PermuteArgs> pa;
+        for (size_t j = 0; j < who.size(); ++j) {
+            p3m_ctx* c = b->sims[who[j]];
+            const int n = b->n[who[j]];
+            pa.push_back({vin[j], c->bodies, c->accel, c->materials, c->bodies_alt, c->accel_alt,
+                          c->materials_alt, c->destinations, n});
+            const size_t tail = (size_t)c->cfg.capacity - (size_t)n;
+            if (tail > 0) {
+                float4* bs = c->bodies + n; float4* bd = c->bodies_alt + n;
+                float2* as = c->accel + n; float2* ad = c->accel_alt + n;
+                float4* ms = c->materials + n; float4* md = c->materials_alt + n;
+                fb.raw([=](unsigned char*, cudaStream_t st) {
+                    cudaError_t e = cudaMemcpyAsync(bd, bs, tail * sizeof(float4), cudaMemcpyDeviceToDevice, st);
+                    if (e == cudaSuccess) e = cudaMemcpyAsync(ad, as, tail * sizeof(float2), cudaMemcpyDeviceToDevice, st);
+                    if (e == cudaSuccess) e = cudaMemcpyAsync(md, ms, tail * sizeof(float4), cudaMemcpyDeviceToDevice, st);
+                    return e;
+                });
+            }
+            role[who[j]].bodies = c->bodies_alt;
+            role[who[j]].accel = c->accel_alt;
+            role[who[j]].materials = c->materials_alt;
+            plan.swap[who[j]] = 1;
+        }
+        fb.stage(pa, blocks, p3m::batched_permute);
+    }
+    // 2. Drift, with the home-cell keys.
+    {
+        std::vector<p3m::DriftArgs> da;
+        std::vector<int> blocks;
+        for (size_t i = 0; i < S; ++i) {
+            if (b->n[i] <= 0) continue;
+            p3m_ctx* c = b->sims[i];
+            const float dt = c->cfg.time_step;
+            da.push_back({role[i].bodies, role[i].accel, c->keys, c->vals, c->status, b->n[i],
+                          0.5f * dt, dt / (float)c->cfg.drift_substeps, c->cfg.drift_substeps,
+                          c->grid.bounded, c->grid.W, c->grid.H});
+            blocks.push_back((b->n[i] + 255) / 256);
+        }
+        fb.stage(da, blocks, p3m::batched_drift);
+    }
+    // 3. Cell lists (simulations with mutual gravity).
+    std::vector<int> mut;
+    for (size_t i = 0; i < S; ++i)
+        if (b->sims[i]->mutual && b->n[i] > 0) mut.push_back((int)i);
+    {
+        std::vector<int> bits;
+        std::vector<uint32_t*> kin, vin;
+        for (int i : mut) {
+            bits.push_back(bits_for(phys_cells(b->sims[i])));
+            kin.push_back(b->sims[i]->keys);
+            vin.push_back(b->sims[i]->vals);
+        }
+        fused_radix(fb, b, mut, bits, kin, vin);
+        std::vector<p3m::ZeroArgs> za;
+        std::vector<int> zb;
+        std::vector<p3m::CellBuildArgs> ca;
+        std::vector<int> cb;
+        for (size_t j = 0; j < mut.size(); ++j) {
+            p3m_ctx* c = b->sims[mut[j]];
+            const long long P = (long long)phys_cells(c);
+            const int zblocks = (int)((P + p3m::kBatchThreads * 16 - 1) / (p3m::kBatchThreads * 16));
+            za.push_back({reinterpret_cast<uint32_t*>(c->cell_count), P});
+            za.push_back({c->cell_mass, P});
+            zb.push_back(zblocks);
+            zb.push_back(zblocks);
+            role[mut[j]].sk = kin[j];
+            role[mut[j]].sv = vin[j];
+            ca.push_back({kin[j], vin[j], role[mut[j]].bodies, role[mut[j]].materials,
+                          c->cell_start, c->cell_count, c->cell_mass, c->entries, b->n[mut[j]]});
+            cb.push_back((b->n[mut[j]] + 255) / 256);
+        }
+        fb.stage(za, zb, p3m::batched_zero);
+        fb.stage(ca, cb, p3m::batched_cell_build);
+    }
+    // 4. Mesh force: clear, deposit, FFT with the Green's multiply, inverse.
+    {
+        std::vector<p3m::ZeroArgs> za;
+        std::vector<int> zb;
+        for (int i : mut) {
+            p3m_ctx* c = b->sims[i];
+            const bool i64 = c->cfg.deposit_mode == P3M_DEPOSIT_I64;
+            const long long words = (long long)mesh_cells(c) * (i64 ? 2 : 1);
+            za.push_back({static_cast<uint32_t*>(c->density), words});
+            zb.push_back((int)((words + p3m::kBatchThreads * 16 - 1) / (p3m::kBatchThreads * 16)));
+        }
+        fb.stage(za, zb, p3m::batched_zero);
+        for (int mode : {P3M_DEPOSIT_U32, P3M_DEPOSIT_I64}) {
+            std::vector<p3m::DepositArgs> dep;
+            std::vector<int> db;
+            std::vector<p3m::FftRowsArgs> fr;
+            std::vector<int> fblocks;
+            size_t smem = 0;
+            for (int i : mut) {
+                p3m_ctx* c = b->sims[i];
+                if (c->cfg.deposit_mode != mode) continue;
+                const p3m::GridShape& g = c->grid;
+                const bool i64 = mode == P3M_DEPOSIT_I64;
+                dep.push_back({c->entries, role[i].sk, c->density, b->n[i], g.W, g.H, g.MW, g.MH,
+                               i64 ? 4294967296.0f : (float)c->mass_scale});
+                db.push_back(p3m::chunk_deposit_blocks(b->n[i]));
+                int rp, cp, ip;
+                size_t rs, cs, is;
+                p3m::fft_batch_shape(g, &rp, &cp, &ip, &rs, &cs, &is);
+                fr.push_back({c->density, c->half, i64 ? 1.0f / 4294967296.0f : 1.0f / (float)c->mass_scale,
+                              g.MW, g.MH, rp});
+                fblocks.push_back((g.MH / 2 + rp - 1) / rp);
+                smem = std::max(smem, rs);
+            }
+            fb.stage(dep, db, [mode](const p3m::DepositArgs* a, p3m::BatchGrid g, cudaStream_t st) {
+                return p3m::batched_deposit(a, g, mode, st);
+            });
+            const float2* tw0 = mut.empty() ? nullptr : b->sims[mut[0]]->twiddles;
+            fb.stage(fr, fblocks, [mode, smem, tw0](const p3m::FftRowsArgs* a, p3m::BatchGrid g, cudaStream_t st) {
+                return p3m::batched_fft_rows(a, g, mode, smem, tw0, st);
+            });
+        }
+        std::vector<p3m::FftColumnsArgs> fc;
+        std::vector<p3m::FftInverseArgs> fi;
+        std::vector<int> cbk, ibk;
+        size_t csm = 0, ism = 0;
+        for (int i : mut) {
+            p3m_ctx* c = b->sims[i];
+            const p3m::GridShape& g = c->grid;
+            int rp, cp, ip;
+            size_t rs, cs, is;
+            p3m::fft_batch_shape(g, &rp, &cp, &ip, &rs, &cs, &is);
+            fc.push_back({c->half, c->green, c->cols, 1.0f / c->normalization_mass, g.MW, g.MH, cp});
+            cbk.push_back((g.MW / 2 + 1 + cp - 1) / cp);
+            fi.push_back({c->cols, c->force, g.MW, g.MH, ip});
+            ibk.push_back((g.MH + ip - 1) / ip);
+            csm = std::max(csm, cs);
+            ism = std::max(ism, is);
+        }
+        const float2* tw0 = mut.empty() ? nullptr : b->sims[mut[0]]->twiddles;
+        fb.stage(fc, cbk, [csm, tw0](const p3m::FftColumnsArgs* a, p3m::BatchGrid g, cudaStream_t st) {
+            return p3m::batched_fft_columns(a, g, csm, tw0, st);
+        });
+        fb.stage(fi, ibk, [ism, tw0](const p3m::FftInverseArgs* a, p3m::BatchGrid g, cudaStream_t st) {
+            return p3m::batched_fft_inverse(a, g, ism, tw0, st);
+        });
+    }
+    // 5. Short range (by stencil shape), then interpolation + kick.
+    {
+        std::map<int, std::vector<int>> groups;  // rx * 64 + ry * 2 + exact2
+        for (int i : mut) {
+            const p3m_ctx* c = b->sims[i];
+            groups[c->rx * 64 + c->ry * 2 + (c->cfg.exact_neighbor_body_limit == 2 ? 1 : 0)].push_back(i);
+        }
+        for (const auto& kv : groups) {
+            std::vector<p3m::ShortRangeArgs> sa;
+            std::vector<int> sb;
+            for (int i : kv.second) {
+                p3m_ctx* c = b->sims[i];
+                sa.push_back({role[i].bodies, c->entries, c->cell_start, c->cell_count, c->cell_mass,
+                              c->a_short, kick_params(c, b->n[i], 0)});
+                sb.push_back((b->n[i] + p3m::kBatchThreads - 1) / p3m::kBatchThreads);
+            }
+            const int rx = kv.first / 64, ry = (kv.first % 64) / 2, ex = kv.first % 2;
+            fb.stage(sa, sb, [rx, ry, ex](const p3m::ShortRangeArgs* a, p3m::BatchGrid g, cudaStream_t st) {
+                return p3m::batched_short_range(a, g, rx, ry, ex, st);
+            });
+        }
+        std::vector<p3m::KickArgs> ka;
+        std::vector<int> kb;
+        for (size_t i = 0; i < S; ++i) {
+            if (b->n[i] <= 0) continue;
+            p3m_ctx* c = b->sims[i];
+            ka.push_back({role[i].bodies, role[i].accel, c->force, c->a_short, kick_params(c, b->n[i], 0)});
+            kb.push_back((b->n[i] + p3m::kBatchThreads - 1) / p3m::kBatchThreads);
+        }
+        fb.stage(ka, kb, p3m::batched_interp_kick);
+    }
+    plan.sorted.resize(S);
+    for (size_t i = 0; i < S; ++i) plan.sorted[i] = {role[i].sk, role[i].sv};
+
+    // Upload the arguments, capture the launches.
+    cudaError_t e = cudaMalloc(&plan.blob, std::max<size_t>(fb.blob.host.size(), 16));
+    if (e != cudaSuccess) return batch_fail(b, P3M_ERR_OUT_OF_MEMORY, "fused plan arguments");
+    e = cudaMemcpyAsync(plan.blob, fb.blob.host.data(), fb.blob.host.size(), cudaMemcpyHostToDevice, b->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(b->stream);
+    if (e != cudaSuccess) return batch_fail(b, P3M_ERR_CUDA, cudaGetErrorString(e));
+    unsigned char* dev = static_cast<unsigned char*>(plan.blob);
+    const long long k0 = p3m_kernel_launches();
+    e = cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal);
+    if (e != cudaSuccess) return batch_fail(b, P3M_ERR_CUDA, cudaGetErrorString(e));
+    cudaError_t le = cudaSuccess;
+    for (auto& fn : fb.launches) {
+        le = fn(dev, b->stream);
+        if (le != cudaSuccess) break;
+    }
+    cudaGraph_t graph = nullptr;
+    e = cudaStreamEndCapture(b->stream, &graph);
+    if (le != cudaSuccess || e != cudaSuccess) {
+        if (graph) cudaGraphDestroy(graph);
+        return batch_fail(b, P3M_ERR_CUDA, std::string("fused capture: ") +
+                                               cudaGetErrorString(le != cudaSuccess ? le : e));
+    }
+    plan.kernels = p3m_kernel_launches() - k0;
+    e = cudaGraphInstantiate(&plan.exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (e != cudaSuccess) return batch_fail(b, P3M_ERR_CUDA, std::string("fused instantiate: ") + cudaGetErrorString(e));
+    return P3M_OK;
+}
+
+int batch_fused_step(p3m_batch* b, const std::vector<char>& sort, const std::vector<uint64_t>& key) {
+    p3m_batch::Plan* plan = nullptr;
+    for (auto& p : b->plans)
+        if (p.key == key) { plan = &p; break; }
+    if (!plan) {
+        p3m_batch::Plan fresh;
+        fresh.key = key;
+        int st = build_fused(b, sort, fresh);
+        if (st != P3M_OK) {
+            if (fresh.exec) cudaGraphExecDestroy(fresh.exec);
+            if (fresh.blob) cudaFree(fresh.blob);
+            return st;
+        }
+        if (b->plans.size() >= 8) {
+            cudaGraphExecDestroy(b->plans.front().exec);
+            cudaFree(b->plans.front().blob);
+            b->plans.erase(b->plans.begin());
+        }
+        b->plans.push_back(std::move(fresh));
+        plan = &b->plans.back();
+    }
+    cudaError_t e = cudaGraphLaunch(plan->exec, b->stream);
+    if (e != cudaSuccess) return batch_fail(b, P3M_ERR_CUDA, cudaGetErrorString(e));
+    p3m::count_launches((int)plan->kernels);
+    for (size_t i = 0; i < b->sims.size(); ++i) {
+        p3m_ctx* c = b->sims[i];
+        if (plan->swap[i]) swap_body_buffers(c);
+        if (c->mutual && b->n[i] > 0) {
+            c->sorted_keys = plan->sorted[i].first;
+            c->sorted_ids = plan->sorted[i].second;
+        }
+    }
     return P3M_OK;
 }
 
@@ -1306,6 +1699,15 @@ int p3m_batch_autotune(p3m_batch* b, int32_t trial_steps, int32_t* chosen) {
         }
         ++tuned;
     }
+    return P3M_OK;
+}
+
+int p3m_batch_set_fused(p3m_batch* b, int32_t enabled) {
+    if (!b) return P3M_ERR_INVALID_ARGUMENT;
+    cudaError_t e = cudaStreamSynchronize(b->stream);
+    if (e != cudaSuccess) return batch_fail(b, P3M_ERR_CUDA, cudaGetErrorString(e));
+    batch_drop_graphs(b);
+    b->fused = enabled != 0;
     return P3M_OK;
 }
 

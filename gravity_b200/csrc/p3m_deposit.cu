@@ -419,15 +419,15 @@ constexpr int kChunkEntries = 2048;
 constexpr int kWindowBytes = 96 * 1024;
 
 template <typename T>
-__global__ void __launch_bounds__(kThreads) deposit_chunks_kernel(
-    const float4* __restrict__ entries, const uint32_t* __restrict__ keys, int n, int W, int H,
-    int MW, int MH, float scale, T* __restrict__ density, int window_cap) {
+__device__ __forceinline__ void deposit_chunks_body(
+    int block, const float4* __restrict__ entries, const uint32_t* __restrict__ keys, int n, int W,
+    int H, int MW, int MH, float scale, T* __restrict__ density, int window_cap) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     T* window = reinterpret_cast<T*>(smem_raw);
     __shared__ long long s_lo;
     __shared__ int s_len;
 
-    const int base = blockIdx.x * kChunkEntries;
+    const int base = block * kChunkEntries;
     const int count = min(kChunkEntries, n - base);
     if (threadIdx.x == 0) {
         const uint32_t c0 = keys[base], c1 = keys[base + count - 1];
@@ -478,6 +478,22 @@ __global__ void __launch_bounds__(kThreads) deposit_chunks_kernel(
     }
 }
 
+template <typename T>
+__global__ void __launch_bounds__(kThreads) deposit_chunks_kernel(
+    const float4* __restrict__ entries, const uint32_t* __restrict__ keys, int n, int W, int H,
+    int MW, int MH, float scale, T* __restrict__ density, int window_cap) {
+    deposit_chunks_body<T>(blockIdx.x, entries, keys, n, W, H, MW, MH, scale, density, window_cap);
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kThreads) deposit_chunks_batched_kernel(
+    const DepositArgs* __restrict__ args, const int* __restrict__ first, int sims) {
+    const int2 sb = batch_block(first, sims);
+    const DepositArgs a = args[sb.x];
+    deposit_chunks_body<T>(sb.y, a.entries, a.keys, a.n, a.W, a.H, a.MW, a.MH, a.scale,
+                           static_cast<T*>(a.density), kWindowBytes / (int)sizeof(T));
+}
+
 TileGeom tile_geom(const GridShape& g) {
     TileGeom t;
     t.W = g.W; t.H = g.H; t.MW = g.MW; t.MH = g.MH;
@@ -492,12 +508,34 @@ TileGeom tile_geom(const GridShape& g) {
 }  // namespace
 
 cudaError_t configure_deposit() {
-    cudaError_t e = cudaFuncSetAttribute(deposit_chunks_kernel<unsigned long long>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, kWindowBytes);
-    if (e != cudaSuccess) return e;
-    return cudaFuncSetAttribute(deposit_chunks_kernel<uint32_t>,
-                                cudaFuncAttributeMaxDynamicSharedMemorySize, kWindowBytes);
+    const void* fns[] = {(const void*)deposit_chunks_kernel<unsigned long long>,
+                         (const void*)deposit_chunks_kernel<uint32_t>,
+                         (const void*)deposit_chunks_batched_kernel<unsigned long long>,
+                         (const void*)deposit_chunks_batched_kernel<uint32_t>};
+    for (const void* f : fns) {
+        cudaError_t e = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             kWindowBytes);
+        if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
 }
+
+int chunk_deposit_blocks(int n) { return n > 0 ? (n + kChunkEntries - 1) / kChunkEntries : 0; }
+int chunk_deposit_smem() { return kWindowBytes; }
+
+cudaError_t batched_deposit(const DepositArgs* a, BatchGrid g, int deposit_mode, cudaStream_t s) {
+    if (g.blocks <= 0) return cudaSuccess;
+    if (deposit_mode == P3M_DEPOSIT_I64)
+        deposit_chunks_batched_kernel<unsigned long long><<<g.blocks, kThreads, kWindowBytes, s>>>(
+            a, g.first, g.sims);
+    else
+        deposit_chunks_batched_kernel<uint32_t><<<g.blocks, kThreads, kWindowBytes, s>>>(
+            a, g.first, g.sims);
+    count_launches(1);
+    return cudaGetLastError();
+}
+
+bool deposit_uses_cell_starts(int n) { return n >= kTileMinBodies; }
 
 size_t deposit_work_entries(int capacity, int MW, int MH) {
     // Each body lies in the runs of at most 2 x 2 tiles; a tile has at most

@@ -15,11 +15,13 @@ namespace {
 
 __device__ __forceinline__ float fractf(float v) { return v - floorf(v); }
 
-__global__ void drift_kernel(float4* __restrict__ bodies, const float2* __restrict__ accel, int n,
-                             float half_kick, float drift_dt, int substeps, int bounded, int W,
-                             int H, uint32_t* __restrict__ keys, uint32_t* __restrict__ vals,
-                             unsigned int* __restrict__ nonfinite) {
-    const int id = blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void drift_body(int block, float4* __restrict__ bodies,
+                                           const float2* __restrict__ accel, int n,
+                                           float half_kick, float drift_dt, int substeps,
+                                           int bounded, int W, int H, uint32_t* __restrict__ keys,
+                                           uint32_t* __restrict__ vals,
+                                           unsigned int* __restrict__ nonfinite) {
+    const int id = block * blockDim.x + threadIdx.x;
     if (id >= n) return;
     float4 b = bodies[id];
     const float2 a = accel[id];
@@ -51,7 +53,30 @@ __global__ void drift_kernel(float4* __restrict__ bodies, const float2* __restri
     }
 }
 
+__global__ void drift_kernel(float4* __restrict__ bodies, const float2* __restrict__ accel, int n,
+                             float half_kick, float drift_dt, int substeps, int bounded, int W,
+                             int H, uint32_t* __restrict__ keys, uint32_t* __restrict__ vals,
+                             unsigned int* __restrict__ nonfinite) {
+    drift_body(blockIdx.x, bodies, accel, n, half_kick, drift_dt, substeps, bounded, W, H, keys,
+               vals, nonfinite);
+}
+
+__global__ void drift_batched_kernel(const DriftArgs* __restrict__ args, const int* __restrict__ first,
+                                     int sims) {
+    const int2 sb = batch_block(first, sims);
+    const DriftArgs a = args[sb.x];
+    drift_body(sb.y, a.bodies, a.accel, a.n, a.half_kick, a.drift_dt, a.substeps, a.bounded, a.W,
+               a.H, a.keys, a.vals, a.nonfinite);
+}
+
 }  // namespace
+
+cudaError_t batched_drift(const DriftArgs* a, BatchGrid g, cudaStream_t s) {
+    if (g.blocks <= 0) return cudaSuccess;
+    drift_batched_kernel<<<g.blocks, kBatchThreads, 0, s>>>(a, g.first, g.sims);
+    count_launches(1);
+    return cudaGetLastError();
+}
 
 cudaError_t launch_drift(float4* bodies, const float2* accel, int n, float half_kick, float drift_dt,
                          int substeps, GridShape g, uint32_t* keys, uint32_t* vals,

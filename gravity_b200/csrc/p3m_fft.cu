@@ -147,13 +147,13 @@ __device__ __forceinline__ int ilog2(int v) { return 31 - __clz(v); }
 // 1. forward rows: fft_init.comp (fixed point -> float) fused with the row
 // transform. Two rows per complex line.
 template <typename T>
-__global__ void __launch_bounds__(256) fft_rows_forward_kernel(const T* __restrict__ density,
-                                                               float inv_scale, int MW, int MH,
-                                                               int pairs_per_cta,
-                                                               const float2* __restrict__ tw,
-                                                               float2* __restrict__ half) {
+__device__ __forceinline__ void fft_rows_forward_body(int block, const T* __restrict__ density,
+                                                      float inv_scale, int MW, int MH,
+                                                      int pairs_per_cta,
+                                                      const float2* __restrict__ tw,
+                                                      float2* __restrict__ half) {
     extern __shared__ __align__(16) float2 sm[];
-    const int pair0 = blockIdx.x * pairs_per_cta;
+    const int pair0 = block * pairs_per_cta;
     const int pairs = min(pairs_per_cta, MH / 2 - pair0);
     float2* a = sm;
     float2* b = sm + pairs_per_cta * MW;
@@ -179,16 +179,35 @@ __global__ void __launch_bounds__(256) fft_rows_forward_kernel(const T* __restri
     }
 }
 
+template <typename T>
+__global__ void __launch_bounds__(256) fft_rows_forward_kernel(const T* __restrict__ density,
+                                                               float inv_scale, int MW, int MH,
+                                                               int pairs_per_cta,
+                                                               const float2* __restrict__ tw,
+                                                               float2* __restrict__ half) {
+    fft_rows_forward_body<T>(blockIdx.x, density, inv_scale, MW, MH, pairs_per_cta, tw, half);
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) fft_rows_forward_batched_kernel(
+    const FftRowsArgs* __restrict__ args, const int* __restrict__ first, int sims,
+    const float2* __restrict__ tw) {
+    const int2 sb = batch_block(first, sims);
+    const FftRowsArgs a = args[sb.x];
+    fft_rows_forward_body<T>(sb.y, static_cast<const T*>(a.density), a.inv_scale, a.MW, a.MH,
+                             a.per_cta, tw, a.half);
+}
+
 // 2. columns: forward along y, Green's multiply (convolve.comp), inverse of Fx
 // and Fy along y. Shared memory: [A: G lines | B: G lines | C: 2G lines].
-__global__ void __launch_bounds__(256) fft_columns_kernel(const float2* __restrict__ half,
-                                                          const float2* __restrict__ green,
-                                                          float inv_total, int MW, int MH, int G,
-                                                          const float2* __restrict__ tw,
-                                                          float4* __restrict__ cols) {
+__device__ __forceinline__ void fft_columns_body(int block, const float2* __restrict__ half,
+                                                 const float2* __restrict__ green, float inv_total,
+                                                 int MW, int MH, int G,
+                                                 const float2* __restrict__ tw,
+                                                 float4* __restrict__ cols) {
     extern __shared__ __align__(16) float2 sm[];
     const int SW = MW / 2 + 1;
-    const int kx0 = blockIdx.x * G;
+    const int kx0 = block * G;
     const int ncols = min(G, SW - kx0);
     const int logH = ilog2(MH);
     float2* A = sm;
@@ -215,6 +234,22 @@ __global__ void __launch_bounds__(256) fft_columns_kernel(const float2* __restri
         const float2 fx = F[c * MH + y], fy = F[(ncols + c) * MH + y];
         cols[(size_t)y * SW + kx0 + c] = make_float4(fx.x, fx.y, fy.x, fy.y);
     }
+}
+
+__global__ void __launch_bounds__(256) fft_columns_kernel(const float2* __restrict__ half,
+                                                          const float2* __restrict__ green,
+                                                          float inv_total, int MW, int MH, int G,
+                                                          const float2* __restrict__ tw,
+                                                          float4* __restrict__ cols) {
+    fft_columns_body(blockIdx.x, half, green, inv_total, MW, MH, G, tw, cols);
+}
+
+__global__ void __launch_bounds__(256) fft_columns_batched_kernel(
+    const FftColumnsArgs* __restrict__ args, const int* __restrict__ first, int sims,
+    const float2* __restrict__ tw) {
+    const int2 sb = batch_block(first, sims);
+    const FftColumnsArgs a = args[sb.x];
+    fft_columns_body(sb.y, a.half, a.green, a.inv_total, a.MW, a.MH, a.per_cta, tw, a.cols);
 }
 
 // 2'. columns of the adjoint (transposed) mesh operator. `half` holds the
@@ -286,12 +321,12 @@ __global__ void __launch_bounds__(256) fft_columns_forward_kernel(float2* half, 
 
 // 3. inverse rows: Z = Fx + i Fy over the full row from the two half spectra
 // (each Hermitian in kx), one complex inverse, (fx, fy) = (Re, Im).
-__global__ void __launch_bounds__(256) fft_rows_inverse_kernel(const float4* __restrict__ cols,
-                                                               int MW, int MH, int rows_per_cta,
-                                                               const float2* __restrict__ tw,
-                                                               float2* __restrict__ force) {
+__device__ __forceinline__ void fft_rows_inverse_body(int block, const float4* __restrict__ cols,
+                                                      int MW, int MH, int rows_per_cta,
+                                                      const float2* __restrict__ tw,
+                                                      float2* __restrict__ force) {
     extern __shared__ __align__(16) float2 sm[];
-    const int row0 = blockIdx.x * rows_per_cta;
+    const int row0 = block * rows_per_cta;
     const int rows = min(rows_per_cta, MH - row0);
     const int SW = MW / 2 + 1;
     float2* a = sm;
@@ -313,6 +348,21 @@ __global__ void __launch_bounds__(256) fft_rows_inverse_kernel(const float4* __r
         const int r = t / MW, x = t - r * MW;
         force[(size_t)(row0 + r) * MW + x] = z[r * MW + x];
     }
+}
+
+__global__ void __launch_bounds__(256) fft_rows_inverse_kernel(const float4* __restrict__ cols,
+                                                               int MW, int MH, int rows_per_cta,
+                                                               const float2* __restrict__ tw,
+                                                               float2* __restrict__ force) {
+    fft_rows_inverse_body(blockIdx.x, cols, MW, MH, rows_per_cta, tw, force);
+}
+
+__global__ void __launch_bounds__(256) fft_rows_inverse_batched_kernel(
+    const FftInverseArgs* __restrict__ args, const int* __restrict__ first, int sims,
+    const float2* __restrict__ tw) {
+    const int2 sb = batch_block(first, sims);
+    const FftInverseArgs a = args[sb.x];
+    fft_rows_inverse_body(sb.y, a.cols, a.MW, a.MH, a.per_cta, tw, a.force);
 }
 
 // ------------------------------------------------------- FP64 Green's table
@@ -432,6 +482,10 @@ cudaError_t configure_fft() {
                          (const void*)fft_rows_forward_kernel<uint32_t>,
                          (const void*)fft_rows_forward_kernel<float>,
                          (const void*)fft_columns_adjoint_kernel,
+                         (const void*)fft_rows_forward_batched_kernel<long long>,
+                         (const void*)fft_rows_forward_batched_kernel<uint32_t>,
+                         (const void*)fft_columns_batched_kernel,
+                         (const void*)fft_rows_inverse_batched_kernel,
                          (const void*)fft_columns_kernel, (const void*)fft_columns_forward_kernel,
                          (const void*)fft_rows_inverse_kernel, (const void*)fft64_line_kernel};
     for (const void* f : fns) {
@@ -518,6 +572,46 @@ cudaError_t launch_fft_adjoint(const float* cotangent, const float2* green, floa
                                                                twiddles, mu2);
         count_launches(1);
     }
+    return cudaGetLastError();
+}
+
+void fft_batch_shape(const GridShape& g, int* rows_per_cta, int* cols_per_cta, int* inv_per_cta,
+                     size_t* rows_smem, size_t* cols_smem, size_t* inv_smem) {
+    int threads;
+    line_shape(g.MH / 2, g.MW, g.MW >= 4096 ? 1 : 4096 / g.MW, rows_per_cta, &threads, g.fft_lines);
+    *rows_smem = (size_t)2 * *rows_per_cta * g.MW * sizeof(float2);
+    column_shape(g.MW, g.MH, 4, cols_per_cta, &threads, g.fft_lines);
+    *cols_smem = (size_t)4 * *cols_per_cta * g.MH * sizeof(float2);
+    line_shape(g.MH, g.MW, g.MW >= 4096 ? 1 : 4096 / g.MW, inv_per_cta, &threads, g.fft_lines);
+    *inv_smem = (size_t)2 * *inv_per_cta * g.MW * sizeof(float2);
+}
+
+cudaError_t batched_fft_rows(const FftRowsArgs* a, BatchGrid g, int deposit_mode, size_t smem,
+                             const float2* twiddles, cudaStream_t s) {
+    if (g.blocks <= 0) return cudaSuccess;
+    if (deposit_mode == P3M_DEPOSIT_I64)
+        fft_rows_forward_batched_kernel<long long><<<g.blocks, 256, smem, s>>>(a, g.first, g.sims,
+                                                                               twiddles);
+    else
+        fft_rows_forward_batched_kernel<uint32_t><<<g.blocks, 256, smem, s>>>(a, g.first, g.sims,
+                                                                              twiddles);
+    count_launches(1);
+    return cudaGetLastError();
+}
+
+cudaError_t batched_fft_columns(const FftColumnsArgs* a, BatchGrid g, size_t smem,
+                                const float2* twiddles, cudaStream_t s) {
+    if (g.blocks <= 0) return cudaSuccess;
+    fft_columns_batched_kernel<<<g.blocks, 256, smem, s>>>(a, g.first, g.sims, twiddles);
+    count_launches(1);
+    return cudaGetLastError();
+}
+
+cudaError_t batched_fft_inverse(const FftInverseArgs* a, BatchGrid g, size_t smem,
+                                const float2* twiddles, cudaStream_t s) {
+    if (g.blocks <= 0) return cudaSuccess;
+    fft_rows_inverse_batched_kernel<<<g.blocks, 256, smem, s>>>(a, g.first, g.sims, twiddles);
+    count_launches(1);
     return cudaGetLastError();
 }
 

@@ -131,6 +131,9 @@ cudaError_t launch_cell_build(const uint32_t* keys, const uint32_t* ids, int n,
 // sorted cells; cell_start: the full CSR). Writes every mesh cell.
 // work: deposit_work_entries(capacity, MW, MH) int4 + 1 counter.
 size_t deposit_work_entries(int capacity, int MW, int MH);
+// Whether launch_deposit reads cell_start for n bodies (it then needs the full
+// CSR); otherwise it reads `keys`.
+bool deposit_uses_cell_starts(int n);
 cudaError_t launch_deposit(const float4* entries, const uint32_t* keys, const int* cell_start,
                            int n, GridShape g, int deposit_mode, float mass_scale, void* density,
                            int4* work, int* work_count, int work_capacity, cudaStream_t stream);
@@ -223,6 +226,95 @@ cudaError_t launch_conservation(const float4* bodies, const float4* materials, i
 
 // Process-wide count of kernels launched by this library (p3m_kernel_launches).
 void count_launches(int kernels);
+
+// ------------------------------------------------------- batched launches
+// One launch runs a stage for many simulations: CTA b runs local block
+// b - first[s] of simulation s, where first[] (sims + 1 entries, on the
+// device) is the prefix of the simulations' block counts; a simulation with
+// no blocks is skipped. Each launcher takes the per-simulation arguments as a
+// device array of its Args struct.
+__device__ __forceinline__ int2 batch_block(const int* __restrict__ first, int sims) {
+    int lo = 0, hi = sims - 1;
+    const int b = (int)blockIdx.x;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (__ldg(&first[mid]) <= b) lo = mid;
+        else hi = mid - 1;
+    }
+    return make_int2(lo, b - __ldg(&first[lo]));
+}
+
+struct BatchGrid {
+    const int* first;  // device, sims + 1
+    int sims;
+    int blocks;        // first[sims]
+};
+
+struct DriftArgs {
+    float4* bodies; const float2* accel; uint32_t* keys; uint32_t* vals; unsigned int* nonfinite;
+    int n; float half_kick, drift_dt; int substeps, bounded, W, H;
+};
+struct MortonArgs { const float4* bodies; uint32_t* keys; uint32_t* vals; int n, wbits, hbits; };
+struct RadixArgs {
+    const uint32_t* keys_in; const uint32_t* vals_in; uint32_t* keys_out; uint32_t* vals_out;
+    uint32_t* hist; int n, shift, bits, tiles;
+};
+struct ScanArgs { uint32_t* data; int n; };
+struct PermuteArgs {
+    const uint32_t* order; const float4* bodies; const float2* accel; const float4* materials;
+    float4* bodies_out; float2* accel_out; float4* materials_out; uint32_t* destinations; int n;
+};
+struct CellBuildArgs {
+    const uint32_t* keys; const uint32_t* ids; const float4* bodies; const float4* materials;
+    int* cell_start; int* cell_count; uint32_t* cell_mass; float4* entries; int n;
+};
+struct ZeroArgs { uint32_t* data; long long words; };  // words of 4 bytes
+struct DepositArgs {
+    const float4* entries; const uint32_t* keys; void* density; int n, W, H, MW, MH; float scale;
+};
+struct FftRowsArgs {
+    const void* density; float2* half; float inv_scale; int MW, MH, per_cta;
+};
+struct FftColumnsArgs {
+    const float2* half; const float2* green; float4* cols; float inv_total; int MW, MH, per_cta;
+};
+struct FftInverseArgs { const float4* cols; float2* force; int MW, MH, per_cta; };
+struct ShortRangeArgs {
+    const float4* bodies; const float4* entries; const int* cell_start; const int* cell_count;
+    const uint32_t* cell_mass; float2* a_short; KickParams p;
+};
+struct KickArgs {
+    float4* bodies; float2* accel; const float2* force; const float2* a_short; KickParams p;
+};
+
+constexpr int kBatchThreads = 256;      // every batched launch but the scan
+constexpr int kBatchScanThreads = 1024;
+int radix_tiles(int n);                 // tiles (CTAs) of one radix pass over n keys
+int radix_scan_limit();                 // largest histogram one scan CTA takes
+int chunk_deposit_blocks(int n);        // CTAs of the entry-chunk deposit
+int chunk_deposit_smem();               // its shared window, bytes
+void fft_batch_shape(const GridShape& g, int* rows_per_cta, int* cols_per_cta, int* inv_per_cta,
+                     size_t* rows_smem, size_t* cols_smem, size_t* inv_smem);
+
+cudaError_t batched_drift(const DriftArgs* a, BatchGrid g, cudaStream_t s);
+cudaError_t batched_morton_keys(const MortonArgs* a, BatchGrid g, cudaStream_t s);
+cudaError_t batched_radix_hist(const RadixArgs* a, BatchGrid g, cudaStream_t s);
+cudaError_t batched_scan(const ScanArgs* a, BatchGrid g, cudaStream_t s);  // one CTA each
+cudaError_t batched_radix_scatter(const RadixArgs* a, BatchGrid g, cudaStream_t s);
+cudaError_t batched_permute(const PermuteArgs* a, BatchGrid g, cudaStream_t s);
+cudaError_t batched_cell_build(const CellBuildArgs* a, BatchGrid g, cudaStream_t s);
+cudaError_t batched_zero(const ZeroArgs* a, BatchGrid g, cudaStream_t s);
+cudaError_t batched_deposit(const DepositArgs* a, BatchGrid g, int deposit_mode, cudaStream_t s);
+cudaError_t batched_fft_rows(const FftRowsArgs* a, BatchGrid g, int deposit_mode, size_t smem,
+                             const float2* twiddles, cudaStream_t s);
+cudaError_t batched_fft_columns(const FftColumnsArgs* a, BatchGrid g, size_t smem,
+                                const float2* twiddles, cudaStream_t s);
+cudaError_t batched_fft_inverse(const FftInverseArgs* a, BatchGrid g, size_t smem,
+                                const float2* twiddles, cudaStream_t s);
+cudaError_t batched_short_range(const ShortRangeArgs* a, BatchGrid g, int rx, int ry, int exact2,
+                                cudaStream_t s);
+cudaError_t batched_interp_kick(const KickArgs* a, BatchGrid g, cudaStream_t s);
+cudaError_t configure_batched();
 
 // Sets the message p3m_last_error(NULL) returns on this thread (entry points
 // without a context).

@@ -14,10 +14,10 @@
 namespace p3m {
 namespace {
 
-__global__ void __launch_bounds__(256) interp_kick_kernel(
-    float4* __restrict__ bodies, float2* __restrict__ accel, const float2* __restrict__ force,
-    const float2* __restrict__ a_short, KickParams p) {
-    const int id = blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void interp_kick_body(
+    int block, float4* __restrict__ bodies, float2* __restrict__ accel,
+    const float2* __restrict__ force, const float2* __restrict__ a_short, const KickParams& p) {
+    const int id = block * blockDim.x + threadIdx.x;
     if (id >= p.n) return;
     float4 b = bodies[id];
     float rx, ry;
@@ -53,7 +53,44 @@ __global__ void __launch_bounds__(256) interp_kick_kernel(
     bodies[id] = b;
 }
 
+__global__ void __launch_bounds__(256) interp_kick_kernel(
+    float4* __restrict__ bodies, float2* __restrict__ accel, const float2* __restrict__ force,
+    const float2* __restrict__ a_short, KickParams p) {
+    interp_kick_body(blockIdx.x, bodies, accel, force, a_short, p);
+}
+
+__global__ void __launch_bounds__(256) interp_kick_batched_kernel(
+    const KickArgs* __restrict__ args, const int* __restrict__ first, int sims) {
+    const int2 sb = batch_block(first, sims);
+    const KickArgs a = args[sb.x];
+    interp_kick_body(sb.y, a.bodies, a.accel, a.force, a.a_short, a.p);
+}
+
 }  // namespace
+
+cudaError_t batched_interp_kick(const KickArgs* a, BatchGrid g, cudaStream_t s) {
+    if (g.blocks <= 0) return cudaSuccess;
+    interp_kick_batched_kernel<<<g.blocks, kBatchThreads, 0, s>>>(a, g.first, g.sims);
+    count_launches(1);
+    return cudaGetLastError();
+}
+
+cudaError_t batched_short_range(const ShortRangeArgs* a, BatchGrid g, int rx, int ry, int exact2,
+                                cudaStream_t s) {
+    if (g.blocks <= 0) return cudaSuccess;
+    cudaError_t e;
+    switch (rx) {
+        case 1: e = batched_short_range_rx<1>(a, g, ry, exact2, s); break;
+        case 2: e = batched_short_range_rx<2>(a, g, ry, exact2, s); break;
+        case 3: e = batched_short_range_rx<3>(a, g, ry, exact2, s); break;
+        case 4: e = batched_short_range_rx<4>(a, g, ry, exact2, s); break;
+        case 5: e = batched_short_range_rx<5>(a, g, ry, exact2, s); break;
+        case 6: e = batched_short_range_rx<6>(a, g, ry, exact2, s); break;
+        default: return cudaErrorInvalidValue;
+    }
+    count_launches(1);
+    return e;
+}
 
 cudaError_t launch_short_range(const float4* bodies, const float4* entries, const int* cell_start,
                                const int* cell_count, const uint32_t* cell_mass, float2* a_short,

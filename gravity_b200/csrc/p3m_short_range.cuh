@@ -72,11 +72,11 @@ __device__ __forceinline__ void pair_add(const PairConst& k, float dx, float dy,
 }
 
 template <int RX, int RY, int EXACT>
-__global__ void __launch_bounds__(256) short_range_kernel(
-    const float4* __restrict__ bodies, const float4* __restrict__ entries,
+__device__ __forceinline__ void short_range_body(
+    int block, const float4* __restrict__ bodies, const float4* __restrict__ entries,
     const int* __restrict__ cell_start, const int* __restrict__ cell_count,
-    const uint32_t* __restrict__ cell_mass, float2* __restrict__ a_short, KickParams p) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t* __restrict__ cell_mass, float2* __restrict__ a_short, const KickParams& p) {
+    const int i = block * blockDim.x + threadIdx.x;
     if (i >= p.n) return;
     const float4 t = bodies[i];
     const uint32_t id = (uint32_t)i;
@@ -147,6 +147,24 @@ __global__ void __launch_bounds__(256) short_range_kernel(
     a_short[id] = make_float2(ax, ay);
 }
 
+template <int RX, int RY, int EXACT>
+__global__ void __launch_bounds__(256) short_range_kernel(
+    const float4* __restrict__ bodies, const float4* __restrict__ entries,
+    const int* __restrict__ cell_start, const int* __restrict__ cell_count,
+    const uint32_t* __restrict__ cell_mass, float2* __restrict__ a_short, KickParams p) {
+    short_range_body<RX, RY, EXACT>(blockIdx.x, bodies, entries, cell_start, cell_count, cell_mass,
+                                    a_short, p);
+}
+
+template <int RX, int RY, int EXACT>
+__global__ void __launch_bounds__(256) short_range_batched_kernel(
+    const ShortRangeArgs* __restrict__ args, const int* __restrict__ first, int sims) {
+    const int2 sb = batch_block(first, sims);
+    const ShortRangeArgs a = args[sb.x];
+    short_range_body<RX, RY, EXACT>(sb.y, a.bodies, a.entries, a.cell_start, a.cell_count,
+                                    a.cell_mass, a.a_short, a.p);
+}
+
 }  // namespace sr
 
 // Launches short_range_kernel<RX, p.ry, 2 or 0>; defined (explicitly
@@ -160,7 +178,13 @@ cudaError_t launch_short_range_rx(const float4* bodies, const float4* entries,
     template <>                                                                                 \
     cudaError_t launch_short_range_rx<RX_>(const float4*, const float4*, const int*, const int*, \
                                            const uint32_t*, float2*, const KickParams&,         \
-                                           cudaStream_t);
+                                           cudaStream_t);                                       \
+    template <>                                                                                 \
+    cudaError_t batched_short_range_rx<RX_>(const ShortRangeArgs*, BatchGrid, int, int,          \
+                                            cudaStream_t);
+template <int RX>
+cudaError_t batched_short_range_rx(const ShortRangeArgs* a, BatchGrid g, int ry, int exact2,
+                                   cudaStream_t stream);
 P3M_DECLARE_SHORT_RANGE_RX(1)
 P3M_DECLARE_SHORT_RANGE_RX(2)
 P3M_DECLARE_SHORT_RANGE_RX(3)
@@ -190,6 +214,27 @@ P3M_DECLARE_SHORT_RANGE_RX(6)
             case 10: sr::short_range_kernel<RX_, 5, 0><<<grid, block, 0, stream>>>(bodies, entries, cell_start, cell_count, cell_mass, a_short, p); break; \
             case 13: sr::short_range_kernel<RX_, 6, 2><<<grid, block, 0, stream>>>(bodies, entries, cell_start, cell_count, cell_mass, a_short, p); break; \
             case 12: sr::short_range_kernel<RX_, 6, 0><<<grid, block, 0, stream>>>(bodies, entries, cell_start, cell_count, cell_mass, a_short, p); break; \
+            default: return cudaErrorInvalidValue;                                              \
+        }                                                                                       \
+        return cudaGetLastError();                                                              \
+    }                                                                                           \
+    template <>                                                                                 \
+    cudaError_t batched_short_range_rx<RX_>(const ShortRangeArgs* a, BatchGrid g, int ry,       \
+                                            int exact2, cudaStream_t stream) {                  \
+        const dim3 grid(g.blocks), block(kBatchThreads);                                        \
+        switch (ry * 2 + (exact2 ? 1 : 0)) {                                                    \
+            case 3: sr::short_range_batched_kernel<RX_, 1, 2><<<grid, block, 0, stream>>>(a, g.first, g.sims); break; \
+            case 2: sr::short_range_batched_kernel<RX_, 1, 0><<<grid, block, 0, stream>>>(a, g.first, g.sims); break; \
+            case 5: sr::short_range_batched_kernel<RX_, 2, 2><<<grid, block, 0, stream>>>(a, g.first, g.sims); break; \
+            case 4: sr::short_range_batched_kernel<RX_, 2, 0><<<grid, block, 0, stream>>>(a, g.first, g.sims); break; \
+            case 7: sr::short_range_batched_kernel<RX_, 3, 2><<<grid, block, 0, stream>>>(a, g.first, g.sims); break; \
+            case 6: sr::short_range_batched_kernel<RX_, 3, 0><<<grid, block, 0, stream>>>(a, g.first, g.sims); break; \
+            case 9: sr::short_range_batched_kernel<RX_, 4, 2><<<grid, block, 0, stream>>>(a, g.first, g.sims); break; \
+            case 8: sr::short_range_batched_kernel<RX_, 4, 0><<<grid, block, 0, stream>>>(a, g.first, g.sims); break; \
+            case 11: sr::short_range_batched_kernel<RX_, 5, 2><<<grid, block, 0, stream>>>(a, g.first, g.sims); break; \
+            case 10: sr::short_range_batched_kernel<RX_, 5, 0><<<grid, block, 0, stream>>>(a, g.first, g.sims); break; \
+            case 13: sr::short_range_batched_kernel<RX_, 6, 2><<<grid, block, 0, stream>>>(a, g.first, g.sims); break; \
+            case 12: sr::short_range_batched_kernel<RX_, 6, 0><<<grid, block, 0, stream>>>(a, g.first, g.sims); break; \
             default: return cudaErrorInvalidValue;                                              \
         }                                                                                       \
         return cudaGetLastError();                                                              \

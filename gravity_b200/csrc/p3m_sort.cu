@@ -67,10 +67,9 @@ constexpr int kScanThreads = 1024;
 constexpr int kScanItems = 8;
 constexpr int kScanBlock = kScanThreads * kScanItems;
 
-__global__ void __launch_bounds__(kScanThreads) scan_local_kernel(uint32_t* data, int n,
-                                                                  uint32_t* sums) {
+__device__ __forceinline__ void scan_local_body(int block, uint32_t* data, int n, uint32_t* sums) {
     __shared__ uint32_t warp_tot[33];
-    const int base = blockIdx.x * kScanBlock + threadIdx.x * kScanItems;
+    const int base = block * kScanBlock + threadIdx.x * kScanItems;
     uint32_t v[kScanItems];
     uint32_t s = 0;
 #pragma unroll
@@ -85,7 +84,12 @@ __global__ void __launch_bounds__(kScanThreads) scan_local_kernel(uint32_t* data
         if (base + i < n) data[base + i] = pre;
         pre += v[i];
     }
-    if (threadIdx.x == 0 && sums) sums[blockIdx.x] = total;
+    if (threadIdx.x == 0 && sums) sums[block] = total;
+}
+
+__global__ void __launch_bounds__(kScanThreads) scan_local_kernel(uint32_t* data, int n,
+                                                                  uint32_t* sums) {
+    scan_local_body(blockIdx.x, data, n, sums);
 }
 
 __global__ void __launch_bounds__(kScanThreads) scan_add_kernel(uint32_t* data, int n,
@@ -103,15 +107,13 @@ constexpr int kSortWarps = kSortThreads / 32;
 // Per-tile digit histogram, written digit-major (hist[d * tiles + tile]) so
 // that one exclusive scan of the whole array yields every tile's output base
 // for every digit.
-__global__ void __launch_bounds__(kSortThreads) radix_hist_kernel(const uint32_t* __restrict__ keys,
-                                                                  int n, int shift, int bits,
-                                                                  int tiles, uint32_t* hist) {
+__device__ __forceinline__ void radix_hist_body(int tile, const uint32_t* __restrict__ keys, int n,
+                                                int shift, int bits, int tiles, uint32_t* hist) {
     __shared__ uint32_t h[kSortMaxRadix];
     const int radix = 1 << bits;
     const uint32_t mask = (uint32_t)radix - 1u;
     for (int i = threadIdx.x; i < radix; i += blockDim.x) h[i] = 0;
     __syncthreads();
-    const int tile = blockIdx.x;
     const int base = tile * kSortTile;
     const int lane = threadIdx.x & 31;
     // Vectorised: each thread reads kSortItems/4 uint4 (the tile base is a
@@ -141,12 +143,18 @@ __global__ void __launch_bounds__(kSortThreads) radix_hist_kernel(const uint32_t
     for (int d = threadIdx.x; d < radix; d += blockDim.x) hist[(size_t)d * tiles + tile] = h[d];
 }
 
+__global__ void __launch_bounds__(kSortThreads) radix_hist_kernel(const uint32_t* __restrict__ keys,
+                                                                  int n, int shift, int bits,
+                                                                  int tiles, uint32_t* hist) {
+    radix_hist_body(blockIdx.x, keys, n, shift, bits, tiles, hist);
+}
+
 // Stable scatter of one tile. Keys of warp w are the contiguous sub-tile
 // [w*32*items, (w+1)*32*items), visited item-major so that (item, lane)
 // increases with the input position. Each key's rank among equal digits comes
 // from __match_any_sync + popc of lower lanes, plus a per-warp running count.
-__global__ void __launch_bounds__(kSortThreads) radix_scatter_kernel(
-    const uint32_t* __restrict__ keys_in, const uint32_t* __restrict__ vals_in,
+__device__ __forceinline__ void radix_scatter_body(
+    int tile, const uint32_t* __restrict__ keys_in, const uint32_t* __restrict__ vals_in,
     uint32_t* __restrict__ keys_out, uint32_t* __restrict__ vals_out, int n, int shift, int bits,
     int tiles, const uint32_t* __restrict__ hist_scanned) {
     __shared__ uint32_t warp_hist[kSortWarps][kSortMaxRadix];
@@ -159,7 +167,6 @@ __global__ void __launch_bounds__(kSortThreads) radix_scatter_kernel(
     const int radix = 1 << bits;
     const uint32_t mask = (uint32_t)radix - 1u;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int tile = blockIdx.x;
     const int tile_base = tile * kSortTile;
     const int sub_base = tile_base + warp * 32 * kSortItems;
 
@@ -226,6 +233,14 @@ __global__ void __launch_bounds__(kSortThreads) radix_scatter_kernel(
     }
 }
 
+__global__ void __launch_bounds__(kSortThreads) radix_scatter_kernel(
+    const uint32_t* __restrict__ keys_in, const uint32_t* __restrict__ vals_in,
+    uint32_t* __restrict__ keys_out, uint32_t* __restrict__ vals_out, int n, int shift, int bits,
+    int tiles, const uint32_t* __restrict__ hist_scanned) {
+    radix_scatter_body(blockIdx.x, keys_in, vals_in, keys_out, vals_out, n, shift, bits, tiles,
+                       hist_scanned);
+}
+
 // ----------------------------------------------------------- key kernels
 // build_grid.comp:71-72: home = ivec2(floor(p * vec2(W, H))), then wrapCell.
 __device__ __forceinline__ uint32_t home_cell(float x, float y, int W, int H) {
@@ -265,9 +280,10 @@ __device__ __forceinline__ uint32_t tile_coord(float p, int size) {
     return (uint32_t)min(max(t, 0), size - 1);
 }
 
-__global__ void morton_keys_kernel(const float4* __restrict__ bodies, int n, int wbits, int hbits,
-                                   uint32_t* keys, uint32_t* vals) {
-    const int id = blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void morton_keys_body(int block, const float4* __restrict__ bodies, int n,
+                                                 int wbits, int hbits, uint32_t* keys,
+                                                 uint32_t* vals) {
+    const int id = block * blockDim.x + threadIdx.x;
     if (id >= n) return;
     const float4 b = bodies[id];
     const uint32_t tx = tile_coord(b.x, 1 << wbits), ty = tile_coord(b.y, 1 << hbits);
@@ -278,19 +294,34 @@ __global__ void morton_keys_kernel(const float4* __restrict__ bodies, int n, int
     vals[id] = (uint32_t)id;
 }
 
+__global__ void morton_keys_kernel(const float4* __restrict__ bodies, int n, int wbits, int hbits,
+                                   uint32_t* keys, uint32_t* vals) {
+    morton_keys_body(blockIdx.x, bodies, n, wbits, hbits, keys, vals);
+}
+
 // spatial_sort_scatter.comp:14-28 and spatial_sort_materials.comp:9-13: a
 // bit-for-bit permutation; destinations[src] = new ID.
-__global__ void permute_kernel(const uint32_t* __restrict__ order, int n,
-                               const float4* __restrict__ bodies, const float2* __restrict__ accel,
-                               const float4* __restrict__ materials, float4* bodies_out,
-                               float2* accel_out, float4* materials_out, uint32_t* destinations) {
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void permute_body(int block, const uint32_t* __restrict__ order, int n,
+                                             const float4* __restrict__ bodies,
+                                             const float2* __restrict__ accel,
+                                             const float4* __restrict__ materials,
+                                             float4* bodies_out, float2* accel_out,
+                                             float4* materials_out, uint32_t* destinations) {
+    const int t = block * blockDim.x + threadIdx.x;
     if (t >= n) return;
     const uint32_t src = order[t];
     bodies_out[t] = bodies[src];
     accel_out[t] = accel[src];
     materials_out[t] = materials[src];
     destinations[src] = (uint32_t)t;
+}
+
+__global__ void permute_kernel(const uint32_t* __restrict__ order, int n,
+                               const float4* __restrict__ bodies, const float2* __restrict__ accel,
+                               const float4* __restrict__ materials, float4* bodies_out,
+                               float2* accel_out, float4* materials_out, uint32_t* destinations) {
+    permute_body(blockIdx.x, order, n, bodies, accel, materials, bodies_out, accel_out,
+                 materials_out, destinations);
 }
 
 // Cell lists from the sorted keys. Run starts write cell_start; counts and
@@ -312,12 +343,14 @@ __device__ __forceinline__ void fill_ranges(int* cell_start, uint32_t f0, uint32
     }
 }
 
-__global__ void cell_build_kernel(const uint32_t* __restrict__ keys, const uint32_t* __restrict__ ids,
-                                  int n, const float4* __restrict__ bodies,
-                                  const float4* __restrict__ materials, int* cell_start,
-                                  int* cell_count, uint32_t* cell_mass, float4* entries,
-                                  int fill_cells) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void cell_build_body(int block, const uint32_t* __restrict__ keys,
+                                                const uint32_t* __restrict__ ids, int n,
+                                                const float4* __restrict__ bodies,
+                                                const float4* __restrict__ materials,
+                                                int* cell_start, int* cell_count,
+                                                uint32_t* cell_mass, float4* entries,
+                                                int fill_cells) {
+    const int i = block * blockDim.x + threadIdx.x;
     const int lane = threadIdx.x & 31;
     const bool valid = i < n;
     const uint32_t c = valid ? keys[i] : 0xffffffffu;
@@ -362,6 +395,74 @@ __global__ void cell_build_kernel(const uint32_t* __restrict__ keys, const uint3
         fill_ranges(cell_start, head ? g0 : 0u, head ? c : 0u, i);
         const bool last = valid && i == n - 1;
         fill_ranges(cell_start, last ? c + 1u : 0u, last ? (uint32_t)fill_cells + 1u : 0u, n);
+    }
+}
+
+__global__ void cell_build_kernel(const uint32_t* __restrict__ keys, const uint32_t* __restrict__ ids,
+                                  int n, const float4* __restrict__ bodies,
+                                  const float4* __restrict__ materials, int* cell_start,
+                                  int* cell_count, uint32_t* cell_mass, float4* entries,
+                                  int fill_cells) {
+    cell_build_body(blockIdx.x, keys, ids, n, bodies, materials, cell_start, cell_count, cell_mass,
+                    entries, fill_cells);
+}
+
+// ------------------------------------------------------- batched launches
+__global__ void __launch_bounds__(kSortThreads) radix_hist_batched_kernel(
+    const RadixArgs* __restrict__ args, const int* __restrict__ first, int sims) {
+    const int2 sb = batch_block(first, sims);
+    const RadixArgs a = args[sb.x];
+    radix_hist_body(sb.y, a.keys_in, a.n, a.shift, a.bits, a.tiles, a.hist);
+}
+
+__global__ void __launch_bounds__(kSortThreads) radix_scatter_batched_kernel(
+    const RadixArgs* __restrict__ args, const int* __restrict__ first, int sims) {
+    const int2 sb = batch_block(first, sims);
+    const RadixArgs a = args[sb.x];
+    radix_scatter_body(sb.y, a.keys_in, a.vals_in, a.keys_out, a.vals_out, a.n, a.shift, a.bits,
+                       a.tiles, a.hist);
+}
+
+__global__ void __launch_bounds__(kScanThreads) scan_batched_kernel(
+    const ScanArgs* __restrict__ args, const int* __restrict__ first, int sims) {
+    const int2 sb = batch_block(first, sims);
+    const ScanArgs a = args[sb.x];
+    scan_local_body(0, a.data, a.n, nullptr);
+}
+
+__global__ void morton_keys_batched_kernel(const MortonArgs* __restrict__ args,
+                                           const int* __restrict__ first, int sims) {
+    const int2 sb = batch_block(first, sims);
+    const MortonArgs a = args[sb.x];
+    morton_keys_body(sb.y, a.bodies, a.n, a.wbits, a.hbits, a.keys, a.vals);
+}
+
+__global__ void permute_batched_kernel(const PermuteArgs* __restrict__ args,
+                                       const int* __restrict__ first, int sims) {
+    const int2 sb = batch_block(first, sims);
+    const PermuteArgs a = args[sb.x];
+    permute_body(sb.y, a.order, a.n, a.bodies, a.accel, a.materials, a.bodies_out, a.accel_out,
+                 a.materials_out, a.destinations);
+}
+
+__global__ void cell_build_batched_kernel(const CellBuildArgs* __restrict__ args,
+                                          const int* __restrict__ first, int sims) {
+    const int2 sb = batch_block(first, sims);
+    const CellBuildArgs a = args[sb.x];
+    cell_build_body(sb.y, a.keys, a.ids, a.n, a.bodies, a.materials, a.cell_start, a.cell_count,
+                    a.cell_mass, a.entries, 0);
+}
+
+// Zeroes `words` 32-bit words per simulation; local block b takes words
+// [b * 1024 * 4, ...) as uint4 where aligned.
+__global__ void zero_batched_kernel(const ZeroArgs* __restrict__ args,
+                                    const int* __restrict__ first, int sims) {
+    const int2 sb = batch_block(first, sims);
+    const ZeroArgs a = args[sb.x];
+    const long long base = (long long)sb.y * (kBatchThreads * 16);
+    for (int i = threadIdx.x; i < kBatchThreads * 16; i += blockDim.x) {
+        const long long w = base + i;
+        if (w < a.words) a.data[w] = 0u;
     }
 }
 
@@ -452,6 +553,25 @@ cudaError_t launch_permute(const uint32_t* order, int n, const float4* bodies, c
     count_launches(1);
     return cudaGetLastError();
 }
+
+int radix_tiles(int n) { return blocks_for(n, kSortTile); }
+int radix_scan_limit() { return kScanBlock; }
+
+#define P3M_BATCHED(name, Args, kernel, threads)                                \
+    cudaError_t name(const Args* a, BatchGrid g, cudaStream_t s) {            \
+        if (g.blocks <= 0) return cudaSuccess;                                 \
+        kernel<<<g.blocks, threads, 0, s>>>(a, g.first, g.sims);               \
+        count_launches(1);                                                     \
+        return cudaGetLastError();                                             \
+    }
+P3M_BATCHED(batched_morton_keys, MortonArgs, morton_keys_batched_kernel, kBatchThreads)
+P3M_BATCHED(batched_radix_hist, RadixArgs, radix_hist_batched_kernel, kSortThreads)
+P3M_BATCHED(batched_scan, ScanArgs, scan_batched_kernel, kScanThreads)
+P3M_BATCHED(batched_radix_scatter, RadixArgs, radix_scatter_batched_kernel, kSortThreads)
+P3M_BATCHED(batched_permute, PermuteArgs, permute_batched_kernel, kBatchThreads)
+P3M_BATCHED(batched_cell_build, CellBuildArgs, cell_build_batched_kernel, kBatchThreads)
+P3M_BATCHED(batched_zero, ZeroArgs, zero_batched_kernel, kBatchThreads)
+#undef P3M_BATCHED
 
 cudaError_t launch_cell_build(const uint32_t* keys, const uint32_t* ids, int n, const float4* bodies,
                               const float4* materials, int* cell_start, int* cell_count,

@@ -271,6 +271,12 @@ int p3m_batch_step(p3m_batch* batch, int32_t steps);
  * 64 rows of (grid_width, grid_height, fft_lines, short_range_threads) to
  * `chosen` when it is not NULL. Results do not depend on the shapes. */
 int p3m_batch_autotune(p3m_batch* batch, int32_t trial_steps, int32_t* chosen);
+/* Fused form (the default): every stage of a batch step is one launch over
+ * all simulations, captured once per plan. Off: every simulation enqueues
+ * its own step (one graph over the simulations' streams). Both give the same
+ * bits. The fused form needs every simulation at most 131,072 bodies; a
+ * batch with a larger one runs the other form. */
+int p3m_batch_set_fused(p3m_batch* batch, int32_t enabled);
 int p3m_batch_synchronize(p3m_batch* batch);
 int p3m_batch_get_stream(p3m_batch* batch, void** stream);
 

@@ -1,9 +1,11 @@
 """The batched form (p3m_batch_*) against simulations stepped one by one.
 
-A batch step is one CUDA graph over every simulation's stream; each
-simulation must come out bit for bit as the same simulation stepped alone in
-its own context, before and after the autotuner changes launch shapes, and
-across the reorder phases (a batch cycles through several captured graphs).
+In both forms of a batch step — fused (one launch per stage for every
+simulation) and per-simulation (one graph over the simulations' streams) —
+each simulation must come out bit for bit as the same simulation stepped
+alone in its own context, before and after the autotuner changes launch
+shapes, and across the reorder phases (a batch cycles through several
+captured plans).
 """
 
 from dataclasses import replace
@@ -41,10 +43,12 @@ def assert_same(got, want, what):
         np.testing.assert_array_equal(g, w, err_msg=f"{what}: {name}")
 
 
-def test_batch_matches_individual_steps(cuda_device):
+@pytest.mark.parametrize("fused", [True, False])
+def test_batch_matches_individual_steps(cuda_device, fused):
     scs = mixed_batch()
     field = (0.0, 3.5)
     with GravityBatch([sc.config for sc in scs]) as batch:
+        batch.set_fused(fused)
         for i, sc in enumerate(scs):
             batch.upload(i, sc.bodies, sc.materials)
         batch.simulation(5).set_field_acceleration(*field)
@@ -55,9 +59,11 @@ def test_batch_matches_individual_steps(cuda_device):
             assert_same(batch.download(i), want, f"simulation {i}")
 
 
-def test_batch_after_autotune_is_unchanged(cuda_device):
+@pytest.mark.parametrize("fused", [True, False])
+def test_batch_after_autotune_is_unchanged(cuda_device, fused):
     scs = mixed_batch()
     with GravityBatch([sc.config for sc in scs]) as batch:
+        batch.set_fused(fused)
         for i, sc in enumerate(scs):
             batch.upload(i, sc.bodies, sc.materials)
         batch.initialize_acceleration()
