@@ -1388,7 +1388,9 @@ int build_fused(p3m_batch* b, const std::vector<char>& sort, p3m_batch::Plan& pl
     }
     // 5. Short range (by stencil shape), then interpolation + kick.
     {
-        std::map<int, std::vector<int>> groups;  // rx * 64 + ry * 2 + exact2
+        // (The branch-free two-slot form of exact limit 2 also beats the list
+        // walk on sparse simulations: measured on the batch workload.)
+        std::map<int, std::vector<int>> groups;  // rx * 64 + ry * 2 + two-slot form
         for (int i : mut) {
             const p3m_ctx* c = b->sims[i];
             groups[c->rx * 64 + c->ry * 2 + (c->cfg.exact_neighbor_body_limit == 2 ? 1 : 0)].push_back(i);

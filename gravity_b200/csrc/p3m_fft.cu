@@ -575,14 +575,26 @@ cudaError_t launch_fft_adjoint(const float* cotangent, const float2* green, floa
     return cudaGetLastError();
 }
 
+// Batched launches run 256 threads per CTA for every simulation: enough
+// lines per CTA that one radix-8 pass gives every thread a butterfly
+// (lines * L / 8 >= 256), within the shared-memory caps of the single
+// launches and the simulation's line count.
 void fft_batch_shape(const GridShape& g, int* rows_per_cta, int* cols_per_cta, int* inv_per_cta,
                      size_t* rows_smem, size_t* cols_smem, size_t* inv_smem) {
-    int threads;
-    line_shape(g.MH / 2, g.MW, g.MW >= 4096 ? 1 : 4096 / g.MW, rows_per_cta, &threads, g.fft_lines);
+    auto fill = [](int lines_total, int L, int cap) {
+        int per = (256 * 8 + L - 1) / L;
+        if (per > cap) per = cap;
+        if (per > lines_total) per = lines_total;
+        return per < 1 ? 1 : per;
+    };
+    const int row_cap = g.MW >= 4096 ? 1 : 4096 / g.MW;
+    int col_cap = (128 * 1024) / (4 * g.MH * (int)sizeof(float2));
+    if (col_cap > 16) col_cap = 16;
+    *rows_per_cta = fill(g.MH / 2, g.MW, row_cap);
     *rows_smem = (size_t)2 * *rows_per_cta * g.MW * sizeof(float2);
-    column_shape(g.MW, g.MH, 4, cols_per_cta, &threads, g.fft_lines);
+    *cols_per_cta = fill(g.MW / 2 + 1, g.MH, col_cap);
     *cols_smem = (size_t)4 * *cols_per_cta * g.MH * sizeof(float2);
-    line_shape(g.MH, g.MW, g.MW >= 4096 ? 1 : 4096 / g.MW, inv_per_cta, &threads, g.fft_lines);
+    *inv_per_cta = fill(g.MH, g.MW, row_cap);
     *inv_smem = (size_t)2 * *inv_per_cta * g.MW * sizeof(float2);
 }
 
