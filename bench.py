@@ -451,6 +451,25 @@ def run_b200(args, ws, rank, local):
     for a in (hb, hm, out):
         a.free()
 
+    # ---- aim previews on the field of the last step (S/trajectory.comp):
+    # one preview, then a fan of 256, 1024 steps each (host wall clock,
+    # synchronous calls, vertices copied back).
+    previews = None
+    if rank == 0 and sc.config.mutual_gravity:
+        w_px, h_px = sc.config.viewport_width, sc.config.viewport_height
+        ang = np.linspace(0.0, 2.0 * np.pi, 256, endpoint=False)
+        fan_o = np.tile(np.array([0.3 * w_px, 0.5 * h_px], np.float32), (256, 1))
+        fan_v = (300.0 * np.stack([np.cos(ang), np.sin(ang)], axis=1)).astype(np.float32)
+        pipe.trajectories(n, fan_o[:1], fan_v[:1], steps=1024)
+        t0 = time.perf_counter()
+        pipe.trajectories(n, fan_o[:1], fan_v[:1], steps=1024)
+        one = time.perf_counter() - t0
+        t0 = time.perf_counter()
+        pipe.trajectories(n, fan_o, fan_v, steps=1024)
+        many = time.perf_counter() - t0
+        previews = {"steps": 1024, "single_ms": 1000.0 * one, "fan": 256,
+                    "fan_ms": 1000.0 * many, "preview_steps_per_s": 256 * 1024 / many}
+
     if rank == 0:
         peak, peak_kind = measured_peaks()
         P, M = mesh_sizes(sc)
@@ -498,6 +517,7 @@ def run_b200(args, ws, rank, local):
                     "d2h_bytes_per_step": 16 * n, "steps": e2e_steps},
             "gpu_launches": launches,
             "clocks": clk,
+            "previews": previews,
         }
         print(json.dumps(line), flush=True)
     pipe.close()

@@ -71,6 +71,20 @@ class P3MConfig(ctypes.Structure):
     ]
 
 
+class P3MTrajectoryConfig(ctypes.Structure):
+    """Mirror of ``p3m_trajectory_config`` (include/p3m.h)."""
+
+    _fields_ = [
+        ("struct_size", ctypes.c_int32),
+        ("steps", ctypes.c_int32),
+        ("maximum_time_step", ctypes.c_float),
+        ("target_segment_pixels", ctypes.c_float),
+        ("maximum_path_viewport_diagonals", ctypes.c_float),
+        ("minimum_dash_pixels", ctypes.c_float),
+        ("restitution_coefficient", ctypes.c_float),
+    ]
+
+
 # Every symbol include/p3m.h declares, with (restype, argtypes).
 _vp = ctypes.c_void_p
 _i32 = ctypes.c_int32
@@ -124,6 +138,9 @@ SIGNATURES = {
     "p3m_adjoint_forward": (ctypes.c_int, [_vp, _i32, _i32, _i32, _i32]),
     "p3m_adjoint_backward": (ctypes.c_int, [_vp, _vp, _vp, _vp, _vp]),
     "p3m_adjoint_release": (ctypes.c_int, [_vp]),
+    "p3m_trajectory_config_default": (ctypes.c_int, [ctypes.POINTER(P3MTrajectoryConfig)]),
+    "p3m_trajectories": (ctypes.c_int, [_vp, _i32, ctypes.POINTER(P3MTrajectoryConfig), _i32, _vp,
+                                        _vp, _vp]),
     "p3m_cell_lists_static": (ctypes.c_int, [_vp, _vp, _i32, _i32, _i32, _vp, _vp, _vp, _vp,
                                              _vp, _vp, _vp]),
 }

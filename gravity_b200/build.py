@@ -34,7 +34,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-O2",
           "--expt-relaxed-constexpr"]
 # Sources whose arithmetic must not contract a*b+c into one rounding.
-NO_FMA = {"p3m_sort.cu", "p3m_deposit.cu", "p3m_drift.cu"}
+NO_FMA = {"p3m_sort.cu", "p3m_deposit.cu", "p3m_drift.cu", "p3m_trajectory.cu"}
 
 
 def nvcc() -> str:

@@ -208,6 +208,8 @@ void free_all(p3m_ctx* ctx) {
     ctx->graphs.clear();
     for (cudaEvent_t e : ctx->free_events) cudaEventDestroy(e);
     ctx->free_events.clear();
+    if (ctx->traj_scratch) cudaFree(ctx->traj_scratch);
+    ctx->traj_scratch = nullptr;
     void* ptrs[] = {ctx->diag, ctx->bodies, ctx->bodies_alt, ctx->accel, ctx->accel_alt, ctx->materials,
                     ctx->materials_alt, ctx->destinations, ctx->status, ctx->keys, ctx->vals,
                     ctx->sort.keys_alt, ctx->sort.vals_alt, ctx->sort.hist, ctx->sort.block_sums,
@@ -303,6 +305,7 @@ int mesh_force(p3m_ctx* ctx, int n) {
         P3M_CUDA(ctx, p3m::launch_fft_inverse_rows(ctx->cols, ctx->grid, ctx->twiddles,
                                                    ctx->force, ctx->stream));
     }
+    ctx->built_n = n;
     return P3M_OK;
 }
 
@@ -431,6 +434,7 @@ int one_step(p3m_ctx* ctx, int n) {
         if (!graph_matches(g, ctx, n, do_sort)) continue;
         P3M_CUDA(ctx, cudaGraphLaunch(g.exec, ctx->stream));
         p3m::count_launches((int)g.kernels);
+        if (ctx->mutual) ctx->built_n = n;
         if (do_sort) swap_body_buffers(ctx);
         ctx->sorted_keys = g.sorted_keys;
         ctx->sorted_ids = g.sorted_ids;
@@ -1075,6 +1079,7 @@ int batch_one_step(p3m_batch* b) {
         if (e != cudaSuccess) return batch_fail(b, P3M_ERR_CUDA, cudaGetErrorString(e));
         p3m::count_launches((int)g.kernels);
         for (size_t i = 0; i < b->sims.size(); ++i) {
+            if (b->sims[i]->mutual) b->sims[i]->built_n = b->n[i];
             if (sort[i]) swap_body_buffers(b->sims[i]);
             b->sims[i]->sorted_keys = g.sorted[i].first;
             b->sims[i]->sorted_ids = g.sorted[i].second;
@@ -1478,6 +1483,7 @@ int batch_fused_step(p3m_batch* b, const std::vector<char>& sort, const std::vec
     for (size_t i = 0; i < b->sims.size(); ++i) {
         p3m_ctx* c = b->sims[i];
         if (plan->swap[i]) swap_body_buffers(c);
+        if (c->mutual) c->built_n = b->n[i];
         if (c->mutual && b->n[i] > 0) {
             c->sorted_keys = plan->sorted[i].first;
             c->sorted_ids = plan->sorted[i].second;
@@ -1987,6 +1993,79 @@ int p3m_adjoint_release(p3m_ctx* ctx) {
     if (!ctx) return P3M_ERR_INVALID_ARGUMENT;
     P3M_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
     adjoint_free(ctx);
+    return P3M_OK;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Aim previews (updateTrajectory, GravityPipeline.kt:514-600; trajectory.comp).
+
+extern "C" {
+
+int p3m_trajectory_config_default(p3m_trajectory_config* c) {
+    if (!c) return P3M_ERR_INVALID_ARGUMENT;
+    // TrajectoryConfig (GravityConfig.kt:739-745), CollisionConfig
+    // restitutionCoefficient (GravityConfig.kt:682).
+    c->struct_size = (int32_t)sizeof(p3m_trajectory_config);
+    c->steps = 1024;
+    c->maximum_time_step = 1.0f;
+    c->target_segment_pixels = 6.0f;
+    c->maximum_path_viewport_diagonals = 1.0f;
+    c->minimum_dash_pixels = 3.0f;
+    c->restitution_coefficient = 0.0f;
+    return P3M_OK;
+}
+
+int p3m_trajectories(p3m_ctx* ctx, int32_t n, const p3m_trajectory_config* tc, int32_t count,
+                     const float* origins_px2, const float* velocities_px2, float* vertices4) {
+    int st = check_n(ctx, n);
+    if (st != P3M_OK) return st;
+    if (!tc || tc->struct_size != (int32_t)sizeof(p3m_trajectory_config))
+        return fail(ctx, P3M_ERR_INVALID_ARGUMENT, "trajectory config missing or of another version");
+    // TrajectoryConfig's checks (GravityConfig.kt:747-756).
+    if (tc->steps < 1 || tc->steps > 65536)
+        return fail(ctx, P3M_ERR_INVALID_ARGUMENT, "steps must be in 1..65536");
+    auto positive = [](float v) { return v > 0.0f && std::isfinite(v); };
+    if (!positive(tc->maximum_time_step) || !positive(tc->target_segment_pixels) ||
+        !positive(tc->maximum_path_viewport_diagonals) || !positive(tc->minimum_dash_pixels))
+        return fail(ctx, P3M_ERR_INVALID_ARGUMENT, "trajectory lengths and times must be positive and finite");
+    if (!(tc->restitution_coefficient >= 0.0f && tc->restitution_coefficient <= 1.0f))
+        return fail(ctx, P3M_ERR_INVALID_ARGUMENT, "restitution must be in [0, 1]");
+    if (count < 0) return fail(ctx, P3M_ERR_INVALID_ARGUMENT, "count must be >= 0");
+    if (count == 0) return P3M_OK;
+    if (!origins_px2 || !velocities_px2 || !vertices4)
+        return fail(ctx, P3M_ERR_INVALID_ARGUMENT, "origins, velocities and vertices are required");
+    if (ctx->mutual && ctx->built_n != n)
+        return fail(ctx, P3M_ERR_STATE, "no force built for this body count: step or initialize first");
+    const size_t in_bytes = (size_t)count * sizeof(float2);
+    const size_t out_bytes = (size_t)count * (size_t)tc->steps * 6 * sizeof(float4);
+    const size_t need = 2 * in_bytes + out_bytes + 64;
+    if (ctx->traj_scratch_bytes < need) {
+        if (ctx->traj_scratch) cudaFree(ctx->traj_scratch);
+        ctx->traj_scratch = nullptr;
+        ctx->traj_scratch_bytes = 0;
+        cudaError_t e = cudaMalloc(&ctx->traj_scratch, need);
+        if (e != cudaSuccess) return fail_cuda(ctx, "trajectory buffers", e);
+        ctx->traj_scratch_bytes = need;
+    }
+    unsigned char* base = static_cast<unsigned char*>(ctx->traj_scratch);
+    float2* d_origins = reinterpret_cast<float2*>(base);
+    float2* d_vel = reinterpret_cast<float2*>(base + in_bytes);
+    float4* d_out = reinterpret_cast<float4*>(base + ((2 * in_bytes + 15) & ~(size_t)15));
+    P3M_CUDA(ctx, cudaMemcpyAsync(d_origins, origins_px2, in_bytes, cudaMemcpyDefault, ctx->stream));
+    P3M_CUDA(ctx, cudaMemcpyAsync(d_vel, velocities_px2, in_bytes, cudaMemcpyDefault, ctx->stream));
+    const p3m::KickParams k = kick_params(ctx, n, 0);
+    const float vw = (float)ctx->cfg.viewport_width, vh = (float)ctx->cfg.viewport_height;
+    const float max_path = tc->maximum_path_viewport_diagonals * std::sqrt(vw * vw + vh * vh);
+    P3M_CUDA(ctx, p3m::launch_trajectories(k, make_float2(vw, vh), ctx->cfg.time_step,
+                                           tc->maximum_time_step, tc->target_segment_pixels,
+                                           max_path, tc->minimum_dash_pixels,
+                                           tc->restitution_coefficient, tc->steps, count, d_origins,
+                                           d_vel, ctx->force, ctx->entries, ctx->cell_start,
+                                           ctx->cell_count, ctx->cell_mass, d_out, ctx->stream));
+    P3M_CUDA(ctx, cudaMemcpyAsync(vertices4, d_out, out_bytes, cudaMemcpyDefault, ctx->stream));
+    P3M_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
     return P3M_OK;
 }
 

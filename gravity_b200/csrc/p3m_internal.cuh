@@ -227,6 +227,15 @@ cudaError_t launch_conservation(const float4* bodies, const float4* materials, i
 // Process-wide count of kernels launched by this library (p3m_kernel_launches).
 void count_launches(int kernels);
 
+// Aim previews (trajectory.comp): one warp per preview, `count` previews.
+cudaError_t launch_trajectories(const KickParams& k, float2 viewport, float min_dt, float max_dt,
+                                float target_segment_px, float max_path_px, float min_dash_px,
+                                float restitution, int steps, int count, const float2* origins_px,
+                                const float2* velocities_px, const float2* force,
+                                const float4* entries, const int* cell_start,
+                                const int* cell_count, const uint32_t* cell_mass,
+                                float4* vertices, cudaStream_t stream);
+
 // ------------------------------------------------------- batched launches
 // One launch runs a stage for many simulations: CTA b runs local block
 // b - first[s] of simulation s, where first[] (sims + 1 entries, on the
@@ -404,6 +413,12 @@ struct p3m_ctx {
 
     // differentiated rollout (checkpoints, recompute slots, cotangents)
     struct p3m_adjoint_store* adjoint = nullptr;
+
+    // aim previews: the body count of the last force build (-1: none), and
+    // the staging buffers of p3m_trajectories
+    int built_n = -1;
+    void* traj_scratch = nullptr;
+    size_t traj_scratch_bytes = 0;
 
     // captured steps (CUDA graphs)
     bool use_graphs = true;

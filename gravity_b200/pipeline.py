@@ -244,6 +244,31 @@ class GravityPipeline:
         self._check(self._lib.p3m_get_stream(self._ctx, ctypes.byref(s)))
         return s.value or 0
 
+    def trajectories(self, n: int, origins_px, velocities_px, steps: int = 1024,
+                     maximum_time_step: float = 1.0, target_segment_pixels: float = 6.0,
+                     maximum_path_viewport_diagonals: float = 1.0,
+                     minimum_dash_pixels: float = 3.0, restitution: float = 0.0) -> np.ndarray:
+        """updateTrajectory (GravityPipeline.kt:514-600) for every row of
+        origins / velocities (px, px/s) on the field of the last force build:
+        (count, steps * 6, 4) float32 vertices (x, y, dash px, distance
+        fraction or -1)."""
+        o = np.ascontiguousarray(origins_px, np.float32).reshape(-1, 2)
+        v = np.ascontiguousarray(velocities_px, np.float32).reshape(-1, 2)
+        if o.shape != v.shape:
+            raise ValueError("origins and velocities must have the same shape")
+        cfg = _abi.P3MTrajectoryConfig()
+        self._check(self._lib.p3m_trajectory_config_default(ctypes.byref(cfg)))
+        cfg.steps = steps
+        cfg.maximum_time_step = maximum_time_step
+        cfg.target_segment_pixels = target_segment_pixels
+        cfg.maximum_path_viewport_diagonals = maximum_path_viewport_diagonals
+        cfg.minimum_dash_pixels = minimum_dash_pixels
+        cfg.restitution_coefficient = restitution
+        out = np.empty((o.shape[0], steps * 6, 4), np.float32)
+        self._check(self._lib.p3m_trajectories(self._ctx, n, ctypes.byref(cfg), o.shape[0],
+                                               _ptr(o), _ptr(v), _ptr(out)))
+        return out
+
     def nonfinite_count(self) -> int:
         c = ctypes.c_int64()
         self._check(self._lib.p3m_nonfinite_count(self._ctx, ctypes.byref(c)))

@@ -308,6 +308,32 @@ int p3m_adjoint_backward(p3m_ctx* ctx, const float* seed_bodies4, const float* s
 /* Frees the checkpoints and recompute storage. */
 int p3m_adjoint_release(p3m_ctx* ctx);
 
+/* ---- aim previews --------------------------------------------------------- */
+
+/* TrajectoryConfig (GravityConfig.kt:739-756) plus the collision
+ * restitution the preview bounces off walls with (GravityConfig.kt:682). */
+typedef struct p3m_trajectory_config {
+    int32_t struct_size;                    /* sizeof(p3m_trajectory_config) */
+    int32_t steps;                          /* 1..65536 (1024) */
+    float maximum_time_step;                /* s (1) */
+    float target_segment_pixels;            /* (6) */
+    float maximum_path_viewport_diagonals;  /* (1) */
+    float minimum_dash_pixels;              /* (3) */
+    float restitution_coefficient;          /* [0, 1] (0) */
+} p3m_trajectory_config;
+
+int p3m_trajectory_config_default(p3m_trajectory_config* config);
+
+/* updateTrajectory (GravityPipeline.kt:514-600, trajectory.comp) for `count`
+ * previews at once, on the field of the last force build for n bodies (a
+ * step or initializeAcceleration; P3M_ERR_STATE otherwise): origins and
+ * launch velocities in px and px/s (count x 2 floats each); vertices: count x
+ * steps x 6 (x, y, dash coordinate px, distance fraction or -1 when unused)
+ * floats x 4, the reference's trajectory buffer per preview. Pointers may be
+ * host or device memory. Synchronous. */
+int p3m_trajectories(p3m_ctx* ctx, int32_t n, const p3m_trajectory_config* config, int32_t count,
+                     const float* origins_px2, const float* velocities_px2, float* vertices4);
+
 /* ---- cell lists without allocation ------------------------------------- */
 
 /* No counterpart in the reference. For callers that cannot allocate device

@@ -87,6 +87,7 @@ def load() -> ctypes.CDLL:
             "oracle_kernel_spectra": (None, [vp, vp, vp]),
             "oracle_destinations": (None, [vp, vp, i]),
             "oracle_direct_sum_f64": (None, [vp, vp, i, vp, i, vp, f, i, vp]),
+            "oracle_trajectory": (None, [vp, i, vp, f, f, f, f, vp]),
             "oracle_adj_create": (vp, [vp, vp, i, ctypes.c_double, ctypes.c_double]),
             "oracle_adj_destroy": (None, [vp]),
             "oracle_adj_force": (None, [vp, vp, vp]),
@@ -293,6 +294,16 @@ class OracleSim:
         ky = np.empty((mh, mw), np.complex64)
         self._lib.oracle_kernel_spectra(self._s, _p(kx), _p(ky))
         return kx, ky
+
+    def trajectory(self, n, origin_px, velocity_px, steps=1024, max_dt=1.0, segment_px=6.0,
+                   path_diagonals=1.0, min_dash_px=3.0, restitution=0.0):
+        """S/trajectory.comp for one preview: (steps * 6, 4) vertices."""
+        prm = np.array([steps, max_dt, segment_px, path_diagonals, min_dash_px, restitution],
+                       np.float32)
+        out = np.empty((steps * 6, 4), np.float32)
+        self._lib.oracle_trajectory(self._s, n, _p(prm), float(origin_px[0]), float(origin_px[1]),
+                                    float(velocity_px[0]), float(velocity_px[1]), _p(out))
+        return out
 
     def destinations(self, n):
         out = np.empty(n, np.uint32)

@@ -725,6 +725,168 @@ void oracle_step(oracle_sim* s, int n, int steps) {
 }
 
 // ---------------------------------------------------------------------------
+// S/trajectory.comp (one preview, the shader's one thread) and the host
+// placement of K/GravityPipeline.kt:514-600, 773-779.
+
+static inline f2 traj_local(const KickParams& k, f2 src, f2 tgt, float m) {
+    return local_acceleration(k, src, tgt, m);  // S/trajectory.comp:78-95 == S/kick.comp:66-80
+}
+
+static f2 traj_acceleration(const oracle_sim* s, const KickParams& k, f2 p) {
+    if (k.mutual == 0) return {k.field_x, k.field_y};
+    f2 interp = interpolate_force(k, s->force_x.data(), s->force_y.data(), p);
+    f2 r = {interp.x + k.field_x, interp.y + k.field_y};
+    int hx = f2i(std::floor(p.x * (float)k.W)), hy = f2i(std::floor(p.y * (float)k.H));
+    for (int dy = -k.ry; dy <= k.ry; ++dy) {
+        for (int dx = -k.rx; dx <= k.rx; ++dx) {
+            int cx = hx + dx, cy = hy + dy;
+            if (k.bounded != 0 && (cx < 0 || cy < 0 || cx >= k.W || cy >= k.H)) continue;
+            int wx = wrap1(cx, k.W), wy = wrap1(cy, k.H);
+            int index = wx + wy * k.W;
+            int count = s->counts[index];
+            bool home = dx == 0 && dy == 0;
+            if (!home && count > k.exact) {
+                f2 center = {((float)wx + 0.5f) / (float)k.W, ((float)wy + 0.5f) / (float)k.H};
+                f2 a = traj_local(k, center, p, (float)s->cell_masses[index] / kCellMassUnits);
+                r.x += a.x; r.y += a.y;
+            } else {
+                int other = s->heads[index];
+                int visited = 0;
+                int limit = home ? k.home_limit : k.exact;
+                while (other >= 0 && visited < limit) {
+                    f2 sp = {s->bodies[(size_t)other * 4], s->bodies[(size_t)other * 4 + 1]};
+                    f2 a = traj_local(k, sp, p, s->materials[(size_t)other * 4]);
+                    r.x += a.x; r.y += a.y;
+                    other = s->next[other];
+                    visited++;
+                }
+            }
+        }
+    }
+    return r;
+}
+
+static void traj_emit(float* out, int step, f2 start, f2 delta, float sd, float dist, float sdc,
+                      float dc) {
+    float* v = out + (size_t)step * 6 * 4;
+    for (int i = 0; i < 6; ++i) { v[4 * i] = 0; v[4 * i + 1] = 0; v[4 * i + 2] = 0; v[4 * i + 3] = -1; }
+    f2 end = {start.x + delta.x, start.y + delta.y};
+    float cuts[4];
+    int cut_count = 2;
+    cuts[0] = 0.0f; cuts[1] = 1.0f;
+    if (end.x < 0.0f) cuts[cut_count++] = -start.x / delta.x;
+    else if (end.x >= 1.0f) cuts[cut_count++] = (1.0f - start.x) / delta.x;
+    if (end.y < 0.0f) cuts[cut_count++] = -start.y / delta.y;
+    else if (end.y >= 1.0f) cuts[cut_count++] = (1.0f - start.y) / delta.y;
+    for (int index = 1; index < cut_count; ++index) {
+        float value = std::min(std::max(cuts[index], 0.0f), 1.0f);
+        int ins = index;
+        while (ins > 0 && cuts[ins - 1] > value) { cuts[ins] = cuts[ins - 1]; ins--; }
+        cuts[ins] = value;
+    }
+    float uniq[4];
+    int uc = 0;
+    for (int index = 0; index < cut_count; ++index)
+        if (uc == 0 || std::fabs(cuts[index] - uniq[uc - 1]) > 1e-6f) uniq[uc++] = cuts[index];
+    for (int piece = 0; piece < uc - 1; ++piece) {
+        float f0 = uniq[piece], f1 = uniq[piece + 1];
+        float mid = 0.5f * (f0 + f1);
+        float tx = std::floor(start.x + delta.x * mid), ty = std::floor(start.y + delta.y * mid);
+        float* q = v + piece * 2 * 4;
+        q[0] = std::min(std::max(start.x + delta.x * f0 - tx, 0.0f), 1.0f);
+        q[1] = std::min(std::max(start.y + delta.y * f0 - ty, 0.0f), 1.0f);
+        q[2] = sdc + dc * f0;
+        q[3] = sd + dist * f0;
+        q[4] = std::min(std::max(start.x + delta.x * f1 - tx, 0.0f), 1.0f);
+        q[5] = std::min(std::max(start.y + delta.y * f1 - ty, 0.0f), 1.0f);
+        q[6] = sdc + dc * f1;
+        q[7] = sd + dist * f1;
+    }
+}
+
+// params: steps, max_dt, target_segment_px, path_diagonals, min_dash_px,
+// restitution. out: steps * 6 vec4.
+void oracle_trajectory(oracle_sim* s, int n, const float* params, float origin_x_px,
+                       float origin_y_px, float vx_px, float vy_px, float* out) {
+    normalize_to(s, n);
+    KickParams k;
+    k.W = s->W; k.H = s->H; k.MW = s->mesh_w(); k.MH = s->mesh_h();
+    k.bounded = s->bounded; k.rx = s->rx; k.ry = s->ry;
+    k.exact = s->cfg.exact_neighbor_body_limit;
+    k.home_limit = s->cfg.maximum_home_body_interactions;
+    k.initial = 0; k.mutual = s->mutual;
+    k.aspect = s->aspect; k.g = s->cfg.gravitational_constant;
+    k.sigma_cells = s->cfg.softening_cells; k.total = s->normalization_mass;
+    k.min_frac = s->cfg.minimum_distance_cell_fraction; k.dt = s->cfg.time_step;
+    k.field_x = s->field_x; k.field_y = s->field_y;
+    const int steps = (int)params[0];
+    const float max_dt = params[1], target = params[2], diagonals = params[3];
+    const float min_dash = params[4], restitution = params[5];
+    const float vw = (float)s->cfg.viewport_width, vh = (float)s->cfg.viewport_height;
+    const float max_path = diagonals * std::sqrt(vw * vw + vh * vh);
+    const float min_dt = s->cfg.time_step;
+    // placeX / placeY, then S/trajectory.comp:262-329.
+    float ox, oy;
+    if (s->bounded) {
+        ox = std::min(std::max(origin_x_px, 0.0f), vw * kMaximumUnit);
+        oy = std::min(std::max(origin_y_px, 0.0f), vh * kMaximumUnit);
+    } else {
+        ox = origin_x_px - std::floor(origin_x_px / vw) * vw;
+        oy = origin_y_px - std::floor(origin_y_px / vh) * vh;
+    }
+    f2 pos = {ox / vw, oy / vh}, vel = {vx_px / vw, vy_px / vh};
+    f2 acc = traj_acceleration(s, k, pos);
+    float path = 0.0f, dash = 0.0f;
+    bool finished = false;
+    for (int step = 0; step < steps; ++step) {
+        if (finished) {
+            float* v = out + (size_t)step * 24;
+            for (int i = 0; i < 6; ++i) { v[4 * i] = 0; v[4 * i + 1] = 0; v[4 * i + 2] = 0; v[4 * i + 3] = -1; }
+            continue;
+        }
+        float sp = std::sqrt((vel.x * vw) * (vel.x * vw) + (vel.y * vh) * (vel.y * vh));
+        float ap = std::sqrt((acc.x * vw) * (acc.x * vw) + (acc.y * vh) * (acc.y * vh));
+        float dt;
+        if (ap > 1e-5f) dt = (std::sqrt(sp * sp + 2.0f * ap * target) - sp) / ap;
+        else dt = target / std::max(sp, 1e-5f);
+        dt = std::min(std::max(dt, min_dt), max_dt);
+        f2 half = {vel.x + acc.x * (0.5f * dt), vel.y + acc.y * (0.5f * dt)};
+        f2 delta = {half.x * dt, half.y * dt};
+        if (s->bounded) {
+            float nx = pos.x + delta.x, ny = pos.y + delta.y;
+            float cx = std::min(std::max(nx, 0.0f), kMaximumUnit), cy = std::min(std::max(ny, 0.0f), kMaximumUnit);
+            if (nx != cx) half.x = -restitution * half.x;
+            if (ny != cy) half.y = -restitution * half.y;
+            delta = {cx - pos.x, cy - pos.y};
+        }
+        float step_px = std::sqrt((delta.x * vw) * (delta.x * vw) + (delta.y * vh) * (delta.y * vh));
+        float remaining = max_path - path;
+        if (step_px > remaining) {
+            delta.x *= remaining / step_px;
+            delta.y *= remaining / step_px;
+            step_px = remaining;
+            finished = true;
+        }
+        float mult = 1.0f + std::sqrt(half.x * half.x + half.y * half.y);
+        float dash_len = min_dash * mult;
+        float step_dash = step_px * min_dash / dash_len;
+        traj_emit(out, step, pos, delta, path, step_px, dash, step_dash);
+        path += step_px;
+        dash += step_dash;
+        if (s->bounded) pos = {pos.x + delta.x, pos.y + delta.y};
+        else pos = {fractf(pos.x + delta.x), fractf(pos.y + delta.y)};
+        if (path >= max_path - 1e-4f) { finished = true; continue; }
+        acc = traj_acceleration(s, k, pos);
+        vel = {half.x + acc.x * (0.5f * dt), half.y + acc.y * (0.5f * dt)};
+    }
+    float inv = 1.0f / std::max(path, 1e-6f);
+    for (int v = 0; v < steps * 6; ++v) {
+        float& w = out[(size_t)v * 4 + 3];
+        if (w >= 0.0f) w = std::min(std::max(w * inv, 0.0f), 1.0f);
+    }
+}
+
+// ---------------------------------------------------------------------------
 // Readback of intermediate buffers, in the library's layouts.
 
 int oracle_normalization(oracle_sim* s, float* total_mass, int* mass_scale) {
