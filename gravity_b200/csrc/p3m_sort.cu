@@ -115,31 +115,38 @@ __device__ __forceinline__ void radix_hist_body(int tile, const uint32_t* __rest
     for (int i = threadIdx.x; i < radix; i += blockDim.x) h[i] = 0;
     __syncthreads();
     const int base = tile * kSortTile;
-    const int lane = threadIdx.x & 31;
-    // Vectorised: each thread reads kSortItems/4 uint4 (the tile base is a
-    // multiple of 4096 keys, so every uint4 is 16-byte aligned).
+    // Each thread counts kSortItems consecutive keys (four uint4 loads; the
+    // tile base is a multiple of 4096 keys, so every uint4 is 16-byte
+    // aligned), adding a run of equal digits with one shared atomic: the
+    // keys are near-sorted (cells of Morton-ordered bodies, or an earlier
+    // pass's output), so runs are long.
+    const int first = base + threadIdx.x * kSortItems;
+    uint32_t run_digit = 0xffffffffu, run = 0;
 #pragma unroll
     for (int j = 0; j < kSortItems / 4; ++j) {
-        const int idx = base + (j * kSortThreads + threadIdx.x) * 4;
+        const int idx = first + j * 4;
         uint32_t k[4];
         if (idx + 3 < n) {
             uint4 q = __ldg(reinterpret_cast<const uint4*>(keys + idx));
             k[0] = q.x; k[1] = q.y; k[2] = q.z; k[3] = q.w;
         } else {
 #pragma unroll
-            for (int e = 0; e < 4; ++e) k[e] = idx + e < n ? keys[idx + e] : 0xffffffffu;
+            for (int e = 0; e < 4; ++e) k[e] = idx + e < n ? keys[idx + e] : 0u;
         }
 #pragma unroll
         for (int e = 0; e < 4; ++e) {
-            const bool valid = idx + e < n;
-            const uint32_t d = valid ? (k[e] >> shift) & mask : 0xffffffffu;
-            // Aggregate equal digits across the warp before the shared atomic.
-            const unsigned peers = __match_any_sync(kFull, d);
-            if (valid && lane == __ffs(peers) - 1) atomicAdd(&h[d], (uint32_t)__popc(peers));
+            if (idx + e >= n) continue;
+            const uint32_t d = (k[e] >> shift) & mask;
+            if (d != run_digit) {
+                if (run) atomicAdd(&h[run_digit], run);
+                run_digit = d;
+                run = 0;
+            }
+            ++run;
         }
     }
+    if (run) atomicAdd(&h[run_digit], run);
     __syncthreads();
-    (void)lane;
     for (int d = threadIdx.x; d < radix; d += blockDim.x) hist[(size_t)d * tiles + tile] = h[d];
 }
 
