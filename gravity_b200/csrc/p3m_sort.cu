@@ -115,8 +115,8 @@ __device__ __forceinline__ void radix_hist_body(int tile, const uint32_t* __rest
     for (int i = threadIdx.x; i < radix; i += blockDim.x) h[i] = 0;
     __syncthreads();
     const int base = tile * kSortTile;
-    // Each thread counts kSortItems consecutive keys (four uint4 loads; the
-    // tile base is a multiple of 4096 keys, so every uint4 is 16-byte
+    // Each thread counts kSortItems consecutive keys (uint4 loads; the tile
+    // base is a multiple of kSortTile keys, so every uint4 is 16-byte
     // aligned), adding a run of equal digits with one shared atomic: the
     // keys are near-sorted (cells of Morton-ordered bodies, or an earlier
     // pass's output), so runs are long.
