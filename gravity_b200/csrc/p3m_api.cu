@@ -203,6 +203,12 @@ void adjoint_free(p3m_ctx* ctx);
 
 void free_all(p3m_ctx* ctx) {
     adjoint_free(ctx);
+    if (ctx->side) cudaStreamSynchronize(ctx->side);
+    if (ctx->ev_fork) cudaEventDestroy(ctx->ev_fork);
+    if (ctx->ev_join) cudaEventDestroy(ctx->ev_join);
+    if (ctx->side) cudaStreamDestroy(ctx->side);
+    ctx->ev_fork = ctx->ev_join = nullptr;
+    ctx->side = nullptr;
     fold_stages(ctx);
     for (auto& g : ctx->graphs) cudaGraphExecDestroy(g.exec);
     ctx->graphs.clear();
@@ -332,9 +338,9 @@ p3m::KickParams kick_params(const p3m_ctx* ctx, int n, int initial) {
     return p;
 }
 
-int apply_kick(p3m_ctx* ctx, int n, int initial) {
+int apply_kick(p3m_ctx* ctx, int n, int initial, bool with_short_range = true) {
     const p3m::KickParams p = kick_params(ctx, n, initial);
-    if (ctx->mutual) {
+    if (ctx->mutual && with_short_range) {
         StageScope scope(ctx, P3M_STAGE_SHORT_RANGE);
         P3M_CUDA(ctx, p3m::launch_short_range(ctx->bodies, ctx->entries, ctx->cell_start,
                                               ctx->cell_count, ctx->cell_mass, ctx->a_short, p,
@@ -397,8 +403,23 @@ int enqueue_step(p3m_ctx* ctx, int n, bool do_sort) {
     if (ctx->mutual) {
         int st = lists_from_keys(ctx, n);
         if (st != P3M_OK) return st;
+        // The short range reads only the lists: outside the profiler it runs
+        // on the side stream beside the deposit and FFT.
+        const bool overlap = !ctx->profiling && n > 0;
+        if (overlap) {
+            P3M_CUDA(ctx, cudaEventRecord(ctx->ev_fork, ctx->stream));
+            P3M_CUDA(ctx, cudaStreamWaitEvent(ctx->side, ctx->ev_fork, 0));
+            P3M_CUDA(ctx, p3m::launch_short_range(ctx->bodies, ctx->entries, ctx->cell_start,
+                                                  ctx->cell_count, ctx->cell_mass, ctx->a_short,
+                                                  kick_params(ctx, n, 0), ctx->side));
+            P3M_CUDA(ctx, cudaEventRecord(ctx->ev_join, ctx->side));
+        }
         st = mesh_force(ctx, n);
         if (st != P3M_OK) return st;
+        if (overlap) {
+            P3M_CUDA(ctx, cudaStreamWaitEvent(ctx->stream, ctx->ev_join, 0));
+            return apply_kick(ctx, n, 0, false);
+        }
     }
     return apply_kick(ctx, n, 0);
 }
@@ -572,8 +593,14 @@ int p3m_create(const p3m_config* config, p3m_ctx** out) {
     ctx->cfg = *config;
     cudaError_t e = cudaGetDevice(&ctx->device);
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&ctx->side, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ctx->ev_fork, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ctx->ev_join, cudaEventDisableTiming);
     if (e != cudaSuccess) {
         fail_cuda(nullptr, "cudaStreamCreate", e);
+        if (ctx->ev_fork) cudaEventDestroy(ctx->ev_fork);
+        if (ctx->side) cudaStreamDestroy(ctx->side);
+        if (ctx->stream) cudaStreamDestroy(ctx->stream);
         delete ctx;
         return P3M_ERR_CUDA;
     }
@@ -974,6 +1001,8 @@ struct p3m_batch {
     std::vector<p3m_ctx*> sims;
     std::vector<int> n;
     cudaStream_t stream = nullptr;
+    cudaStream_t side = nullptr;  // fused form: the short range beside the mesh force
+    cudaEvent_t side_fork = nullptr, side_join = nullptr;
     cudaEvent_t fork = nullptr;
     std::vector<cudaEvent_t> join;
     struct Graph {
@@ -1324,7 +1353,41 @@ int build_fused(p3m_batch* b, const std::vector<char>& sort, p3m_batch::Plan& pl
         fb.stage(za, zb, p3m::batched_zero);
         fb.stage(ca, cb, p3m::batched_cell_build);
     }
-    // 4. Mesh force: clear, deposit, FFT with the Green's multiply, inverse.
+    // 4. Short range (by stencil shape) on the side stream: it reads only the
+    // cell lists, so it runs beside the deposit and FFT.
+    {
+        cudaStream_t side = b->side;
+        cudaEvent_t fork_ev = b->side_fork;
+        fb.raw([=](unsigned char*, cudaStream_t st) {
+            cudaError_t e = cudaEventRecord(fork_ev, st);
+            if (e == cudaSuccess) e = cudaStreamWaitEvent(side, fork_ev, 0);
+            return e;
+        });
+        // (The branch-free two-slot form of exact limit 2 also beats the list
+        // walk on sparse simulations: measured on the batch workload.)
+        std::map<int, std::vector<int>> groups;  // rx * 64 + ry * 2 + two-slot form
+        for (int i : mut) {
+            const p3m_ctx* c = b->sims[i];
+            groups[c->rx * 64 + c->ry * 2 + (c->cfg.exact_neighbor_body_limit == 2 ? 1 : 0)].push_back(i);
+        }
+        for (const auto& kv : groups) {
+            std::vector<p3m::ShortRangeArgs> sa;
+            std::vector<int> sb;
+            for (int i : kv.second) {
+                p3m_ctx* c = b->sims[i];
+                sa.push_back({role[i].bodies, c->entries, c->cell_start, c->cell_count, c->cell_mass,
+                              c->a_short, kick_params(c, b->n[i], 0)});
+                sb.push_back((b->n[i] + p3m::kBatchThreads - 1) / p3m::kBatchThreads);
+            }
+            const int rx = kv.first / 64, ry = (kv.first % 64) / 2, ex = kv.first % 2;
+            fb.stage(sa, sb, [rx, ry, ex, side](const p3m::ShortRangeArgs* a, p3m::BatchGrid g, cudaStream_t) {
+                return p3m::batched_short_range(a, g, rx, ry, ex, side);
+            });
+        }
+        cudaEvent_t join_ev = b->side_join;
+        fb.raw([=](unsigned char*, cudaStream_t) { return cudaEventRecord(join_ev, side); });
+    }
+    // 5. Mesh force: clear, deposit, FFT with the Green's multiply, inverse.
     {
         std::vector<p3m::ZeroArgs> za;
         std::vector<int> zb;
@@ -1391,29 +1454,10 @@ int build_fused(p3m_batch* b, const std::vector<char>& sort, p3m_batch::Plan& pl
             return p3m::batched_fft_inverse(a, g, ism, tw0, st);
         });
     }
-    // 5. Short range (by stencil shape), then interpolation + kick.
+    // 6. Interpolation + kick, after the short range has joined.
     {
-        // (The branch-free two-slot form of exact limit 2 also beats the list
-        // walk on sparse simulations: measured on the batch workload.)
-        std::map<int, std::vector<int>> groups;  // rx * 64 + ry * 2 + two-slot form
-        for (int i : mut) {
-            const p3m_ctx* c = b->sims[i];
-            groups[c->rx * 64 + c->ry * 2 + (c->cfg.exact_neighbor_body_limit == 2 ? 1 : 0)].push_back(i);
-        }
-        for (const auto& kv : groups) {
-            std::vector<p3m::ShortRangeArgs> sa;
-            std::vector<int> sb;
-            for (int i : kv.second) {
-                p3m_ctx* c = b->sims[i];
-                sa.push_back({role[i].bodies, c->entries, c->cell_start, c->cell_count, c->cell_mass,
-                              c->a_short, kick_params(c, b->n[i], 0)});
-                sb.push_back((b->n[i] + p3m::kBatchThreads - 1) / p3m::kBatchThreads);
-            }
-            const int rx = kv.first / 64, ry = (kv.first % 64) / 2, ex = kv.first % 2;
-            fb.stage(sa, sb, [rx, ry, ex](const p3m::ShortRangeArgs* a, p3m::BatchGrid g, cudaStream_t st) {
-                return p3m::batched_short_range(a, g, rx, ry, ex, st);
-            });
-        }
+        cudaEvent_t join_ev = b->side_join;
+        fb.raw([=](unsigned char*, cudaStream_t st) { return cudaStreamWaitEvent(st, join_ev, 0); });
         std::vector<p3m::KickArgs> ka;
         std::vector<int> kb;
         for (size_t i = 0; i < S; ++i) {
@@ -1528,11 +1572,17 @@ int p3m_batch_create(const p3m_config* configs, int32_t count, p3m_batch** out) 
         for (p3m_ctx* c : b->sims) p3m_destroy(c);
         for (cudaEvent_t e : b->join) cudaEventDestroy(e);
         if (b->fork) cudaEventDestroy(b->fork);
+        if (b->side_fork) cudaEventDestroy(b->side_fork);
+        if (b->side_join) cudaEventDestroy(b->side_join);
+        if (b->side) cudaStreamDestroy(b->side);
         if (b->stream) cudaStreamDestroy(b->stream);
         delete b;
         return st;
     };
     cudaError_t e = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&b->side, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->side_fork, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->side_join, cudaEventDisableTiming);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming);
     if (e != cudaSuccess) return undo(fail_cuda(nullptr, "batch stream/event", e));
     for (int32_t i = 0; i < count; ++i) {
@@ -1560,6 +1610,10 @@ int p3m_batch_destroy(p3m_batch* b) {
     for (p3m_ctx* c : b->sims) p3m_destroy(c);
     for (cudaEvent_t e : b->join) cudaEventDestroy(e);
     cudaEventDestroy(b->fork);
+    cudaEventDestroy(b->side_fork);
+    cudaEventDestroy(b->side_join);
+    cudaStreamSynchronize(b->side);
+    cudaStreamDestroy(b->side);
     cudaStreamDestroy(b->stream);
     delete b;
     return P3M_OK;

@@ -359,6 +359,10 @@ struct p3m_ctx {
     p3m_config cfg{};
     int device = 0;
     cudaStream_t stream = nullptr;
+    // The short range needs only the cell lists: in a step it runs on `side`
+    // beside the deposit and FFT (fork / join events).
+    cudaStream_t side = nullptr;
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     p3m::GridShape grid{};
     bool walls_supported = false;
     float aspect = 1.0f;
