@@ -219,8 +219,8 @@ void free_all(p3m_ctx* ctx) {
     void* ptrs[] = {ctx->diag, ctx->bodies, ctx->bodies_alt, ctx->accel, ctx->accel_alt, ctx->materials,
                     ctx->materials_alt, ctx->destinations, ctx->status, ctx->keys, ctx->vals,
                     ctx->sort.keys_alt, ctx->sort.vals_alt, ctx->sort.hist, ctx->sort.block_sums,
-                    ctx->cell_start, ctx->cell_count, ctx->cell_mass, ctx->entries, ctx->a_short,
-                    ctx->deposit_work, ctx->density,
+                    ctx->cell_start, ctx->cell_count, ctx->cell_mass, ctx->entries, ctx->cell_slots,
+                    ctx->a_short, ctx->deposit_work, ctx->density,
                     ctx->half, ctx->cols, ctx->force, ctx->green, ctx->twiddles};
     for (void* p : ptrs)
         if (p) cudaFree(p);
@@ -338,13 +338,25 @@ p3m::KickParams kick_params(const p3m_ctx* ctx, int n, int initial) {
     return p;
 }
 
+// The short range over the current cell lists; with exact limit 2 it reads
+// the per-cell slot table, built first on the same stream.
+int short_range(p3m_ctx* ctx, const p3m::KickParams& p, cudaStream_t stream) {
+    if (p.exact == 2 && p.n > 0)
+        P3M_CUDA(ctx, p3m::launch_cell_slots(ctx->cell_start, ctx->cell_count, ctx->cell_mass,
+                                             ctx->entries, ctx->grid.W, ctx->grid.H,
+                                             ctx->cell_slots, stream));
+    P3M_CUDA(ctx, p3m::launch_short_range(ctx->bodies, ctx->entries, ctx->cell_start,
+                                          ctx->cell_count, ctx->cell_mass, ctx->cell_slots,
+                                          ctx->a_short, p, stream));
+    return P3M_OK;
+}
+
 int apply_kick(p3m_ctx* ctx, int n, int initial, bool with_short_range = true) {
     const p3m::KickParams p = kick_params(ctx, n, initial);
     if (ctx->mutual && with_short_range) {
         StageScope scope(ctx, P3M_STAGE_SHORT_RANGE);
-        P3M_CUDA(ctx, p3m::launch_short_range(ctx->bodies, ctx->entries, ctx->cell_start,
-                                              ctx->cell_count, ctx->cell_mass, ctx->a_short, p,
-                                              ctx->stream));
+        const int st = short_range(ctx, p, ctx->stream);
+        if (st != P3M_OK) return st;
     }
     StageScope scope(ctx, P3M_STAGE_KICK);
     P3M_CUDA(ctx, p3m::launch_interp_kick(ctx->bodies, ctx->accel, ctx->force, ctx->a_short, p,
@@ -409,9 +421,8 @@ int enqueue_step(p3m_ctx* ctx, int n, bool do_sort) {
         if (overlap) {
             P3M_CUDA(ctx, cudaEventRecord(ctx->ev_fork, ctx->stream));
             P3M_CUDA(ctx, cudaStreamWaitEvent(ctx->side, ctx->ev_fork, 0));
-            P3M_CUDA(ctx, p3m::launch_short_range(ctx->bodies, ctx->entries, ctx->cell_start,
-                                                  ctx->cell_count, ctx->cell_mass, ctx->a_short,
-                                                  kick_params(ctx, n, 0), ctx->side));
+            st = short_range(ctx, kick_params(ctx, n, 0), ctx->side);
+            if (st != P3M_OK) return st;
             P3M_CUDA(ctx, cudaEventRecord(ctx->ev_join, ctx->side));
         }
         st = mesh_force(ctx, n);
@@ -644,6 +655,7 @@ int p3m_create(const p3m_config* config, p3m_ctx** out) {
     ALLOC(ctx->cell_start, P + 1);
     ALLOC(ctx->cell_count, P);
     ALLOC(ctx->cell_mass, P);
+    ALLOC(ctx->cell_slots, 2 * P);
     ALLOC(ctx->entries, cap);
     ALLOC(ctx->a_short, cap);
     ctx->deposit_work_capacity = p3m::deposit_work_entries((int)cap, mw_max, mh_max);
@@ -1363,6 +1375,22 @@ int build_fused(p3m_batch* b, const std::vector<char>& sort, p3m_batch::Plan& pl
             if (e == cudaSuccess) e = cudaStreamWaitEvent(side, fork_ev, 0);
             return e;
         });
+        // The two-slot form (exact limit 2) first builds each cell's slots.
+        {
+            std::vector<p3m::SlotsArgs> sl;
+            std::vector<int> slb;
+            for (int i : mut) {
+                p3m_ctx* c = b->sims[i];
+                if (c->cfg.exact_neighbor_body_limit != 2) continue;
+                sl.push_back({c->cell_start, c->cell_count, c->cell_mass, c->entries,
+                              c->cell_slots, c->grid.W, c->grid.H});
+                slb.push_back((int)((phys_cells(c) + p3m::kBatchThreads - 1) / p3m::kBatchThreads));
+            }
+            if (!sl.empty())
+                fb.stage(sl, slb, [side](const p3m::SlotsArgs* a, p3m::BatchGrid g, cudaStream_t) {
+                    return p3m::batched_cell_slots(a, g, side);
+                });
+        }
         // (The branch-free two-slot form of exact limit 2 also beats the list
         // walk on sparse simulations: measured on the batch workload.)
         std::map<int, std::vector<int>> groups;  // rx * 64 + ry * 2 + two-slot form
@@ -1376,7 +1404,7 @@ int build_fused(p3m_batch* b, const std::vector<char>& sort, p3m_batch::Plan& pl
             for (int i : kv.second) {
                 p3m_ctx* c = b->sims[i];
                 sa.push_back({role[i].bodies, c->entries, c->cell_start, c->cell_count, c->cell_mass,
-                              c->a_short, kick_params(c, b->n[i], 0)});
+                              c->cell_slots, c->a_short, kick_params(c, b->n[i], 0)});
                 sb.push_back((b->n[i] + p3m::kBatchThreads - 1) / p3m::kBatchThreads);
             }
             const int rx = kv.first / 64, ry = (kv.first % 64) / 2, ex = kv.first % 2;

@@ -168,8 +168,15 @@ struct KickParams {
 // Short-range correction over the cell stencil (kick.comp:122-151), one
 // thread per body; writes a_short[id]. Radii 1..6.
 cudaError_t launch_short_range(const float4* bodies, const float4* entries, const int* cell_start,
-                               const int* cell_count, const uint32_t* cell_mass, float2* a_short,
-                               KickParams p, cudaStream_t stream);
+                               const int* cell_count, const uint32_t* cell_mass,
+                               const float4* slots, float2* a_short, KickParams p,
+                               cudaStream_t stream);
+// The two source slots of every cell for the two-slot short range (exact
+// limit 2): the monopole at the cell centre (count > 2), the first one or
+// two list entries, or empty slots (mass 0) at the centre; 2 float4 per cell.
+cudaError_t launch_cell_slots(const int* cell_start, const int* cell_count,
+                              const uint32_t* cell_mass, const float4* entries, int W, int H,
+                              float4* slots, cudaStream_t stream);
 // CIC interpolation + field + a_short, then the half kick (kick.comp:82-103,
 // :153-154), one thread per body in ID order.
 cudaError_t launch_interp_kick(float4* bodies, float2* accel, const float2* force,
@@ -290,7 +297,11 @@ struct FftColumnsArgs {
 struct FftInverseArgs { const float4* cols; float2* force; int MW, MH, per_cta; };
 struct ShortRangeArgs {
     const float4* bodies; const float4* entries; const int* cell_start; const int* cell_count;
-    const uint32_t* cell_mass; float2* a_short; KickParams p;
+    const uint32_t* cell_mass; const float4* slots; float2* a_short; KickParams p;
+};
+struct SlotsArgs {
+    const int* cell_start; const int* cell_count; const uint32_t* cell_mass; const float4* entries;
+    float4* slots; int W, H;
 };
 struct KickArgs {
     float4* bodies; float2* accel; const float2* force; const float2* a_short; KickParams p;
@@ -323,6 +334,7 @@ cudaError_t batched_fft_inverse(const FftInverseArgs* a, BatchGrid g, size_t sme
 cudaError_t batched_short_range(const ShortRangeArgs* a, BatchGrid g, int rx, int ry, int exact2,
                                 cudaStream_t s);
 cudaError_t batched_interp_kick(const KickArgs* a, BatchGrid g, cudaStream_t s);
+cudaError_t batched_cell_slots(const SlotsArgs* a, BatchGrid g, cudaStream_t s);
 cudaError_t configure_batched();
 
 // Sets the message p3m_last_error(NULL) returns on this thread (entry points
@@ -399,6 +411,7 @@ struct p3m_ctx {
     int* cell_count = nullptr;
     uint32_t* cell_mass = nullptr;
     float4* entries = nullptr;
+    float4* cell_slots = nullptr;  // per cell: the two source slots of the short range
     float2* a_short = nullptr;  // short-range accelerations, by body ID
     int4* deposit_work = nullptr;  // pieces of heavy mesh tiles (+1 counter)
     size_t deposit_work_capacity = 0;

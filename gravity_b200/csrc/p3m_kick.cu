@@ -59,6 +59,48 @@ __global__ void __launch_bounds__(256) interp_kick_kernel(
     interp_kick_body(blockIdx.x, bodies, accel, force, a_short, p);
 }
 
+// One thread per cell: the two source slots the two-slot short range reads
+// for a non-home cell (kick.comp:128-146 with exact limit 2). A cell of more
+// than two bodies is its monopole at the cell centre; one of up to two bodies
+// gives its entries; missing slots are massless at the centre, so they add
+// nothing. The short range then reads 32 bytes per cell instead of the
+// count -> start -> entries chain; the values are those it read before.
+__device__ __forceinline__ void cell_slots_body(
+    int block, const int* __restrict__ cell_start, const int* __restrict__ cell_count,
+    const uint32_t* __restrict__ cell_mass, const float4* __restrict__ entries, int W, int H,
+    float4* __restrict__ slots) {
+    const int index = block * blockDim.x + threadIdx.x;
+    if (index >= W * H) return;
+    const int row = index / W, col = index - row * W;
+    const float inv_w = 1.0f / (float)W, inv_h = 1.0f / (float)H;
+    float4 s0 = make_float4(((float)col + 0.5f) * inv_w, ((float)row + 0.5f) * inv_h, 0.0f, 0.0f);
+    float4 s1 = s0;
+    const int count = cell_count[index];
+    if (count > 2) {
+        s0.z = (float)cell_mass[index] * (1.0f / kCellMassUnits);
+    } else if (count > 0) {
+        const int start = cell_start[index];
+        s0 = entries[start];
+        if (count == 2) s1 = entries[start + 1];
+    }
+    slots[2 * index] = s0;
+    slots[2 * index + 1] = s1;
+}
+
+__global__ void __launch_bounds__(256) cell_slots_kernel(
+    const int* __restrict__ cell_start, const int* __restrict__ cell_count,
+    const uint32_t* __restrict__ cell_mass, const float4* __restrict__ entries, int W, int H,
+    float4* __restrict__ slots) {
+    cell_slots_body(blockIdx.x, cell_start, cell_count, cell_mass, entries, W, H, slots);
+}
+
+__global__ void __launch_bounds__(256) cell_slots_batched_kernel(
+    const SlotsArgs* __restrict__ args, const int* __restrict__ first, int sims) {
+    const int2 sb = batch_block(first, sims);
+    const SlotsArgs a = args[sb.x];
+    cell_slots_body(sb.y, a.cell_start, a.cell_count, a.cell_mass, a.entries, a.W, a.H, a.slots);
+}
+
 __global__ void __launch_bounds__(256) interp_kick_batched_kernel(
     const KickArgs* __restrict__ args, const int* __restrict__ first, int sims) {
     const int2 sb = batch_block(first, sims);
@@ -71,6 +113,24 @@ __global__ void __launch_bounds__(256) interp_kick_batched_kernel(
 cudaError_t batched_interp_kick(const KickArgs* a, BatchGrid g, cudaStream_t s) {
     if (g.blocks <= 0) return cudaSuccess;
     interp_kick_batched_kernel<<<g.blocks, kBatchThreads, 0, s>>>(a, g.first, g.sims);
+    count_launches(1);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_cell_slots(const int* cell_start, const int* cell_count,
+                              const uint32_t* cell_mass, const float4* entries, int W, int H,
+                              float4* slots, cudaStream_t stream) {
+    const int cells = W * H;
+    if (cells <= 0) return cudaSuccess;
+    cell_slots_kernel<<<(cells + 255) / 256, 256, 0, stream>>>(cell_start, cell_count, cell_mass,
+                                                                entries, W, H, slots);
+    count_launches(1);
+    return cudaGetLastError();
+}
+
+cudaError_t batched_cell_slots(const SlotsArgs* a, BatchGrid g, cudaStream_t s) {
+    if (g.blocks <= 0) return cudaSuccess;
+    cell_slots_batched_kernel<<<g.blocks, kBatchThreads, 0, s>>>(a, g.first, g.sims);
     count_launches(1);
     return cudaGetLastError();
 }
@@ -93,17 +153,18 @@ cudaError_t batched_short_range(const ShortRangeArgs* a, BatchGrid g, int rx, in
 }
 
 cudaError_t launch_short_range(const float4* bodies, const float4* entries, const int* cell_start,
-                               const int* cell_count, const uint32_t* cell_mass, float2* a_short,
-                               KickParams p, cudaStream_t stream) {
+                               const int* cell_count, const uint32_t* cell_mass,
+                               const float4* slots, float2* a_short, KickParams p,
+                               cudaStream_t stream) {
     if (p.n <= 0 || p.mutual == 0) return cudaSuccess;
     cudaError_t e;
     switch (p.rx) {
-        case 1: e = launch_short_range_rx<1>(bodies, entries, cell_start, cell_count, cell_mass, a_short, p, stream); break;
-        case 2: e = launch_short_range_rx<2>(bodies, entries, cell_start, cell_count, cell_mass, a_short, p, stream); break;
-        case 3: e = launch_short_range_rx<3>(bodies, entries, cell_start, cell_count, cell_mass, a_short, p, stream); break;
-        case 4: e = launch_short_range_rx<4>(bodies, entries, cell_start, cell_count, cell_mass, a_short, p, stream); break;
-        case 5: e = launch_short_range_rx<5>(bodies, entries, cell_start, cell_count, cell_mass, a_short, p, stream); break;
-        case 6: e = launch_short_range_rx<6>(bodies, entries, cell_start, cell_count, cell_mass, a_short, p, stream); break;
+        case 1: e = launch_short_range_rx<1>(bodies, entries, cell_start, cell_count, cell_mass, slots, a_short, p, stream); break;
+        case 2: e = launch_short_range_rx<2>(bodies, entries, cell_start, cell_count, cell_mass, slots, a_short, p, stream); break;
+        case 3: e = launch_short_range_rx<3>(bodies, entries, cell_start, cell_count, cell_mass, slots, a_short, p, stream); break;
+        case 4: e = launch_short_range_rx<4>(bodies, entries, cell_start, cell_count, cell_mass, slots, a_short, p, stream); break;
+        case 5: e = launch_short_range_rx<5>(bodies, entries, cell_start, cell_count, cell_mass, slots, a_short, p, stream); break;
+        case 6: e = launch_short_range_rx<6>(bodies, entries, cell_start, cell_count, cell_mass, slots, a_short, p, stream); break;
         default: return cudaErrorInvalidValue;
     }
     count_launches(1);

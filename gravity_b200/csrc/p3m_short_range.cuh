@@ -84,7 +84,8 @@ template <int RX, int RY, int EXACT>
 __device__ __forceinline__ void short_range_body(
     int block, const float4* __restrict__ bodies, const float4* __restrict__ entries,
     const int* __restrict__ cell_start, const int* __restrict__ cell_count,
-    const uint32_t* __restrict__ cell_mass, float2* __restrict__ a_short, const KickParams& p) {
+    const uint32_t* __restrict__ cell_mass, const float4* __restrict__ slots,
+    float2* __restrict__ a_short, const KickParams& p) {
     const int i = block * blockDim.x + threadIdx.x;
     if (i >= p.n) return;
     const float4 t = bodies[i];
@@ -119,23 +120,16 @@ __device__ __forceinline__ void short_range_body(
         for (int a = 0; a < 2 * RX + 1; ++a) {
             if (!ok_x[a]) continue;
             const int index = row + col[a];
-            const int count = __ldg(&cell_count[index]);
             const bool home = (a == RX) && (b == RY);
             if (EXACT == 2 && !home) {
-                const float cxr = ((float)col[a] + 0.5f) * inv_w;  // wrapped column centre
-                float4 s0 = make_float4(cxr, cyr, 0.0f, 0.0f);
-                float4 s1 = s0;
-                if (count > 2) {
-                    s0.z = (float)__ldg(&cell_mass[index]) * (1.0f / kCellMassUnits);
-                } else if (count > 0) {
-                    const int start = __ldg(&cell_start[index]);
-                    s0 = __ldg(&entries[start]);
-                    if (count == 2) s1 = __ldg(&entries[start + 1]);
-                }
+                // The cell's two slots, prepared once per step (cell_slots).
+                const float4 s0 = __ldg(&slots[2 * index]);
+                const float4 s1 = __ldg(&slots[2 * index + 1]);
                 pair_add(k, (s0.x + shift_x[a]) - t.x, (s0.y + shift_y) - t.y, s0.z, ax, ay);
                 pair_add(k, (s1.x + shift_x[a]) - t.x, (s1.y + shift_y) - t.y, s1.z, ax, ay);
                 continue;
             }
+            const int count = __ldg(&cell_count[index]);
             if (count == 0) continue;
             if (!home && count > p.exact) {
                 const float mass = (float)__ldg(&cell_mass[index]) * (1.0f / kCellMassUnits);
@@ -160,9 +154,10 @@ template <int RX, int RY, int EXACT>
 __global__ void __launch_bounds__(256) short_range_kernel(
     const float4* __restrict__ bodies, const float4* __restrict__ entries,
     const int* __restrict__ cell_start, const int* __restrict__ cell_count,
-    const uint32_t* __restrict__ cell_mass, float2* __restrict__ a_short, KickParams p) {
+    const uint32_t* __restrict__ cell_mass, const float4* __restrict__ slots,
+    float2* __restrict__ a_short, KickParams p) {
     short_range_body<RX, RY, EXACT>(blockIdx.x, bodies, entries, cell_start, cell_count, cell_mass,
-                                    a_short, p);
+                                    slots, a_short, p);
 }
 
 template <int RX, int RY, int EXACT>
@@ -171,7 +166,7 @@ __global__ void __launch_bounds__(256) short_range_batched_kernel(
     const int2 sb = batch_block(first, sims);
     const ShortRangeArgs a = args[sb.x];
     short_range_body<RX, RY, EXACT>(sb.y, a.bodies, a.entries, a.cell_start, a.cell_count,
-                                    a.cell_mass, a.a_short, a.p);
+                                    a.cell_mass, a.slots, a.a_short, a.p);
 }
 
 }  // namespace sr
@@ -181,13 +176,13 @@ __global__ void __launch_bounds__(256) short_range_batched_kernel(
 template <int RX>
 cudaError_t launch_short_range_rx(const float4* bodies, const float4* entries,
                                   const int* cell_start, const int* cell_count,
-                                  const uint32_t* cell_mass, float2* a_short, const KickParams& p,
-                                  cudaStream_t stream);
+                                  const uint32_t* cell_mass, const float4* slots, float2* a_short,
+                                  const KickParams& p, cudaStream_t stream);
 #define P3M_DECLARE_SHORT_RANGE_RX(RX_)                                                       \
     template <>                                                                                 \
     cudaError_t launch_short_range_rx<RX_>(const float4*, const float4*, const int*, const int*, \
-                                           const uint32_t*, float2*, const KickParams&,         \
-                                           cudaStream_t);                                       \
+                                           const uint32_t*, const float4*, float2*,             \
+                                           const KickParams&, cudaStream_t);                    \
     template <>                                                                                 \
     cudaError_t batched_short_range_rx<RX_>(const ShortRangeArgs*, BatchGrid, int, int,          \
                                             cudaStream_t);
@@ -206,23 +201,24 @@ P3M_DECLARE_SHORT_RANGE_RX(6)
     template <>                                                                                 \
     cudaError_t launch_short_range_rx<RX_>(const float4* bodies, const float4* entries,         \
                                            const int* cell_start, const int* cell_count,        \
-                                           const uint32_t* cell_mass, float2* a_short,          \
-                                           const KickParams& p, cudaStream_t stream) {          \
+                                           const uint32_t* cell_mass, const float4* slots,      \
+                                           float2* a_short, const KickParams& p,                \
+                                           cudaStream_t stream) {                               \
         const int threads_ = p.sr_threads > 0 ? p.sr_threads : 256;                               \
         const dim3 grid((p.n + threads_ - 1) / threads_), block(threads_);                      \
         switch (p.ry * 2 + (p.exact == 2 ? 1 : 0)) {                                            \
-            case 3: sr::short_range_kernel<RX_, 1, 2><<<grid, block, 0, stream>>>(bodies, entries, cell_start, cell_count, cell_mass, a_short, p); break; \
-            case 2: sr::short_range_kernel<RX_, 1, 0><<<grid, block, 0, stream>>>(bodies, entries, cell_start, cell_count, cell_mass, a_short, p); break; \
-            case 5: sr::short_range_kernel<RX_, 2, 2><<<grid, block, 0, stream>>>(bodies, entries, cell_start, cell_count, cell_mass, a_short, p); break; \
-            case 4: sr::short_range_kernel<RX_, 2, 0><<<grid, block, 0, stream>>>(bodies, entries, cell_start, cell_count, cell_mass, a_short, p); break; \
-            case 7: sr::short_range_kernel<RX_, 3, 2><<<grid, block, 0, stream>>>(bodies, entries, cell_start, cell_count, cell_mass, a_short, p); break; \
-            case 6: sr::short_range_kernel<RX_, 3, 0><<<grid, block, 0, stream>>>(bodies, entries, cell_start, cell_count, cell_mass, a_short, p); break; \
-            case 9: sr::short_range_kernel<RX_, 4, 2><<<grid, block, 0, stream>>>(bodies, entries, cell_start, cell_count, cell_mass, a_short, p); break; \
-            case 8: sr::short_range_kernel<RX_, 4, 0><<<grid, block, 0, stream>>>(bodies, entries, cell_start, cell_count, cell_mass, a_short, p); break; \
-            case 11: sr::short_range_kernel<RX_, 5, 2><<<grid, block, 0, stream>>>(bodies, entries, cell_start, cell_count, cell_mass, a_short, p); break; \
-            case 10: sr::short_range_kernel<RX_, 5, 0><<<grid, block, 0, stream>>>(bodies, entries, cell_start, cell_count, cell_mass, a_short, p); break; \
-            case 13: sr::short_range_kernel<RX_, 6, 2><<<grid, block, 0, stream>>>(bodies, entries, cell_start, cell_count, cell_mass, a_short, p); break; \
-            case 12: sr::short_range_kernel<RX_, 6, 0><<<grid, block, 0, stream>>>(bodies, entries, cell_start, cell_count, cell_mass, a_short, p); break; \
+            case 3: sr::short_range_kernel<RX_, 1, 2><<<grid, block, 0, stream>>>(bodies, entries, cell_start, cell_count, cell_mass, slots, a_short, p); break; \
+            case 2: sr::short_range_kernel<RX_, 1, 0><<<grid, block, 0, stream>>>(bodies, entries, cell_start, cell_count, cell_mass, slots, a_short, p); break; \
+            case 5: sr::short_range_kernel<RX_, 2, 2><<<grid, block, 0, stream>>>(bodies, entries, cell_start, cell_count, cell_mass, slots, a_short, p); break; \
+            case 4: sr::short_range_kernel<RX_, 2, 0><<<grid, block, 0, stream>>>(bodies, entries, cell_start, cell_count, cell_mass, slots, a_short, p); break; \
+            case 7: sr::short_range_kernel<RX_, 3, 2><<<grid, block, 0, stream>>>(bodies, entries, cell_start, cell_count, cell_mass, slots, a_short, p); break; \
+            case 6: sr::short_range_kernel<RX_, 3, 0><<<grid, block, 0, stream>>>(bodies, entries, cell_start, cell_count, cell_mass, slots, a_short, p); break; \
+            case 9: sr::short_range_kernel<RX_, 4, 2><<<grid, block, 0, stream>>>(bodies, entries, cell_start, cell_count, cell_mass, slots, a_short, p); break; \
+            case 8: sr::short_range_kernel<RX_, 4, 0><<<grid, block, 0, stream>>>(bodies, entries, cell_start, cell_count, cell_mass, slots, a_short, p); break; \
+            case 11: sr::short_range_kernel<RX_, 5, 2><<<grid, block, 0, stream>>>(bodies, entries, cell_start, cell_count, cell_mass, slots, a_short, p); break; \
+            case 10: sr::short_range_kernel<RX_, 5, 0><<<grid, block, 0, stream>>>(bodies, entries, cell_start, cell_count, cell_mass, slots, a_short, p); break; \
+            case 13: sr::short_range_kernel<RX_, 6, 2><<<grid, block, 0, stream>>>(bodies, entries, cell_start, cell_count, cell_mass, slots, a_short, p); break; \
+            case 12: sr::short_range_kernel<RX_, 6, 0><<<grid, block, 0, stream>>>(bodies, entries, cell_start, cell_count, cell_mass, slots, a_short, p); break; \
             default: return cudaErrorInvalidValue;                                              \
         }                                                                                       \
         return cudaGetLastError();                                                              \
