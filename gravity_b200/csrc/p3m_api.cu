@@ -344,7 +344,7 @@ int short_range(p3m_ctx* ctx, const p3m::KickParams& p, cudaStream_t stream) {
     if (p.exact == 2 && p.n > 0)
         P3M_CUDA(ctx, p3m::launch_cell_slots(ctx->cell_start, ctx->cell_count, ctx->cell_mass,
                                              ctx->entries, ctx->grid.W, ctx->grid.H,
-                                             ctx->cell_slots, stream));
+                                             p.gravity, p.total_mass, ctx->cell_slots, stream));
     P3M_CUDA(ctx, p3m::launch_short_range(ctx->bodies, ctx->entries, ctx->cell_start,
                                           ctx->cell_count, ctx->cell_mass, ctx->cell_slots,
                                           ctx->a_short, p, stream));
@@ -655,7 +655,7 @@ int p3m_create(const p3m_config* config, p3m_ctx** out) {
     ALLOC(ctx->cell_start, P + 1);
     ALLOC(ctx->cell_count, P);
     ALLOC(ctx->cell_mass, P);
-    ALLOC(ctx->cell_slots, 2 * P);
+    ALLOC(ctx->cell_slots, (3 * P + 1) / 2);  // float4 plane + float2 plane
     ALLOC(ctx->entries, cap);
     ALLOC(ctx->a_short, cap);
     ctx->deposit_work_capacity = p3m::deposit_work_entries((int)cap, mw_max, mh_max);
@@ -1382,8 +1382,9 @@ int build_fused(p3m_batch* b, const std::vector<char>& sort, p3m_batch::Plan& pl
             for (int i : mut) {
                 p3m_ctx* c = b->sims[i];
                 if (c->cfg.exact_neighbor_body_limit != 2) continue;
+                const p3m::KickParams kp = kick_params(c, b->n[i], 0);
                 sl.push_back({c->cell_start, c->cell_count, c->cell_mass, c->entries,
-                              c->cell_slots, c->grid.W, c->grid.H});
+                              c->cell_slots, c->grid.W, c->grid.H, kp.gravity, kp.total_mass});
                 slb.push_back((int)((phys_cells(c) + p3m::kBatchThreads - 1) / p3m::kBatchThreads));
             }
             if (!sl.empty())

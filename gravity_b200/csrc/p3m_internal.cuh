@@ -173,10 +173,12 @@ cudaError_t launch_short_range(const float4* bodies, const float4* entries, cons
                                cudaStream_t stream);
 // The two source slots of every cell for the two-slot short range (exact
 // limit 2): the monopole at the cell centre (count > 2), the first one or
-// two list entries, or empty slots (mass 0) at the centre; 2 float4 per cell.
+// two list entries, or empty slots (mass 0) at the centre. Two planes of W*H
+// cells: float4 (x0, y0, G m0 / M_tot, x1), then float2 (y1, G m1 / M_tot).
 cudaError_t launch_cell_slots(const int* cell_start, const int* cell_count,
                               const uint32_t* cell_mass, const float4* entries, int W, int H,
-                              float4* slots, cudaStream_t stream);
+                              float gravity, float total_mass, float4* slots,
+                              cudaStream_t stream);
 // CIC interpolation + field + a_short, then the half kick (kick.comp:82-103,
 // :153-154), one thread per body in ID order.
 cudaError_t launch_interp_kick(float4* bodies, float2* accel, const float2* force,
@@ -301,7 +303,7 @@ struct ShortRangeArgs {
 };
 struct SlotsArgs {
     const int* cell_start; const int* cell_count; const uint32_t* cell_mass; const float4* entries;
-    float4* slots; int W, H;
+    float4* slots; int W, H; float gravity, total_mass;
 };
 struct KickArgs {
     float4* bodies; float2* accel; const float2* force; const float2* a_short; KickParams p;
@@ -411,7 +413,7 @@ struct p3m_ctx {
     int* cell_count = nullptr;
     uint32_t* cell_mass = nullptr;
     float4* entries = nullptr;
-    float4* cell_slots = nullptr;  // per cell: the two source slots of the short range
+    float4* cell_slots = nullptr;  // per cell: the two source slots of the short range (24 B)
     float2* a_short = nullptr;  // short-range accelerations, by body ID
     int4* deposit_work = nullptr;  // pieces of heavy mesh tiles (+1 counter)
     size_t deposit_work_capacity = 0;

@@ -63,12 +63,13 @@ __global__ void __launch_bounds__(256) interp_kick_kernel(
 // for a non-home cell (kick.comp:128-146 with exact limit 2). A cell of more
 // than two bodies is its monopole at the cell centre; one of up to two bodies
 // gives its entries; missing slots are massless at the centre, so they add
-// nothing. The short range then reads 32 bytes per cell instead of the
-// count -> start -> entries chain; the values are those it read before.
+// nothing. The short range then reads 24 bytes per cell instead of the
+// count -> start -> entries chain. A slot holds x, y and G m / M_tot, the
+// product the pair term forms first.
 __device__ __forceinline__ void cell_slots_body(
     int block, const int* __restrict__ cell_start, const int* __restrict__ cell_count,
     const uint32_t* __restrict__ cell_mass, const float4* __restrict__ entries, int W, int H,
-    float4* __restrict__ slots) {
+    float gravity, float total_mass, float4* __restrict__ slots) {
     const int index = block * blockDim.x + threadIdx.x;
     if (index >= W * H) return;
     const int row = index / W, col = index - row * W;
@@ -83,22 +84,26 @@ __device__ __forceinline__ void cell_slots_body(
         s0 = entries[start];
         if (count == 2) s1 = entries[start + 1];
     }
-    slots[2 * index] = s0;
-    slots[2 * index + 1] = s1;
+    const float g_over_m = gravity / total_mass;
+    // Two planes: (x0, y0, gm0, x1) for every cell, then (y1, gm1).
+    slots[index] = make_float4(s0.x, s0.y, g_over_m * s0.z, s1.x);
+    reinterpret_cast<float2*>(slots + (size_t)W * H)[index] = make_float2(s1.y, g_over_m * s1.z);
 }
 
 __global__ void __launch_bounds__(256) cell_slots_kernel(
     const int* __restrict__ cell_start, const int* __restrict__ cell_count,
     const uint32_t* __restrict__ cell_mass, const float4* __restrict__ entries, int W, int H,
-    float4* __restrict__ slots) {
-    cell_slots_body(blockIdx.x, cell_start, cell_count, cell_mass, entries, W, H, slots);
+    float gravity, float total_mass, float4* __restrict__ slots) {
+    cell_slots_body(blockIdx.x, cell_start, cell_count, cell_mass, entries, W, H, gravity,
+                    total_mass, slots);
 }
 
 __global__ void __launch_bounds__(256) cell_slots_batched_kernel(
     const SlotsArgs* __restrict__ args, const int* __restrict__ first, int sims) {
     const int2 sb = batch_block(first, sims);
     const SlotsArgs a = args[sb.x];
-    cell_slots_body(sb.y, a.cell_start, a.cell_count, a.cell_mass, a.entries, a.W, a.H, a.slots);
+    cell_slots_body(sb.y, a.cell_start, a.cell_count, a.cell_mass, a.entries, a.W, a.H,
+                    a.gravity, a.total_mass, a.slots);
 }
 
 __global__ void __launch_bounds__(256) interp_kick_batched_kernel(
@@ -119,11 +124,12 @@ cudaError_t batched_interp_kick(const KickArgs* a, BatchGrid g, cudaStream_t s) 
 
 cudaError_t launch_cell_slots(const int* cell_start, const int* cell_count,
                               const uint32_t* cell_mass, const float4* entries, int W, int H,
-                              float4* slots, cudaStream_t stream) {
+                              float gravity, float total_mass, float4* slots,
+                              cudaStream_t stream) {
     const int cells = W * H;
     if (cells <= 0) return cudaSuccess;
-    cell_slots_kernel<<<(cells + 255) / 256, 256, 0, stream>>>(cell_start, cell_count, cell_mass,
-                                                                entries, W, H, slots);
+    cell_slots_kernel<<<(cells + 255) / 256, 256, 0, stream>>>(
+        cell_start, cell_count, cell_mass, entries, W, H, gravity, total_mass, slots);
     count_launches(1);
     return cudaGetLastError();
 }

@@ -80,6 +80,17 @@ __device__ __forceinline__ void pair_add(const PairConst& k, float dx, float dy,
     ay = fmaf(phys, dy, ay);
 }
 
+// pair_add with the source's G m / M_tot already formed (a cell slot).
+__device__ __forceinline__ void pair_add_gm(const PairConst& k, float dx, float dy, float gm,
+                                            float& ax, float& ay) {
+    const float px = dx * k.aspect;
+    const float r2 = fmaf(px, px, dy * dy);
+    const float w = fast_exp2(r2 * k.neg_log2e_over_2s2);
+    const float phys = __fdividef(gm * w, fmaxf(r2, k.min_dist2));
+    ax = fmaf(phys, dx, ax);
+    ay = fmaf(phys, dy, ay);
+}
+
 template <int RX, int RY, int EXACT>
 __device__ __forceinline__ void short_range_body(
     int block, const float4* __restrict__ bodies, const float4* __restrict__ entries,
@@ -92,12 +103,17 @@ __device__ __forceinline__ void short_range_body(
     const uint32_t id = (uint32_t)i;
     const PairConst k = pair_const(p);
     const float inv_w = 1.0f / (float)p.W, inv_h = 1.0f / (float)p.H;
+    const float2* __restrict__ slots_b =
+        reinterpret_cast<const float2*>(slots + (size_t)p.W * p.H);
     const int hx = guard_coord(float_to_int(floorf(t.x * (float)p.W)), p.W);
     const int hy = guard_coord(float_to_int(floorf(t.y * (float)p.H)), p.H);
 
     // Per stencil column: wrapped column, periodic image shift, validity.
+    // off_x: the image shift less the target's x, so that a source at x on
+    // that column is at dx = x + off_x (exactly x - t.x where no wrap).
     int col[2 * RX + 1];
     float shift_x[2 * RX + 1];
+    float off_x[2 * RX + 1];
     bool ok_x[2 * RX + 1];
 #pragma unroll
     for (int a = 0; a < 2 * RX + 1; ++a) {
@@ -105,6 +121,7 @@ __device__ __forceinline__ void short_range_body(
         const int wx = wrap_index(cx, p.W);
         col[a] = wx;
         shift_x[a] = (float)(cx - wx) * inv_w;
+        off_x[a] = shift_x[a] - t.x;
         ok_x[a] = !p.bounded || (cx >= 0 && cx < p.W);
     }
     float ax = 0.0f, ay = 0.0f;
@@ -116,17 +133,19 @@ __device__ __forceinline__ void short_range_body(
         const int row = wy * p.W;
         const float shift_y = (float)(cy - wy) * inv_h;
         const float cyr = ((float)wy + 0.5f) * inv_h;  // wrapped row centre
+        const float off_y = shift_y - t.y;
 #pragma unroll
         for (int a = 0; a < 2 * RX + 1; ++a) {
             if (!ok_x[a]) continue;
             const int index = row + col[a];
             const bool home = (a == RX) && (b == RY);
             if (EXACT == 2 && !home) {
-                // The cell's two slots, prepared once per step (cell_slots).
-                const float4 s0 = __ldg(&slots[2 * index]);
-                const float4 s1 = __ldg(&slots[2 * index + 1]);
-                pair_add(k, (s0.x + shift_x[a]) - t.x, (s0.y + shift_y) - t.y, s0.z, ax, ay);
-                pair_add(k, (s1.x + shift_x[a]) - t.x, (s1.y + shift_y) - t.y, s1.z, ax, ay);
+                // The cell's two slots, prepared once per step (cell_slots):
+                // (x0, y0, G m0 / M_tot, x1) and (y1, G m1 / M_tot).
+                const float4 s0 = __ldg(&slots[index]);
+                const float2 s1 = __ldg(&slots_b[index]);
+                pair_add_gm(k, s0.x + off_x[a], s0.y + off_y, s0.z, ax, ay);
+                pair_add_gm(k, s0.w + off_x[a], s1.x + off_y, s1.y, ax, ay);
                 continue;
             }
             const int count = __ldg(&cell_count[index]);
