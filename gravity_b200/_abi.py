@@ -121,6 +121,7 @@ SIGNATURES = {
     "p3m_host_alloc": (ctypes.c_int, [ctypes.c_size_t, ctypes.POINTER(_vp)]),
     "p3m_host_free": (ctypes.c_int, [_vp]),
     "p3m_nonfinite_count": (ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_int64)]),
+    "p3m_wait_timeouts": (ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_int64)]),
     "p3m_direct_accel_f64": (ctypes.c_int, [_vp, _i32, _vp, _i32, _vp]),
     "p3m_diagnostics_f64": (ctypes.c_int, [_vp, _i32, _vp]),
     "p3m_batch_create": (ctypes.c_int, [ctypes.POINTER(P3MConfig), _i32, ctypes.POINTER(_vp)]),

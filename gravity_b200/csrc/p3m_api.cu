@@ -219,6 +219,7 @@ void free_all(p3m_ctx* ctx) {
     void* ptrs[] = {ctx->diag, ctx->bodies, ctx->bodies_alt, ctx->accel, ctx->accel_alt, ctx->materials,
                     ctx->materials_alt, ctx->destinations, ctx->status, ctx->keys, ctx->vals,
                     ctx->sort.keys_alt, ctx->sort.vals_alt, ctx->sort.hist, ctx->sort.block_sums,
+                    ctx->sort.lookback,
                     ctx->cell_start, ctx->cell_count, ctx->cell_mass, ctx->entries, ctx->cell_slots,
                     ctx->a_short, ctx->deposit_work, ctx->density,
                     ctx->half, ctx->cols, ctx->force, ctx->green, ctx->twiddles};
@@ -645,13 +646,15 @@ int p3m_create(const p3m_config* config, p3m_ctx** out) {
     ALLOC(ctx->materials, cap);
     ALLOC(ctx->materials_alt, cap);
     ALLOC(ctx->destinations, cap);
-    ALLOC(ctx->status, 4);
+    ALLOC(ctx->status, 4);  // [0] non-finite bodies, [1] look-back waits that gave up
+    ctx->sort.wait_timeouts = ctx->status + 1;
     ALLOC(ctx->keys, cap);
     ALLOC(ctx->vals, cap);
     ALLOC(ctx->sort.keys_alt, cap);
     ALLOC(ctx->sort.vals_alt, cap);
     ALLOC(ctx->sort.hist, p3m::sort_hist_entries((int)cap));
     ALLOC(ctx->sort.block_sums, p3m::sort_block_sum_entries((int)cap));
+    ALLOC(ctx->sort.lookback, p3m::sort_lookback_words((int)cap));
     ALLOC(ctx->cell_start, P + 1);
     ALLOC(ctx->cell_count, P);
     ALLOC(ctx->cell_mass, P);
@@ -940,6 +943,16 @@ int p3m_nonfinite_count(p3m_ctx* ctx, int64_t* count) {
     if (!ctx || !count) return P3M_ERR_INVALID_ARGUMENT;
     unsigned int v = 0;
     P3M_CUDA(ctx, cudaMemcpyAsync(&v, ctx->status, sizeof(v), cudaMemcpyDeviceToHost, ctx->stream));
+    P3M_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    *count = (int64_t)v;
+    return P3M_OK;
+}
+
+int p3m_wait_timeouts(p3m_ctx* ctx, int64_t* count) {
+    if (!ctx || !count) return P3M_ERR_INVALID_ARGUMENT;
+    unsigned int v = 0;
+    P3M_CUDA(ctx, cudaMemcpyAsync(&v, ctx->status + 1, sizeof(v), cudaMemcpyDeviceToHost,
+                                  ctx->stream));
     P3M_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
     *count = (int64_t)v;
     return P3M_OK;

@@ -72,16 +72,25 @@ constexpr int kSortItems = 16;
 constexpr int kSortTile = kSortThreads * kSortItems;  // 4096 keys per tile
 constexpr int kSortMaxRadix = 256;
 
+constexpr int kSortMaxPasses = 4;
+
 struct SortScratch {
     uint32_t* keys_alt = nullptr;
     uint32_t* vals_alt = nullptr;
     uint32_t* hist = nullptr;       // kSortMaxRadix * tiles
     uint32_t* block_sums = nullptr; // scan partials
+    // One-kernel-per-pass form (all null: three kernels per pass instead).
+    // `lookback` holds sort_lookback_words(capacity) words: the digit totals
+    // of every pass, the tile counters and the tiles' published counts;
+    // `wait_timeouts` counts look-back waits that gave up.
+    uint32_t* lookback = nullptr;
+    unsigned int* wait_timeouts = nullptr;
     int capacity = 0;
 };
 
 size_t sort_hist_entries(int capacity);
 size_t sort_block_sum_entries(int capacity);
+size_t sort_lookback_words(int capacity);
 
 // Stable LSD radix sort of (keys, vals) on bits [0, key_bits). Passes
 // alternate between the inputs and the scratch pair; *out_keys/*out_vals

@@ -156,21 +156,91 @@ __global__ void __launch_bounds__(kSortThreads) radix_hist_kernel(const uint32_t
     radix_hist_body(blockIdx.x, keys, n, shift, bits, tiles, hist);
 }
 
+// Look-back words: bits 31:30 say what a tile has published for a digit
+// (0 nothing yet, 1 its own count, 2 its inclusive prefix over tiles), bits
+// 29:0 the value. Key counts stay below 2^30.
+constexpr uint32_t kLookbackAggregate = 1u << 30;
+constexpr uint32_t kLookbackInclusive = 2u << 30;
+constexpr uint32_t kLookbackValue = (1u << 30) - 1u;
+constexpr int kLookbackWindow = 16;    // predecessors read per round trip
+constexpr int kLookbackSpins = 200000; // polls of one word before giving up
+constexpr int kLookbackHeader = kSortMaxPasses * kSortMaxRadix + 32;  // totals + tile counters
+
+__device__ __forceinline__ uint32_t load_relaxed(const uint32_t* p) {
+    uint32_t v;
+    asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+__device__ __forceinline__ void store_relaxed(uint32_t* p, uint32_t v) {
+    asm volatile("st.relaxed.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+// Where one tile's keys go, for one digit, with decoupled look-back: the
+// tiles before this one (in the order they took their indices) publish their
+// counts; the sum back to the first inclusive prefix is this tile's offset.
+// Every tile waited on took its index earlier, so it is running and will
+// publish; each wait is still bounded (kLookbackSpins polls), after which it
+// is counted in `timeouts` and taken as 0 so that the kernel always ends.
+__device__ __forceinline__ uint32_t lookback_exclusive(const uint32_t* status, int tile, int d,
+                                                       unsigned int* timeouts) {
+    uint32_t excl = 0;
+    int j = tile - 1;
+    while (j >= 0) {
+        uint32_t w[kLookbackWindow];
+#pragma unroll
+        for (int i = 0; i < kLookbackWindow; ++i)
+            w[i] = j - i >= 0 ? load_relaxed(&status[(size_t)(j - i) * kSortMaxRadix + d])
+                              : kLookbackInclusive;
+#pragma unroll
+        for (int i = 0; i < kLookbackWindow; ++i) {
+            if (j - i < 0) return excl;
+            uint32_t v = w[i];
+            int spins = 0;
+            while ((v & ~kLookbackValue) == 0) {
+                if (++spins > kLookbackSpins) {
+                    atomicAdd(timeouts, 1u);
+                    v = kLookbackInclusive;
+                    break;
+                }
+                __nanosleep(64);
+                v = load_relaxed(&status[(size_t)(j - i) * kSortMaxRadix + d]);
+            }
+            excl += v & kLookbackValue;
+            if (v & kLookbackInclusive) return excl;
+        }
+        j -= kLookbackWindow;
+    }
+    return excl;
+}
+
 // Stable scatter of one tile. Keys of warp w are the contiguous sub-tile
 // [w*32*items, (w+1)*32*items), visited item-major so that (item, lane)
 // increases with the input position. Each key's rank among equal digits comes
 // from __match_any_sync + popc of lower lanes, plus a per-warp running count.
+// The tile's output base per digit comes from the scanned tile histograms
+// (LOOKBACK false), or from the pass's digit totals and a look-back over the
+// tiles before it (LOOKBACK true: the tile index is taken from `counter`, and
+// `hist_scanned` holds the pass's digit totals).
+template <bool LOOKBACK>
 __device__ __forceinline__ void radix_scatter_body(
     int tile, const uint32_t* __restrict__ keys_in, const uint32_t* __restrict__ vals_in,
     uint32_t* __restrict__ keys_out, uint32_t* __restrict__ vals_out, int n, int shift, int bits,
-    int tiles, const uint32_t* __restrict__ hist_scanned) {
+    int tiles, const uint32_t* __restrict__ hist_scanned, uint32_t* counter = nullptr,
+    uint32_t* status = nullptr, unsigned int* timeouts = nullptr) {
     __shared__ uint32_t warp_hist[kSortWarps][kSortMaxRadix];
     __shared__ uint32_t tile_start[kSortMaxRadix];
     __shared__ uint32_t out_base[kSortMaxRadix];
     __shared__ uint32_t warp_tot[33];
     __shared__ uint32_t s_keys[kSortTile];
     __shared__ uint32_t s_vals[kSortTile];
+    __shared__ int s_tile;
 
+    if (LOOKBACK) {
+        if (threadIdx.x == 0) s_tile = (int)atomicAdd(counter, 1u);
+        __syncthreads();
+        tile = s_tile;
+    }
     const int radix = 1 << bits;
     const uint32_t mask = (uint32_t)radix - 1u;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -209,7 +279,25 @@ __device__ __forceinline__ void radix_scatter_body(
             warp_hist[w][d] = count;
             count += t;
         }
-        out_base[d] = hist_scanned[(size_t)d * tiles + tile];
+        if (LOOKBACK)  // publish this tile's count at once, so successors can go on
+            store_relaxed(&status[(size_t)tile * kSortMaxRadix + d],
+                          (tile == 0 ? kLookbackInclusive : kLookbackAggregate) | count);
+        else
+            out_base[d] = hist_scanned[(size_t)d * tiles + tile];
+    }
+    if (LOOKBACK) {
+        // Start of each digit in the output: exclusive scan of the totals.
+        uint32_t digit_start;
+        block_exclusive_scan(threadIdx.x < radix ? __ldg(&hist_scanned[threadIdx.x]) : 0u,
+                             warp_tot, &digit_start);
+        if (threadIdx.x < radix) {
+            const int d = threadIdx.x;
+            const uint32_t before = lookback_exclusive(status, tile, d, timeouts);
+            if (tile > 0)
+                store_relaxed(&status[(size_t)tile * kSortMaxRadix + d],
+                              kLookbackInclusive | (before + count));
+            out_base[d] = digit_start + before;
+        }
     }
     uint32_t start;
     block_exclusive_scan(threadIdx.x < radix ? count : 0u, warp_tot, &start);
@@ -244,8 +332,77 @@ __global__ void __launch_bounds__(kSortThreads) radix_scatter_kernel(
     const uint32_t* __restrict__ keys_in, const uint32_t* __restrict__ vals_in,
     uint32_t* __restrict__ keys_out, uint32_t* __restrict__ vals_out, int n, int shift, int bits,
     int tiles, const uint32_t* __restrict__ hist_scanned) {
-    radix_scatter_body(blockIdx.x, keys_in, vals_in, keys_out, vals_out, n, shift, bits, tiles,
-                       hist_scanned);
+    radix_scatter_body<false>(blockIdx.x, keys_in, vals_in, keys_out, vals_out, n, shift, bits,
+                              tiles, hist_scanned);
+}
+
+// One pass of the one-kernel-per-pass sort: `totals` = this pass's digit
+// totals, `status` = this pass's [tiles][kSortMaxRadix] look-back words.
+__global__ void __launch_bounds__(kSortThreads) lookback_scatter_kernel(
+    const uint32_t* __restrict__ keys_in, const uint32_t* __restrict__ vals_in,
+    uint32_t* __restrict__ keys_out, uint32_t* __restrict__ vals_out, int n, int shift, int bits,
+    int tiles, const uint32_t* __restrict__ totals, uint32_t* counter, uint32_t* status,
+    unsigned int* timeouts) {
+    radix_scatter_body<true>(0, keys_in, vals_in, keys_out, vals_out, n, shift, bits, tiles,
+                             totals, counter, status, timeouts);
+}
+
+// Digit totals of every pass in one read of the keys: per-CTA shared counts
+// (runs of equal digits added at once, as in radix_hist_body), then one global
+// atomic per CTA and digit. totals[p * kSortMaxRadix + d] must start at zero.
+__global__ void __launch_bounds__(kSortThreads) lookback_totals_kernel(
+    const uint32_t* __restrict__ keys, int n, int passes, int bits, int key_bits,
+    uint32_t* totals) {
+    __shared__ uint32_t h[kSortMaxPasses][kSortMaxRadix];
+    for (int i = threadIdx.x; i < kSortMaxPasses * kSortMaxRadix; i += blockDim.x)
+        (&h[0][0])[i] = 0;
+    __syncthreads();
+    uint32_t run_digit[kSortMaxPasses], run[kSortMaxPasses], mask[kSortMaxPasses];
+#pragma unroll
+    for (int p = 0; p < kSortMaxPasses; ++p) {
+        run_digit[p] = 0xffffffffu;
+        run[p] = 0;
+        const int pb = min(bits, key_bits - p * bits);
+        mask[p] = pb > 0 ? (1u << pb) - 1u : 0u;
+    }
+    for (int base = blockIdx.x * kSortTile; base < n; base += gridDim.x * kSortTile) {
+        const int first = base + threadIdx.x * kSortItems;
+#pragma unroll
+        for (int j = 0; j < kSortItems / 4; ++j) {
+            const int idx = first + j * 4;
+            uint32_t k[4];
+            if (idx + 3 < n) {
+                const uint4 q = __ldg(reinterpret_cast<const uint4*>(keys + idx));
+                k[0] = q.x; k[1] = q.y; k[2] = q.z; k[3] = q.w;
+            } else {
+#pragma unroll
+                for (int e = 0; e < 4; ++e) k[e] = idx + e < n ? keys[idx + e] : 0u;
+            }
+#pragma unroll
+            for (int e = 0; e < 4; ++e) {
+                if (idx + e >= n) continue;
+#pragma unroll
+                for (int p = 0; p < kSortMaxPasses; ++p) {
+                    if (p >= passes) break;
+                    const uint32_t d = (k[e] >> (p * bits)) & mask[p];
+                    if (d != run_digit[p]) {
+                        if (run[p]) atomicAdd(&h[p][run_digit[p]], run[p]);
+                        run_digit[p] = d;
+                        run[p] = 0;
+                    }
+                    ++run[p];
+                }
+            }
+        }
+    }
+#pragma unroll
+    for (int p = 0; p < kSortMaxPasses; ++p)
+        if (p < passes && run[p]) atomicAdd(&h[p][run_digit[p]], run[p]);
+    __syncthreads();
+    for (int i = threadIdx.x; i < passes * kSortMaxRadix; i += blockDim.x) {
+        const uint32_t v = (&h[0][0])[i];
+        if (v) atomicAdd(&totals[i], v);
+    }
 }
 
 // ----------------------------------------------------------- key kernels
@@ -426,7 +583,7 @@ __global__ void __launch_bounds__(kSortThreads) radix_scatter_batched_kernel(
     const RadixArgs* __restrict__ args, const int* __restrict__ first, int sims) {
     const int2 sb = batch_block(first, sims);
     const RadixArgs a = args[sb.x];
-    radix_scatter_body(sb.y, a.keys_in, a.vals_in, a.keys_out, a.vals_out, a.n, a.shift, a.bits,
+    radix_scatter_body<false>(sb.y, a.keys_in, a.vals_in, a.keys_out, a.vals_out, a.n, a.shift, a.bits,
                        a.tiles, a.hist);
 }
 
@@ -482,6 +639,11 @@ size_t sort_hist_entries(int capacity) {
     return (size_t)kSortMaxRadix * (tiles > 0 ? tiles : 1);
 }
 
+size_t sort_lookback_words(int capacity) {
+    const size_t tiles = ((size_t)capacity + kSortTile - 1) / kSortTile;
+    return (size_t)kLookbackHeader + (size_t)kSortMaxPasses * (tiles > 0 ? tiles : 1) * kSortMaxRadix;
+}
+
 size_t sort_block_sum_entries(int capacity) {
     const size_t h = sort_hist_entries(capacity);
     return (h + kScanBlock - 1) / kScanBlock + 1;
@@ -517,6 +679,31 @@ cudaError_t radix_sort_pairs(uint32_t* keys, uint32_t* vals, const SortScratch& 
     uint32_t* vin = vals;
     uint32_t* kout = s.keys_alt;
     uint32_t* vout = s.vals_alt;
+    if (s.lookback && s.wait_timeouts && n < (1 << 30) && passes <= kSortMaxPasses) {
+        // One kernel per pass: the digit totals of all passes first, then each
+        // pass's tiles find their offsets by look-back.
+        const size_t words = (size_t)kLookbackHeader + (size_t)passes * tiles * kSortMaxRadix;
+        cudaError_t e = cudaMemsetAsync(s.lookback, 0, words * sizeof(uint32_t), stream);
+        if (e != cudaSuccess) return e;
+        const int tblocks = min(tiles, 4 * 148);
+        lookback_totals_kernel<<<tblocks, kSortThreads, 0, stream>>>(kin, n, passes, bits,
+                                                                     key_bits, s.lookback);
+        count_launches(1);
+        for (int p = 0; p < passes; ++p) {
+            const int shift = p * bits;
+            const int pbits = min(bits, key_bits - shift);
+            lookback_scatter_kernel<<<tiles, kSortThreads, 0, stream>>>(
+                kin, vin, kout, vout, n, shift, pbits, tiles, s.lookback + p * kSortMaxRadix,
+                s.lookback + kSortMaxPasses * kSortMaxRadix + p,
+                s.lookback + kLookbackHeader + (size_t)p * tiles * kSortMaxRadix, s.wait_timeouts);
+            count_launches(1);
+            uint32_t* tk = kin; kin = kout; kout = tk;
+            uint32_t* tv = vin; vin = vout; vout = tv;
+        }
+        *out_keys = kin;
+        *out_vals = vin;
+        return cudaGetLastError();
+    }
     for (int p = 0; p < passes; ++p) {
         const int shift = p * bits;
         const int pbits = min(bits, key_bits - shift);

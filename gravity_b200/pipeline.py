@@ -274,6 +274,12 @@ class GravityPipeline:
         self._check(self._lib.p3m_nonfinite_count(self._ctx, ctypes.byref(c)))
         return c.value
 
+    def wait_timeouts(self) -> int:
+        """Bounded device waits (sort look-back) that gave up; expected 0."""
+        c = ctypes.c_int64()
+        self._check(self._lib.p3m_wait_timeouts(self._ctx, ctypes.byref(c)))
+        return c.value
+
     def direct_accel_f64(self, n: int, targets) -> np.ndarray:
         """FP64 direct-sum accelerations (unit/s^2) of the target bodies."""
         t = np.ascontiguousarray(targets, np.int32)

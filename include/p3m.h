@@ -223,6 +223,15 @@ int p3m_host_free(void* host);
  * (the reference counts them in measureCluster, GravityPipeline.kt:817-819). */
 int p3m_nonfinite_count(p3m_ctx* ctx, int64_t* count);
 
+/* Bounded device-side waits that gave up since the context was created. The
+ * cell and Morton sorts find each tile's output offsets by looking back at
+ * the tiles before it; every such wait has a poll limit, so a kernel always
+ * ends. A nonzero count means a wait ran out and the results since then
+ * cannot be trusted. Expected to stay 0. No counterpart in the reference
+ * (its sorts are the atomic pushes of build_grid.comp and
+ * spatial_sort_scatter.comp). */
+int p3m_wait_timeouts(p3m_ctx* ctx, int64_t* count);
+
 /* FP64 direct-sum acceleration (unit/s^2) of `n_targets` bodies (IDs in
  * `targets`, host array) from all n bodies: the law the P3M split
  * approximates, G*m*d / (M_tot * max(r^2, r_min^2)) with the minimum image on

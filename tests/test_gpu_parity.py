@@ -99,6 +99,55 @@ def test_steps_match_oracle(cuda_device, name):
         assert rel_rms(b_gpu[:, :2], b_ref[:, :2]) < REL_RMS_TOL
         assert rel_rms(b_gpu[:, 2:], b_ref[:, 2:]) < REL_RMS_TOL
         assert rel_rms(a_gpu, a_ref) < REL_RMS_TOL
+        assert gpu.wait_timeouts() == 0
+
+
+def _numpy_cell_lists(bodies, W, H):
+    """Home cells (build_grid.comp:71-72 in float32) and the list order:
+    cell ascending, body ID descending."""
+    x = bodies[:, 0].astype(np.float32)
+    y = bodies[:, 1].astype(np.float32)
+    hx = np.floor(x * np.float32(W)).astype(np.int64) % W
+    hy = np.floor(y * np.float32(H)).astype(np.int64) % H
+    cell = (hx + hy * W).astype(np.uint32)
+    ids = np.arange(len(bodies), dtype=np.int64)
+    order = np.lexsort((-ids, cell))
+    return cell[order], order.astype(np.int32)
+
+
+@pytest.mark.parametrize("n,grid,seed", [
+    (400_000, (512, 256), 3),        # 17 key bits: 3 passes, 98 tiles
+    (3_000_000, (2048, 1024), 4),    # 21 bits: 3 passes, 733 tiles
+    (1_500_000, (4096, 4096), 5),    # 24 bits (the largest grid): 3 passes of 8
+    (70_000, (256, 128), 6),         # 15 bits: 2 passes
+])
+def test_cell_lists_many_tiles_match_a_stable_sort(cuda_device, n, grid, seed):
+    """Cell lists from the sort whose tiles find their offsets by looking
+    back at earlier tiles: bit-exact against numpy's stable sort, with
+    clustered bodies (long runs of one cell) mixed with uniform ones, and no
+    look-back wait given up."""
+    from gravity_b200.config import GravityFieldConfig, P3MConfig
+    from gravity_b200 import scenarios
+
+    rng = np.random.default_rng(seed)
+    b = np.zeros((n, 4), np.float32)
+    b[:, :2] = rng.uniform(0.0, 1.0, (n, 2))
+    k = n // 3
+    b[:k, :2] = np.clip(rng.normal(0.5, 0.01, (k, 2)), 0.0, 0.99999994)
+    b[:, :2] = np.minimum(b[:, :2], np.float32(0.99999994))
+    cfg = P3MConfig(viewport_width=grid[0], viewport_height=grid[1],
+                    gravity=GravityFieldConfig(grid_width=grid[0], grid_height=grid[1]),
+                    capacity=n)
+    with GravityPipeline(cfg) as gpu:
+        gpu.upload(b, scenarios.unit_materials(n))
+        for _ in range(2):  # twice: the look-back words are cleared per sort
+            gpu.build_cell_lists(n)
+        keys, ids, start, count, _ = gpu.cell_lists(n)
+        assert gpu.wait_timeouts() == 0
+    ek, ei = _numpy_cell_lists(b, *grid)
+    np.testing.assert_array_equal(keys, ek)
+    np.testing.assert_array_equal(ids, ei)
+    np.testing.assert_array_equal(count, np.bincount(ek, minlength=grid[0] * grid[1]))
 
 
 def test_sort_bodies_is_bit_exact_permutation(cuda_device):
