@@ -112,9 +112,17 @@ def stage_bytes(sc, stage: str, radix_passes: int) -> float:
     return 0.0
 
 
+def radix_passes_for_bits(bits: int) -> int:
+    """Passes of the library's radix sort over `bits` key bits: 8-bit digits,
+    or 9-bit digits where they save a pass."""
+    p = (bits + 7) // 8
+    if p > 1 and (bits + 8) // 9 < p:
+        p = (bits + 8) // 9
+    return p
+
+
 def radix_passes_for(count: int) -> int:
-    bits = max(1, (count - 1).bit_length())
-    return (bits + 7) // 8
+    return radix_passes_for_bits(max(1, (count - 1).bit_length()))
 
 
 def read_traffic(stage: str, workload: str):
@@ -477,7 +485,7 @@ def run_b200(args, ws, rank, local):
         cell_passes = radix_passes_for(P)
         from gravity_b200.config import sort_axis_bits
         morton_bits = sort_axis_bits(sc.config.viewport_width) + sort_axis_bits(sc.config.viewport_height)
-        morton_passes = (morton_bits + 7) // 8
+        morton_passes = radix_passes_for_bits(morton_bits)
         stage_rows = {}
         for name, (ms, cnt) in stages.items():
             if cnt == 0:
@@ -622,8 +630,8 @@ def run_batch(args, ws, rank, local):
             passes = radix_passes_for(P)
             if name == "spatial_sort":
                 from gravity_b200.config import sort_axis_bits
-                passes = (sort_axis_bits(sc.config.viewport_width)
-                          + sort_axis_bits(sc.config.viewport_height) + 7) // 8
+                passes = radix_passes_for_bits(sort_axis_bits(sc.config.viewport_width)
+                                               + sort_axis_bits(sc.config.viewport_height))
             r = stage_rows.setdefault(name, {"ms": 0.0, "launches": 0, "bytes": 0.0})
             r["ms"] += ms
             r["launches"] += cnt

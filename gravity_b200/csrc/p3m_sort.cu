@@ -164,7 +164,9 @@ constexpr uint32_t kLookbackInclusive = 2u << 30;
 constexpr uint32_t kLookbackValue = (1u << 30) - 1u;
 constexpr int kLookbackWindow = 16;    // predecessors read per round trip
 constexpr int kLookbackSpins = 200000; // polls of one word before giving up
-constexpr int kLookbackHeader = kSortMaxPasses * kSortMaxRadix + 32;  // totals + tile counters
+// Digits of the look-back sort: 8 bits, or 9 where that saves a pass.
+constexpr int kLookbackMaxRadix = 512;
+constexpr int kLookbackHeader = kSortMaxPasses * kLookbackMaxRadix + 32;  // totals + counters
 
 __device__ __forceinline__ uint32_t load_relaxed(const uint32_t* p) {
     uint32_t v;
@@ -182,6 +184,7 @@ __device__ __forceinline__ void store_relaxed(uint32_t* p, uint32_t v) {
 // Every tile waited on took its index earlier, so it is running and will
 // publish; each wait is still bounded (kLookbackSpins polls), after which it
 // is counted in `timeouts` and taken as 0 so that the kernel always ends.
+// `status` rows are kLookbackMaxRadix words per tile.
 __device__ __forceinline__ uint32_t lookback_exclusive(const uint32_t* status, int tile, int d,
                                                        unsigned int* timeouts) {
     uint32_t excl = 0;
@@ -190,7 +193,7 @@ __device__ __forceinline__ uint32_t lookback_exclusive(const uint32_t* status, i
         uint32_t w[kLookbackWindow];
 #pragma unroll
         for (int i = 0; i < kLookbackWindow; ++i)
-            w[i] = j - i >= 0 ? load_relaxed(&status[(size_t)(j - i) * kSortMaxRadix + d])
+            w[i] = j - i >= 0 ? load_relaxed(&status[(size_t)(j - i) * kLookbackMaxRadix + d])
                               : kLookbackInclusive;
 #pragma unroll
         for (int i = 0; i < kLookbackWindow; ++i) {
@@ -204,7 +207,7 @@ __device__ __forceinline__ uint32_t lookback_exclusive(const uint32_t* status, i
                     break;
                 }
                 __nanosleep(64);
-                v = load_relaxed(&status[(size_t)(j - i) * kSortMaxRadix + d]);
+                v = load_relaxed(&status[(size_t)(j - i) * kLookbackMaxRadix + d]);
             }
             excl += v & kLookbackValue;
             if (v & kLookbackInclusive) return excl;
@@ -221,20 +224,27 @@ __device__ __forceinline__ uint32_t lookback_exclusive(const uint32_t* status, i
 // The tile's output base per digit comes from the scanned tile histograms
 // (LOOKBACK false), or from the pass's digit totals and a look-back over the
 // tiles before it (LOOKBACK true: the tile index is taken from `counter`, and
-// `hist_scanned` holds the pass's digit totals).
-template <bool LOOKBACK>
+// `hist_scanned` holds the pass's digit totals). MAXR bounds the digit count
+// (2^bits); a thread handles MAXR / 256 digits where that is above 1. The
+// per-warp digit counts and the tile staged in digit order share one shared
+// region: each key's slot is taken from the counts before the tile is staged.
+template <bool LOOKBACK, int MAXR>
 __device__ __forceinline__ void radix_scatter_body(
     int tile, const uint32_t* __restrict__ keys_in, const uint32_t* __restrict__ vals_in,
     uint32_t* __restrict__ keys_out, uint32_t* __restrict__ vals_out, int n, int shift, int bits,
     int tiles, const uint32_t* __restrict__ hist_scanned, uint32_t* counter = nullptr,
     uint32_t* status = nullptr, unsigned int* timeouts = nullptr) {
-    __shared__ uint32_t warp_hist[kSortWarps][kSortMaxRadix];
-    __shared__ uint32_t tile_start[kSortMaxRadix];
-    __shared__ uint32_t out_base[kSortMaxRadix];
+    constexpr int kPer = MAXR > kSortThreads ? MAXR / kSortThreads : 1;
+    constexpr int kWarpHist = kSortWarps * MAXR;
+    constexpr int kShared = kWarpHist > 2 * kSortTile ? kWarpHist : 2 * kSortTile;
+    __shared__ uint32_t shared[kShared];  // warp counts, then the staged tile
+    __shared__ uint32_t tile_start[MAXR];
+    __shared__ uint32_t out_base[MAXR];
     __shared__ uint32_t warp_tot[33];
-    __shared__ uint32_t s_keys[kSortTile];
-    __shared__ uint32_t s_vals[kSortTile];
     __shared__ int s_tile;
+    uint32_t* warp_hist = shared;  // [warp * radix + d]
+    uint32_t* s_keys = shared;
+    uint32_t* s_vals = shared + kSortTile;
 
     if (LOOKBACK) {
         if (threadIdx.x == 0) s_tile = (int)atomicAdd(counter, 1u);
@@ -246,9 +256,9 @@ __device__ __forceinline__ void radix_scatter_body(
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int tile_base = tile * kSortTile;
     const int sub_base = tile_base + warp * 32 * kSortItems;
+    uint32_t* my_hist = warp_hist + warp * radix;
 
-    for (int i = threadIdx.x; i < kSortWarps * kSortMaxRadix; i += blockDim.x)
-        (&warp_hist[0][0])[i] = 0;
+    for (int i = threadIdx.x; i < kSortWarps * radix; i += blockDim.x) warp_hist[i] = 0;
     __syncthreads();
 
     uint32_t key[kSortItems], val[kSortItems], rank[kSortItems];
@@ -261,57 +271,88 @@ __device__ __forceinline__ void radix_scatter_body(
         const uint32_t d = valid ? (key[j] >> shift) & mask : 0xffffffffu;
         const unsigned peers = __match_any_sync(kFull, d);
         const uint32_t below = (uint32_t)__popc(peers & lanemask_lt());
-        const uint32_t seen = valid ? warp_hist[warp][d] : 0u;
+        const uint32_t seen = valid ? my_hist[d] : 0u;
         __syncwarp();
-        if (valid && lane == __ffs(peers) - 1) warp_hist[warp][d] = seen + (uint32_t)__popc(peers);
+        if (valid && lane == __ffs(peers) - 1) my_hist[d] = seen + (uint32_t)__popc(peers);
         __syncwarp();
         rank[j] = seen + below;
     }
     __syncthreads();
 
-    // Per digit: exclusive prefix over warps, and the tile's count.
-    uint32_t count = 0;
-    if (threadIdx.x < radix) {
-        const int d = threadIdx.x;
+    // Per digit: exclusive prefix over warps, and the tile's count; thread t
+    // takes digits t*kPer .. t*kPer + kPer - 1.
+    uint32_t count[kPer];
+    uint32_t sum = 0;
 #pragma unroll
-        for (int w = 0; w < kSortWarps; ++w) {
-            uint32_t t = warp_hist[w][d];
-            warp_hist[w][d] = count;
-            count += t;
+    for (int q = 0; q < kPer; ++q) {
+        count[q] = 0;
+        const int d = threadIdx.x * kPer + q;
+        if (d < radix) {
+#pragma unroll
+            for (int w = 0; w < kSortWarps; ++w) {
+                const uint32_t t = warp_hist[w * radix + d];
+                warp_hist[w * radix + d] = count[q];
+                count[q] += t;
+            }
+            if (LOOKBACK)  // publish this tile's count at once, so successors can go on
+                store_relaxed(&status[(size_t)tile * kLookbackMaxRadix + d],
+                              (tile == 0 ? kLookbackInclusive : kLookbackAggregate) | count[q]);
+            else
+                out_base[d] = hist_scanned[(size_t)d * tiles + tile];
+            sum += count[q];
         }
-        if (LOOKBACK)  // publish this tile's count at once, so successors can go on
-            store_relaxed(&status[(size_t)tile * kSortMaxRadix + d],
-                          (tile == 0 ? kLookbackInclusive : kLookbackAggregate) | count);
-        else
-            out_base[d] = hist_scanned[(size_t)d * tiles + tile];
     }
     if (LOOKBACK) {
         // Start of each digit in the output: exclusive scan of the totals.
+        uint32_t total = 0;
+        uint32_t totals[kPer];
+#pragma unroll
+        for (int q = 0; q < kPer; ++q) {
+            const int d = threadIdx.x * kPer + q;
+            totals[q] = d < radix ? __ldg(&hist_scanned[d]) : 0u;
+            total += totals[q];
+        }
         uint32_t digit_start;
-        block_exclusive_scan(threadIdx.x < radix ? __ldg(&hist_scanned[threadIdx.x]) : 0u,
-                             warp_tot, &digit_start);
-        if (threadIdx.x < radix) {
-            const int d = threadIdx.x;
-            const uint32_t before = lookback_exclusive(status, tile, d, timeouts);
-            if (tile > 0)
-                store_relaxed(&status[(size_t)tile * kSortMaxRadix + d],
-                              kLookbackInclusive | (before + count));
-            out_base[d] = digit_start + before;
+        block_exclusive_scan(total, warp_tot, &digit_start);
+#pragma unroll
+        for (int q = 0; q < kPer; ++q) {
+            const int d = threadIdx.x * kPer + q;
+            if (d < radix) {
+                const uint32_t before = lookback_exclusive(status, tile, d, timeouts);
+                if (tile > 0)
+                    store_relaxed(&status[(size_t)tile * kLookbackMaxRadix + d],
+                                  kLookbackInclusive | (before + count[q]));
+                out_base[d] = digit_start + before;
+            }
+            digit_start += totals[q];
         }
     }
     uint32_t start;
-    block_exclusive_scan(threadIdx.x < radix ? count : 0u, warp_tot, &start);
-    if (threadIdx.x < radix) tile_start[threadIdx.x] = start;
+    block_exclusive_scan(sum, warp_tot, &start);
+#pragma unroll
+    for (int q = 0; q < kPer; ++q) {
+        const int d = threadIdx.x * kPer + q;
+        if (d < radix) tile_start[d] = start;
+        start += count[q];
+    }
     __syncthreads();
 
+    // Each key's slot in the tile staged in digit order.
 #pragma unroll
     for (int j = 0; j < kSortItems; ++j) {
         const int idx = sub_base + j * 32 + lane;
         if (idx < n) {
             const uint32_t d = (key[j] >> shift) & mask;
-            const uint32_t pos = tile_start[d] + warp_hist[warp][d] + rank[j];
-            s_keys[pos] = key[j];
-            s_vals[pos] = val[j];
+            rank[j] += tile_start[d] + my_hist[d];
+        }
+    }
+    __syncthreads();  // the counts are read; their space becomes the staged tile
+#pragma unroll
+    for (int j = 0; j < kSortItems; ++j) {
+        const int idx = sub_base + j * 32 + lane;
+        if (idx < n) {
+            s_keys[rank[j]] = key[j];
+            s_vals[rank[j]] = val[j];
         }
     }
     __syncthreads();
@@ -332,29 +373,32 @@ __global__ void __launch_bounds__(kSortThreads) radix_scatter_kernel(
     const uint32_t* __restrict__ keys_in, const uint32_t* __restrict__ vals_in,
     uint32_t* __restrict__ keys_out, uint32_t* __restrict__ vals_out, int n, int shift, int bits,
     int tiles, const uint32_t* __restrict__ hist_scanned) {
-    radix_scatter_body<false>(blockIdx.x, keys_in, vals_in, keys_out, vals_out, n, shift, bits,
-                              tiles, hist_scanned);
+    radix_scatter_body<false, kSortMaxRadix>(blockIdx.x, keys_in, vals_in, keys_out, vals_out, n,
+                                             shift, bits, tiles, hist_scanned);
 }
 
 // One pass of the one-kernel-per-pass sort: `totals` = this pass's digit
-// totals, `status` = this pass's [tiles][kSortMaxRadix] look-back words.
+// totals, `status` = this pass's [tiles][kLookbackMaxRadix] look-back words.
+// MAXR: 256 for 8-bit digits, 512 for 9-bit ones.
+template <int MAXR>
 __global__ void __launch_bounds__(kSortThreads) lookback_scatter_kernel(
     const uint32_t* __restrict__ keys_in, const uint32_t* __restrict__ vals_in,
     uint32_t* __restrict__ keys_out, uint32_t* __restrict__ vals_out, int n, int shift, int bits,
     int tiles, const uint32_t* __restrict__ totals, uint32_t* counter, uint32_t* status,
     unsigned int* timeouts) {
-    radix_scatter_body<true>(0, keys_in, vals_in, keys_out, vals_out, n, shift, bits, tiles,
-                             totals, counter, status, timeouts);
+    radix_scatter_body<true, MAXR>(0, keys_in, vals_in, keys_out, vals_out, n, shift, bits,
+                                   tiles, totals, counter, status, timeouts);
 }
 
 // Digit totals of every pass in one read of the keys: per-CTA shared counts
 // (runs of equal digits added at once, as in radix_hist_body), then one global
-// atomic per CTA and digit. totals[p * kSortMaxRadix + d] must start at zero.
+// atomic per CTA and digit. totals[p * kLookbackMaxRadix + d] must start at
+// zero.
 __global__ void __launch_bounds__(kSortThreads) lookback_totals_kernel(
     const uint32_t* __restrict__ keys, int n, int passes, int bits, int key_bits,
     uint32_t* totals) {
-    __shared__ uint32_t h[kSortMaxPasses][kSortMaxRadix];
-    for (int i = threadIdx.x; i < kSortMaxPasses * kSortMaxRadix; i += blockDim.x)
+    __shared__ uint32_t h[kSortMaxPasses][kLookbackMaxRadix];
+    for (int i = threadIdx.x; i < kSortMaxPasses * kLookbackMaxRadix; i += blockDim.x)
         (&h[0][0])[i] = 0;
     __syncthreads();
     uint32_t run_digit[kSortMaxPasses], run[kSortMaxPasses], mask[kSortMaxPasses];
@@ -399,7 +443,7 @@ __global__ void __launch_bounds__(kSortThreads) lookback_totals_kernel(
     for (int p = 0; p < kSortMaxPasses; ++p)
         if (p < passes && run[p]) atomicAdd(&h[p][run_digit[p]], run[p]);
     __syncthreads();
-    for (int i = threadIdx.x; i < passes * kSortMaxRadix; i += blockDim.x) {
+    for (int i = threadIdx.x; i < passes * kLookbackMaxRadix; i += blockDim.x) {
         const uint32_t v = (&h[0][0])[i];
         if (v) atomicAdd(&totals[i], v);
     }
@@ -583,7 +627,7 @@ __global__ void __launch_bounds__(kSortThreads) radix_scatter_batched_kernel(
     const RadixArgs* __restrict__ args, const int* __restrict__ first, int sims) {
     const int2 sb = batch_block(first, sims);
     const RadixArgs a = args[sb.x];
-    radix_scatter_body<false>(sb.y, a.keys_in, a.vals_in, a.keys_out, a.vals_out, a.n, a.shift, a.bits,
+    radix_scatter_body<false, kSortMaxRadix>(sb.y, a.keys_in, a.vals_in, a.keys_out, a.vals_out, a.n, a.shift, a.bits,
                        a.tiles, a.hist);
 }
 
@@ -641,7 +685,8 @@ size_t sort_hist_entries(int capacity) {
 
 size_t sort_lookback_words(int capacity) {
     const size_t tiles = ((size_t)capacity + kSortTile - 1) / kSortTile;
-    return (size_t)kLookbackHeader + (size_t)kSortMaxPasses * (tiles > 0 ? tiles : 1) * kSortMaxRadix;
+    return (size_t)kLookbackHeader +
+           (size_t)kSortMaxPasses * (tiles > 0 ? tiles : 1) * kLookbackMaxRadix;
 }
 
 size_t sort_block_sum_entries(int capacity) {
@@ -681,21 +726,36 @@ cudaError_t radix_sort_pairs(uint32_t* keys, uint32_t* vals, const SortScratch& 
     uint32_t* vout = s.vals_alt;
     if (s.lookback && s.wait_timeouts && n < (1 << 30) && passes <= kSortMaxPasses) {
         // One kernel per pass: the digit totals of all passes first, then each
-        // pass's tiles find their offsets by look-back.
-        const size_t words = (size_t)kLookbackHeader + (size_t)passes * tiles * kSortMaxRadix;
+        // pass's tiles find their offsets by look-back. With no per-pass
+        // histogram or scan to pay for, 9-bit digits are used where they save
+        // a pass (17 or 18 key bits: 2 passes instead of 3).
+        int lb_passes = passes, lb_bits = bits;
+        if (passes > 1 && (key_bits + 8) / 9 < passes) {
+            lb_passes = (key_bits + 8) / 9;
+            lb_bits = (key_bits + lb_passes - 1) / lb_passes;
+        }
+        const size_t words =
+            (size_t)kLookbackHeader + (size_t)lb_passes * tiles * kLookbackMaxRadix;
         cudaError_t e = cudaMemsetAsync(s.lookback, 0, words * sizeof(uint32_t), stream);
         if (e != cudaSuccess) return e;
         const int tblocks = min(tiles, 4 * 148);
-        lookback_totals_kernel<<<tblocks, kSortThreads, 0, stream>>>(kin, n, passes, bits,
+        lookback_totals_kernel<<<tblocks, kSortThreads, 0, stream>>>(kin, n, lb_passes, lb_bits,
                                                                      key_bits, s.lookback);
         count_launches(1);
-        for (int p = 0; p < passes; ++p) {
-            const int shift = p * bits;
-            const int pbits = min(bits, key_bits - shift);
-            lookback_scatter_kernel<<<tiles, kSortThreads, 0, stream>>>(
-                kin, vin, kout, vout, n, shift, pbits, tiles, s.lookback + p * kSortMaxRadix,
-                s.lookback + kSortMaxPasses * kSortMaxRadix + p,
-                s.lookback + kLookbackHeader + (size_t)p * tiles * kSortMaxRadix, s.wait_timeouts);
+        for (int p = 0; p < lb_passes; ++p) {
+            const int shift = p * lb_bits;
+            const int pbits = min(lb_bits, key_bits - shift);
+            const uint32_t* totals = s.lookback + p * kLookbackMaxRadix;
+            uint32_t* counter = s.lookback + kSortMaxPasses * kLookbackMaxRadix + p;
+            uint32_t* status = s.lookback + kLookbackHeader + (size_t)p * tiles * kLookbackMaxRadix;
+            if (pbits > 8)
+                lookback_scatter_kernel<512><<<tiles, kSortThreads, 0, stream>>>(
+                    kin, vin, kout, vout, n, shift, pbits, tiles, totals, counter, status,
+                    s.wait_timeouts);
+            else
+                lookback_scatter_kernel<256><<<tiles, kSortThreads, 0, stream>>>(
+                    kin, vin, kout, vout, n, shift, pbits, tiles, totals, counter, status,
+                    s.wait_timeouts);
             count_launches(1);
             uint32_t* tk = kin; kin = kout; kout = tk;
             uint32_t* tv = vin; vin = vout; vout = tv;
