@@ -143,6 +143,11 @@ __device__ float2* line_fft(float2* a, float2* b, int L, int log2L, int lines, i
 
 __device__ __forceinline__ int ilog2(int v) { return 31 - __clz(v); }
 
+// Global loads a thread issues before it uses the first of them, in the loops
+// that fill shared memory: a CTA of 64 threads moving a 512-point column would
+// otherwise wait out one memory latency per point.
+constexpr int kLoadBatch = 8;
+
 // ---------------------------------------------------------------- kernels
 // 1. forward rows: fft_init.comp (fixed point -> float) fused with the row
 // transform. Two rows per complex line.
@@ -157,12 +162,25 @@ __device__ __forceinline__ void fft_rows_forward_body(int block, const T* __rest
     const int pairs = min(pairs_per_cta, MH / 2 - pair0);
     float2* a = sm;
     float2* b = sm + pairs_per_cta * MW;
-    for (int t = threadIdx.x; t < pairs * MW; t += blockDim.x) {
-        const int p = t / MW, x = t - p * MW;
-        const size_t row = (size_t)(pair0 + p) * 2;
-        const float re = (float)density[row * MW + x] * inv_scale;
-        const float im = (float)density[(row + 1) * MW + x] * inv_scale;
-        a[p * MW + x] = make_float2(re, im);
+    const int total = pairs * MW;
+    for (int t0 = threadIdx.x; t0 < total; t0 += kLoadBatch * blockDim.x) {
+        T lo[kLoadBatch], hi[kLoadBatch];
+#pragma unroll
+        for (int u = 0; u < kLoadBatch; ++u) {
+            const int t = t0 + u * blockDim.x;
+            if (t < total) {
+                const int p = t / MW, x = t - p * MW;
+                const size_t row = (size_t)(pair0 + p) * 2;
+                lo[u] = density[row * MW + x];
+                hi[u] = density[(row + 1) * MW + x];
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < kLoadBatch; ++u) {
+            const int t = t0 + u * blockDim.x;
+            if (t < total)
+                a[t] = make_float2((float)lo[u] * inv_scale, (float)hi[u] * inv_scale);
+        }
     }
     __syncthreads();
     float2* z = line_fft(a, b, MW, ilog2(MW), pairs, MW, false, tw);
@@ -213,19 +231,64 @@ __device__ __forceinline__ void fft_columns_body(int block, const float2* __rest
     float2* A = sm;
     float2* B = sm + G * MH;
     float2* C = sm + 2 * G * MH;
-    for (int t = threadIdx.x; t < ncols * MH; t += blockDim.x) {
-        const int y = t / ncols, c = t - y * ncols;
-        A[c * MH + y] = half[(size_t)y * SW + kx0 + c];
+    const int total = ncols * MH;
+    for (int t0 = threadIdx.x; t0 < total; t0 += kLoadBatch * blockDim.x) {
+        float2 v[kLoadBatch];
+#pragma unroll
+        for (int u = 0; u < kLoadBatch; ++u) {
+            const int t = t0 + u * blockDim.x;
+            if (t < total) {
+                const int y = t / ncols, c = t - y * ncols;
+                v[u] = half[(size_t)y * SW + kx0 + c];
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < kLoadBatch; ++u) {
+            const int t = t0 + u * blockDim.x;
+            if (t < total) {
+                const int y = t / ncols, c = t - y * ncols;
+                A[c * MH + y] = v[u];
+            }
+        }
+    }
+    // The Green's table entries of the block's bins, fetched while the
+    // forward transform runs.
+    float2 gv[kLoadBatch];
+    const bool g_fits = total <= kLoadBatch * (int)blockDim.x;
+    if (g_fits) {
+#pragma unroll
+        for (int u = 0; u < kLoadBatch; ++u) {
+            const int t = threadIdx.x + u * blockDim.x;
+            if (t < total) {
+                const int y = t / ncols, c = t - y * ncols;
+                gv[u] = __ldg(&green[(size_t)y * SW + kx0 + c]);
+            }
+        }
     }
     __syncthreads();
     const float2* R = line_fft(A, B, MH, logH, ncols, MH, false, tw);
-    for (int t = threadIdx.x; t < ncols * MH; t += blockDim.x) {
-        const int y = t / ncols, c = t - y * ncols;
-        const float2 rho = R[c * MH + y];
-        const float2 g = __ldg(&green[(size_t)y * SW + kx0 + c]);
-        const float gx = g.x * inv_total, gy = g.y * inv_total;
-        C[c * MH + y] = make_float2(-rho.y * gx, rho.x * gx);
-        C[(ncols + c) * MH + y] = make_float2(-rho.y * gy, rho.x * gy);
+    for (int t0 = threadIdx.x; t0 < total; t0 += kLoadBatch * blockDim.x) {
+        if (!g_fits) {
+#pragma unroll
+            for (int u = 0; u < kLoadBatch; ++u) {
+                const int t = t0 + u * blockDim.x;
+                if (t < total) {
+                    const int y = t / ncols, c = t - y * ncols;
+                    gv[u] = __ldg(&green[(size_t)y * SW + kx0 + c]);
+                }
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < kLoadBatch; ++u) {
+            const int t = t0 + u * blockDim.x;
+            if (t < total) {
+                const int y = t / ncols, c = t - y * ncols;
+                const float2 rho = R[c * MH + y];
+                const float gx = gv[u].x * inv_total, gy = gv[u].y * inv_total;
+                C[c * MH + y] = make_float2(-rho.y * gx, rho.x * gx);
+                C[(ncols + c) * MH + y] = make_float2(-rho.y * gy, rho.x * gy);
+            }
+        }
     }
     __syncthreads();
     const float2* F = line_fft(C, A, MH, logH, 2 * ncols, MH, true, tw);
@@ -331,15 +394,31 @@ __device__ __forceinline__ void fft_rows_inverse_body(int block, const float4* _
     const int SW = MW / 2 + 1;
     float2* a = sm;
     float2* b = sm + rows_per_cta * MW;
-    for (int t = threadIdx.x; t < rows * SW; t += blockDim.x) {
-        const int r = t / SW, kx = t - r * SW;
-        const float4 q = cols[(size_t)(row0 + r) * SW + kx];  // (Fx.re, Fx.im, Fy.re, Fy.im)
-        if (kx == 0 || kx == MW / 2) {
-            // DC and Nyquist bins of a real row are real.
-            a[r * MW + kx] = make_float2(q.x, q.z);
-        } else {
-            a[r * MW + kx] = make_float2(q.x - q.w, q.y + q.z);
-            a[r * MW + (MW - kx)] = make_float2(q.x + q.w, q.z - q.y);
+    const int total = rows * SW;
+    for (int t0 = threadIdx.x; t0 < total; t0 += kLoadBatch * blockDim.x) {
+        float4 v[kLoadBatch];
+#pragma unroll
+        for (int u = 0; u < kLoadBatch; ++u) {
+            const int t = t0 + u * blockDim.x;
+            if (t < total) {
+                const int r = t / SW, kx = t - r * SW;
+                v[u] = cols[(size_t)(row0 + r) * SW + kx];  // (Fx.re, Fx.im, Fy.re, Fy.im)
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < kLoadBatch; ++u) {
+            const int t = t0 + u * blockDim.x;
+            if (t < total) {
+                const int r = t / SW, kx = t - r * SW;
+                const float4 q = v[u];
+                if (kx == 0 || kx == MW / 2) {
+                    // DC and Nyquist bins of a real row are real.
+                    a[r * MW + kx] = make_float2(q.x, q.z);
+                } else {
+                    a[r * MW + kx] = make_float2(q.x - q.w, q.y + q.z);
+                    a[r * MW + (MW - kx)] = make_float2(q.x + q.w, q.z - q.y);
+                }
+            }
         }
     }
     __syncthreads();
