@@ -91,6 +91,90 @@ __device__ __forceinline__ void pair_add_gm(const PairConst& k, float dx, float 
     ay = fmaf(phys, dy, ay);
 }
 
+// Cells of the slot table a CTA stages in shared memory (24 bytes each): the
+// box spanned by its bodies' stencils, when it holds at most this many.
+constexpr int kStageCells = 1536;
+
+struct StageBox {
+    int x0, y0, w;  // box origin (unwrapped cell coordinates) and width
+    bool staged;
+};
+
+// The two-slot form (EXACT = 2) stages, per CTA, the slot-table box covering
+// every stencil of its bodies: after the Morton reorder a CTA's bodies are a
+// compact patch, so the box is a few hundred cells that every lane then reads
+// from shared memory instead of each lane fetching its 48 cells through L1.
+// A CTA whose box is larger than kStageCells (a patch split across the torus
+// seam, or sparse bodies) reads the table from global memory. All threads of
+// the CTA take part (none may have returned).
+template <int RX, int RY>
+__device__ __forceinline__ StageBox stage_slots(bool valid, int hx, int hy,
+                                                const float4* __restrict__ slots,
+                                                const float2* __restrict__ slots_b,
+                                                const KickParams& p, float4* st_a, float2* st_b,
+                                                int* red) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, warps = blockDim.x >> 5;
+    const int mnx = __reduce_min_sync(0xffffffffu, valid ? hx : 0x7fffffff);
+    const int mxx = __reduce_max_sync(0xffffffffu, valid ? hx : (int)0x80000000);
+    const int mny = __reduce_min_sync(0xffffffffu, valid ? hy : 0x7fffffff);
+    const int mxy = __reduce_max_sync(0xffffffffu, valid ? hy : (int)0x80000000);
+    if (lane == 0) {
+        red[warp * 4 + 0] = mnx;
+        red[warp * 4 + 1] = mxx;
+        red[warp * 4 + 2] = mny;
+        red[warp * 4 + 3] = mxy;
+    }
+    __syncthreads();
+    int x0 = 0x7fffffff, x1 = (int)0x80000000, y0 = 0x7fffffff, y1 = (int)0x80000000;
+    for (int w = 0; w < warps; ++w) {
+        x0 = min(x0, red[w * 4 + 0]);
+        x1 = max(x1, red[w * 4 + 1]);
+        y0 = min(y0, red[w * 4 + 2]);
+        y1 = max(y1, red[w * 4 + 3]);
+    }
+    StageBox box;
+    box.x0 = x0 - RX;
+    box.y0 = y0 - RY;
+    const long long bw = (long long)x1 - x0 + 1 + 2 * RX;
+    const long long bh = (long long)y1 - y0 + 1 + 2 * RY;
+    box.w = (int)bw;
+    box.staged = bw * bh <= kStageCells;
+    if (box.staged) {
+        const int cells = (int)(bw * bh);
+        constexpr int kBatch = 4;
+        for (int c0 = threadIdx.x; c0 < cells; c0 += kBatch * blockDim.x) {
+            float4 va[kBatch];
+            float2 vb[kBatch];
+#pragma unroll
+            for (int u = 0; u < kBatch; ++u) {
+                const int c = c0 + u * blockDim.x;
+                va[u] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+                vb[u] = make_float2(0.0f, 0.0f);
+                if (c < cells) {
+                    const int r = c / box.w;
+                    const int cx = box.x0 + (c - r * box.w), cy = box.y0 + r;
+                    // Cells beyond a wall are never read.
+                    if (!p.bounded || (cx >= 0 && cx < p.W && cy >= 0 && cy < p.H)) {
+                        const int cell = wrap_index(cy, p.H) * p.W + wrap_index(cx, p.W);
+                        va[u] = __ldg(&slots[cell]);
+                        vb[u] = __ldg(&slots_b[cell]);
+                    }
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < kBatch; ++u) {
+                const int c = c0 + u * blockDim.x;
+                if (c < cells) {
+                    st_a[c] = va[u];
+                    st_b[c] = vb[u];
+                }
+            }
+        }
+    }
+    __syncthreads();
+    return box;
+}
+
 template <int RX, int RY, int EXACT>
 __device__ __forceinline__ void short_range_body(
     int block, const float4* __restrict__ bodies, const float4* __restrict__ entries,
@@ -98,8 +182,9 @@ __device__ __forceinline__ void short_range_body(
     const uint32_t* __restrict__ cell_mass, const float4* __restrict__ slots,
     float2* __restrict__ a_short, const KickParams& p) {
     const int i = block * blockDim.x + threadIdx.x;
-    if (i >= p.n) return;
-    const float4 t = bodies[i];
+    const bool valid = i < p.n;
+    if (EXACT != 2 && !valid) return;
+    const float4 t = valid ? bodies[i] : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
     const uint32_t id = (uint32_t)i;
     const PairConst k = pair_const(p);
     const float inv_w = 1.0f / (float)p.W, inv_h = 1.0f / (float)p.H;
@@ -107,6 +192,21 @@ __device__ __forceinline__ void short_range_body(
         reinterpret_cast<const float2*>(slots + (size_t)p.W * p.H);
     const int hx = guard_coord(float_to_int(floorf(t.x * (float)p.W)), p.W);
     const int hy = guard_coord(float_to_int(floorf(t.y * (float)p.H)), p.H);
+
+    StageBox box{0, 0, 0, false};
+    int sbase = 0;
+    float4* st_a = nullptr;
+    float2* st_b = nullptr;
+    if (EXACT == 2) {
+        __shared__ float4 stage_a[kStageCells];
+        __shared__ float2 stage_b[kStageCells];
+        __shared__ int red[4 * 32];
+        st_a = stage_a;
+        st_b = stage_b;
+        box = stage_slots<RX, RY>(valid, hx, hy, slots, slots_b, p, stage_a, stage_b, red);
+        if (!valid) return;
+        if (box.staged) sbase = (hy - RY - box.y0) * box.w + (hx - RX - box.x0);
+    }
 
     // Per stencil column: wrapped column, periodic image shift, validity.
     // off_x: the image shift less the target's x, so that a source at x on
@@ -142,8 +242,16 @@ __device__ __forceinline__ void short_range_body(
             if (EXACT == 2 && !home) {
                 // The cell's two slots, prepared once per step (cell_slots):
                 // (x0, y0, G m0 / M_tot, x1) and (y1, G m1 / M_tot).
-                const float4 s0 = __ldg(&slots[index]);
-                const float2 s1 = __ldg(&slots_b[index]);
+                float4 s0;
+                float2 s1;
+                if (box.staged) {
+                    const int si = sbase + b * box.w + a;
+                    s0 = st_a[si];
+                    s1 = st_b[si];
+                } else {
+                    s0 = __ldg(&slots[index]);
+                    s1 = __ldg(&slots_b[index]);
+                }
                 pair_add_gm(k, s0.x + off_x[a], s0.y + off_y, s0.z, ax, ay);
                 pair_add_gm(k, s0.w + off_x[a], s1.x + off_y, s1.y, ax, ay);
                 continue;
