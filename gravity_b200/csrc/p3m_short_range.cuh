@@ -80,6 +80,30 @@ __device__ __forceinline__ void pair_add(const PairConst& k, float dx, float dy,
     ay = fmaf(phys, dy, ay);
 }
 
+// 1/x by the hardware's approximate reciprocal (PTX rcp.approx.ftz.f32): the
+// pair term's division is by max(r^2, r_min^2), far from the flushed range.
+__device__ __forceinline__ float fast_rcp(float x) {
+    float y;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+
+// A cell's two slots at once with Blackwell's packed FP32x2 arithmetic (each
+// half rounded as one scalar operation): the pair term of pair_add_gm for
+// source 0 in .x and source 1 in .y, accumulated into (ax, ay) per slot.
+__device__ __forceinline__ void pair_add2_gm(const PairConst& k, float2 dx, float2 dy, float2 gm,
+                                             float2& ax, float2& ay) {
+    const float2 px = __fmul2_rn(dx, make_float2(k.aspect, k.aspect));
+    const float2 r2 = __ffma2_rn(px, px, __fmul2_rn(dy, dy));
+    const float2 e = __fmul2_rn(r2, make_float2(k.neg_log2e_over_2s2, k.neg_log2e_over_2s2));
+    const float2 num = __fmul2_rn(gm, make_float2(fast_exp2(e.x), fast_exp2(e.y)));
+    const float2 inv = make_float2(fast_rcp(fmaxf(r2.x, k.min_dist2)),
+                                   fast_rcp(fmaxf(r2.y, k.min_dist2)));
+    const float2 phys = __fmul2_rn(num, inv);
+    ax = __ffma2_rn(phys, dx, ax);
+    ay = __ffma2_rn(phys, dy, ay);
+}
+
 // pair_add with the source's G m / M_tot already formed (a cell slot).
 __device__ __forceinline__ void pair_add_gm(const PairConst& k, float dx, float dy, float gm,
                                             float& ax, float& ay) {
@@ -225,6 +249,7 @@ __device__ __forceinline__ void short_range_body(
         ok_x[a] = !p.bounded || (cx >= 0 && cx < p.W);
     }
     float ax = 0.0f, ay = 0.0f;
+    float2 ax2 = make_float2(0.0f, 0.0f), ay2 = make_float2(0.0f, 0.0f);  // per slot
 #pragma unroll
     for (int b = 0; b < 2 * RY + 1; ++b) {
         const int cy = hy + b - RY;
@@ -252,8 +277,11 @@ __device__ __forceinline__ void short_range_body(
                     s0 = __ldg(&slots[index]);
                     s1 = __ldg(&slots_b[index]);
                 }
-                pair_add_gm(k, s0.x + off_x[a], s0.y + off_y, s0.z, ax, ay);
-                pair_add_gm(k, s0.w + off_x[a], s1.x + off_y, s1.y, ax, ay);
+                const float2 ox = make_float2(off_x[a], off_x[a]);
+                const float2 oy = make_float2(off_y, off_y);
+                pair_add2_gm(k, __fadd2_rn(make_float2(s0.x, s0.w), ox),
+                             __fadd2_rn(make_float2(s0.y, s1.x), oy), make_float2(s0.z, s1.y),
+                             ax2, ay2);
                 continue;
             }
             const int count = __ldg(&cell_count[index]);
@@ -274,7 +302,7 @@ __device__ __forceinline__ void short_range_body(
             }
         }
     }
-    a_short[id] = make_float2(ax, ay);
+    a_short[id] = make_float2(ax + (ax2.x + ax2.y), ay + (ay2.x + ay2.y));
 }
 
 template <int RX, int RY, int EXACT>
