@@ -349,6 +349,7 @@ __global__ void __launch_bounds__(kThreads) deposit_tiles_kernel(
     const float4* __restrict__ entries, const int* __restrict__ cell_start, TileGeom g,
     float scale, T* __restrict__ density, int4* __restrict__ work, int* __restrict__ work_count,
     int work_capacity) {
+    grid_dependency_wait();
     __shared__ TileAcc<T> acc;
     __shared__ int run_begin[kMaxRuns], run_end[kMaxRuns], run_prefix[kMaxRuns];
     __shared__ int s_total;
@@ -386,6 +387,7 @@ __global__ void __launch_bounds__(kThreads) deposit_heavy_kernel(
     const float4* __restrict__ entries, const int* __restrict__ cell_start, TileGeom g,
     float scale, T* __restrict__ density, const int4* __restrict__ work,
     const int* __restrict__ work_count, int work_capacity) {
+    grid_dependency_wait();
     __shared__ TileAcc<T> acc;
     __shared__ int run_begin[kMaxRuns], run_end[kMaxRuns], run_prefix[kMaxRuns];
     __shared__ int s_total;
@@ -482,6 +484,7 @@ template <typename T>
 __global__ void __launch_bounds__(kThreads) deposit_chunks_kernel(
     const float4* __restrict__ entries, const uint32_t* __restrict__ keys, int n, int W, int H,
     int MW, int MH, float scale, T* __restrict__ density, int window_cap) {
+    grid_dependency_wait();
     deposit_chunks_body<T>(blockIdx.x, entries, keys, n, W, H, MW, MH, scale, density, window_cap);
 }
 
@@ -555,12 +558,12 @@ cudaError_t launch_deposit(const float4* entries, const uint32_t* keys, const in
         const int blocks = (n + kChunkEntries - 1) / kChunkEntries;
         if (i64) {
             using T = unsigned long long;
-            deposit_chunks_kernel<T><<<blocks, kThreads, kWindowBytes, stream>>>(
+            launch_chained(deposit_chunks_kernel<T>, blocks, kThreads, kWindowBytes, stream,
                 entries, keys, n, g.W, g.H, g.MW, g.MH, 4294967296.0f, static_cast<T*>(density),
                 kWindowBytes / (int)sizeof(T));
         } else {
             using T = uint32_t;
-            deposit_chunks_kernel<T><<<blocks, kThreads, kWindowBytes, stream>>>(
+            launch_chained(deposit_chunks_kernel<T>, blocks, kThreads, kWindowBytes, stream,
                 entries, keys, n, g.W, g.H, g.MW, g.MH, mass_scale, static_cast<T*>(density),
                 kWindowBytes / (int)sizeof(T));
         }
@@ -575,18 +578,18 @@ cudaError_t launch_deposit(const float4* entries, const uint32_t* keys, const in
     if (heavy_blocks > work_capacity) heavy_blocks = work_capacity > 0 ? work_capacity : 1;
     if (deposit_mode == P3M_DEPOSIT_I64) {
         using T = unsigned long long;
-        deposit_tiles_kernel<T><<<tiles, kThreads, 0, stream>>>(
+        launch_chained(deposit_tiles_kernel<T>, tiles, kThreads, 0, stream,
             entries, cell_start, t, 4294967296.0f, static_cast<T*>(density), work, work_count,
             work_capacity);
-        deposit_heavy_kernel<T><<<heavy_blocks, kThreads, 0, stream>>>(
+        launch_chained(deposit_heavy_kernel<T>, heavy_blocks, kThreads, 0, stream,
             entries, cell_start, t, 4294967296.0f, static_cast<T*>(density), work, work_count,
             work_capacity);
     } else {
         using T = uint32_t;
-        deposit_tiles_kernel<T><<<tiles, kThreads, 0, stream>>>(
+        launch_chained(deposit_tiles_kernel<T>, tiles, kThreads, 0, stream,
             entries, cell_start, t, mass_scale, static_cast<T*>(density), work, work_count,
             work_capacity);
-        deposit_heavy_kernel<T><<<heavy_blocks, kThreads, 0, stream>>>(
+        launch_chained(deposit_heavy_kernel<T>, heavy_blocks, kThreads, 0, stream,
             entries, cell_start, t, mass_scale, static_cast<T*>(density), work, work_count,
             work_capacity);
     }

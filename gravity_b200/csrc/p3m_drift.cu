@@ -57,6 +57,7 @@ __global__ void drift_kernel(float4* __restrict__ bodies, const float2* __restri
                              float half_kick, float drift_dt, int substeps, int bounded, int W,
                              int H, uint32_t* __restrict__ keys, uint32_t* __restrict__ vals,
                              unsigned int* __restrict__ nonfinite) {
+    grid_dependency_wait();
     drift_body(blockIdx.x, bodies, accel, n, half_kick, drift_dt, substeps, bounded, W, H, keys,
                vals, nonfinite);
 }
@@ -82,7 +83,7 @@ cudaError_t launch_drift(float4* bodies, const float2* accel, int n, float half_
                          int substeps, GridShape g, uint32_t* keys, uint32_t* vals,
                          unsigned int* nonfinite, cudaStream_t stream) {
     if (n <= 0) return cudaSuccess;
-    drift_kernel<<<(n + 255) / 256, 256, 0, stream>>>(bodies, accel, n, half_kick, drift_dt,
+    launch_chained(drift_kernel, (n + 255) / 256, 256, 0, stream, bodies, accel, n, half_kick, drift_dt,
                                                       substeps, g.bounded, g.W, g.H, keys, vals,
                                                       nonfinite);
     count_launches(1);

@@ -203,6 +203,7 @@ __global__ void __launch_bounds__(256) fft_rows_forward_kernel(const T* __restri
                                                                int pairs_per_cta,
                                                                const float2* __restrict__ tw,
                                                                float2* __restrict__ half) {
+    grid_dependency_wait();
     fft_rows_forward_body<T>(blockIdx.x, density, inv_scale, MW, MH, pairs_per_cta, tw, half);
 }
 
@@ -304,6 +305,7 @@ __global__ void __launch_bounds__(256) fft_columns_kernel(const float2* __restri
                                                           float inv_total, int MW, int MH, int G,
                                                           const float2* __restrict__ tw,
                                                           float4* __restrict__ cols) {
+    grid_dependency_wait();
     fft_columns_body(blockIdx.x, half, green, inv_total, MW, MH, G, tw, cols);
 }
 
@@ -433,6 +435,7 @@ __global__ void __launch_bounds__(256) fft_rows_inverse_kernel(const float4* __r
                                                                int MW, int MH, int rows_per_cta,
                                                                const float2* __restrict__ tw,
                                                                float2* __restrict__ force) {
+    grid_dependency_wait();
     fft_rows_inverse_body(blockIdx.x, cols, MW, MH, rows_per_cta, tw, force);
 }
 
@@ -590,11 +593,11 @@ cudaError_t launch_fft_forward_rows(const void* density, int deposit_mode, float
     const int blocks = (pairs + pairs_per_cta - 1) / pairs_per_cta;
     const size_t smem = (size_t)2 * pairs_per_cta * g.MW * sizeof(float2);
     if (deposit_mode == P3M_DEPOSIT_I64) {
-        fft_rows_forward_kernel<long long><<<blocks, threads, smem, stream>>>(
+        launch_chained(fft_rows_forward_kernel<long long>, blocks, threads, smem, stream,
             static_cast<const long long*>(density), inv_scale, g.MW, g.MH, pairs_per_cta, twiddles,
             half);
     } else {
-        fft_rows_forward_kernel<uint32_t><<<blocks, threads, smem, stream>>>(
+        launch_chained(fft_rows_forward_kernel<uint32_t>, blocks, threads, smem, stream,
             static_cast<const uint32_t*>(density), inv_scale, g.MW, g.MH, pairs_per_cta, twiddles,
             half);
     }
@@ -610,7 +613,7 @@ cudaError_t launch_fft_columns(const float2* half, const float2* green, float in
     const int SW = g.MW / 2 + 1;
     const int blocks = (SW + G - 1) / G;
     const size_t smem = (size_t)4 * G * g.MH * sizeof(float2);
-    fft_columns_kernel<<<blocks, threads, smem, stream>>>(half, green, inv_total, g.MW, g.MH, G,
+    launch_chained(fft_columns_kernel, blocks, threads, smem, stream, half, green, inv_total, g.MW, g.MH, G,
                                                       twiddles, cols);
     count_launches(1);
     return cudaGetLastError();
@@ -647,7 +650,7 @@ cudaError_t launch_fft_adjoint(const float* cotangent, const float2* green, floa
         line_shape(rows, g.MW, g.MW >= 4096 ? 1 : 4096 / g.MW, &rows_per_cta, &threads, g.fft_lines);
         const int blocks = (rows + rows_per_cta - 1) / rows_per_cta;
         const size_t smem = (size_t)2 * rows_per_cta * g.MW * sizeof(float2);
-        fft_rows_inverse_kernel<<<blocks, threads, smem, stream>>>(cols, g.MW, rows, rows_per_cta,
+        launch_chained(fft_rows_inverse_kernel, blocks, threads, smem, stream, cols, g.MW, rows, rows_per_cta,
                                                                twiddles, mu2);
         count_launches(1);
     }
@@ -724,7 +727,7 @@ cudaError_t launch_fft_inverse_rows(const float4* cols, GridShape g, const float
     line_shape(g.MH, g.MW, g.MW >= 4096 ? 1 : 4096 / g.MW, &rows_per_cta, &threads, g.fft_lines);
     const int blocks = (g.MH + rows_per_cta - 1) / rows_per_cta;
     const size_t smem = (size_t)2 * rows_per_cta * g.MW * sizeof(float2);
-    fft_rows_inverse_kernel<<<blocks, threads, smem, stream>>>(cols, g.MW, g.MH, rows_per_cta,
+    launch_chained(fft_rows_inverse_kernel, blocks, threads, smem, stream, cols, g.MW, g.MH, rows_per_cta,
                                                            twiddles, force);
     count_launches(1);
     return cudaGetLastError();

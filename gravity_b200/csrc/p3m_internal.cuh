@@ -245,6 +245,32 @@ cudaError_t launch_conservation(const float4* bodies, const float4* materials, i
 // Process-wide count of kernels launched by this library (p3m_kernel_launches).
 void count_launches(int kernels);
 
+// Kernels of the step's chain start with grid_dependency_wait() and are
+// launched by launch_chained with programmatic stream serialization: the
+// next kernel's CTAs are dispatched while the previous grid drains, and each
+// waits at its first statement until that grid has completed and its writes
+// are visible, so the order of the chain is unchanged. Launched the ordinary
+// way (or after a memset or event), the wait returns at once.
+__device__ __forceinline__ void grid_dependency_wait() {
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+}
+
+template <typename... Params, typename... Args>
+inline cudaError_t launch_chained(void (*kernel)(Params...), dim3 grid, dim3 block, size_t smem,
+                                  cudaStream_t stream, Args... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, kernel, static_cast<Params>(args)...);
+}
+
 // Aim previews (trajectory.comp): one warp per preview, `count` previews.
 cudaError_t launch_trajectories(const KickParams& k, float2 viewport, float min_dt, float max_dt,
                                 float target_segment_px, float max_path_px, float min_dash_px,

@@ -56,6 +56,7 @@ __device__ __forceinline__ void interp_kick_body(
 __global__ void __launch_bounds__(256) interp_kick_kernel(
     float4* __restrict__ bodies, float2* __restrict__ accel, const float2* __restrict__ force,
     const float2* __restrict__ a_short, KickParams p) {
+    grid_dependency_wait();
     interp_kick_body(blockIdx.x, bodies, accel, force, a_short, p);
 }
 
@@ -94,6 +95,7 @@ __global__ void __launch_bounds__(256) cell_slots_kernel(
     const int* __restrict__ cell_start, const int* __restrict__ cell_count,
     const uint32_t* __restrict__ cell_mass, const float4* __restrict__ entries, int W, int H,
     float gravity, float total_mass, float4* __restrict__ slots) {
+    grid_dependency_wait();
     cell_slots_body(blockIdx.x, cell_start, cell_count, cell_mass, entries, W, H, gravity,
                     total_mass, slots);
 }
@@ -128,7 +130,7 @@ cudaError_t launch_cell_slots(const int* cell_start, const int* cell_count,
                               cudaStream_t stream) {
     const int cells = W * H;
     if (cells <= 0) return cudaSuccess;
-    cell_slots_kernel<<<(cells + 255) / 256, 256, 0, stream>>>(
+    launch_chained(cell_slots_kernel, (cells + 255) / 256, 256, 0, stream,
         cell_start, cell_count, cell_mass, entries, W, H, gravity, total_mass, slots);
     count_launches(1);
     return cudaGetLastError();
@@ -180,7 +182,7 @@ cudaError_t launch_short_range(const float4* bodies, const float4* entries, cons
 cudaError_t launch_interp_kick(float4* bodies, float2* accel, const float2* force,
                                const float2* a_short, KickParams p, cudaStream_t stream) {
     if (p.n <= 0) return cudaSuccess;
-    interp_kick_kernel<<<(p.n + 255) / 256, 256, 0, stream>>>(bodies, accel, force, a_short, p);
+    launch_chained(interp_kick_kernel, (p.n + 255) / 256, 256, 0, stream, bodies, accel, force, a_short, p);
     count_launches(1);
     return cudaGetLastError();
 }

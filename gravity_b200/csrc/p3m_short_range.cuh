@@ -311,6 +311,7 @@ __global__ void __launch_bounds__(256) short_range_kernel(
     const int* __restrict__ cell_start, const int* __restrict__ cell_count,
     const uint32_t* __restrict__ cell_mass, const float4* __restrict__ slots,
     float2* __restrict__ a_short, KickParams p) {
+    grid_dependency_wait();
     short_range_body<RX, RY, EXACT>(blockIdx.x, bodies, entries, cell_start, cell_count, cell_mass,
                                     slots, a_short, p);
 }
@@ -362,18 +363,18 @@ P3M_DECLARE_SHORT_RANGE_RX(6)
         const int threads_ = p.sr_threads > 0 ? p.sr_threads : 256;                               \
         const dim3 grid((p.n + threads_ - 1) / threads_), block(threads_);                      \
         switch (p.ry * 2 + (p.exact == 2 ? 1 : 0)) {                                            \
-            case 3: sr::short_range_kernel<RX_, 1, 2><<<grid, block, 0, stream>>>(bodies, entries, cell_start, cell_count, cell_mass, slots, a_short, p); break; \
-            case 2: sr::short_range_kernel<RX_, 1, 0><<<grid, block, 0, stream>>>(bodies, entries, cell_start, cell_count, cell_mass, slots, a_short, p); break; \
-            case 5: sr::short_range_kernel<RX_, 2, 2><<<grid, block, 0, stream>>>(bodies, entries, cell_start, cell_count, cell_mass, slots, a_short, p); break; \
-            case 4: sr::short_range_kernel<RX_, 2, 0><<<grid, block, 0, stream>>>(bodies, entries, cell_start, cell_count, cell_mass, slots, a_short, p); break; \
-            case 7: sr::short_range_kernel<RX_, 3, 2><<<grid, block, 0, stream>>>(bodies, entries, cell_start, cell_count, cell_mass, slots, a_short, p); break; \
-            case 6: sr::short_range_kernel<RX_, 3, 0><<<grid, block, 0, stream>>>(bodies, entries, cell_start, cell_count, cell_mass, slots, a_short, p); break; \
-            case 9: sr::short_range_kernel<RX_, 4, 2><<<grid, block, 0, stream>>>(bodies, entries, cell_start, cell_count, cell_mass, slots, a_short, p); break; \
-            case 8: sr::short_range_kernel<RX_, 4, 0><<<grid, block, 0, stream>>>(bodies, entries, cell_start, cell_count, cell_mass, slots, a_short, p); break; \
-            case 11: sr::short_range_kernel<RX_, 5, 2><<<grid, block, 0, stream>>>(bodies, entries, cell_start, cell_count, cell_mass, slots, a_short, p); break; \
-            case 10: sr::short_range_kernel<RX_, 5, 0><<<grid, block, 0, stream>>>(bodies, entries, cell_start, cell_count, cell_mass, slots, a_short, p); break; \
-            case 13: sr::short_range_kernel<RX_, 6, 2><<<grid, block, 0, stream>>>(bodies, entries, cell_start, cell_count, cell_mass, slots, a_short, p); break; \
-            case 12: sr::short_range_kernel<RX_, 6, 0><<<grid, block, 0, stream>>>(bodies, entries, cell_start, cell_count, cell_mass, slots, a_short, p); break; \
+            case 3: launch_chained(sr::short_range_kernel<RX_, 1, 2>, grid, block, 0, stream, bodies, entries, cell_start, cell_count, cell_mass, slots, a_short, p); break; \
+            case 2: launch_chained(sr::short_range_kernel<RX_, 1, 0>, grid, block, 0, stream, bodies, entries, cell_start, cell_count, cell_mass, slots, a_short, p); break; \
+            case 5: launch_chained(sr::short_range_kernel<RX_, 2, 2>, grid, block, 0, stream, bodies, entries, cell_start, cell_count, cell_mass, slots, a_short, p); break; \
+            case 4: launch_chained(sr::short_range_kernel<RX_, 2, 0>, grid, block, 0, stream, bodies, entries, cell_start, cell_count, cell_mass, slots, a_short, p); break; \
+            case 7: launch_chained(sr::short_range_kernel<RX_, 3, 2>, grid, block, 0, stream, bodies, entries, cell_start, cell_count, cell_mass, slots, a_short, p); break; \
+            case 6: launch_chained(sr::short_range_kernel<RX_, 3, 0>, grid, block, 0, stream, bodies, entries, cell_start, cell_count, cell_mass, slots, a_short, p); break; \
+            case 9: launch_chained(sr::short_range_kernel<RX_, 4, 2>, grid, block, 0, stream, bodies, entries, cell_start, cell_count, cell_mass, slots, a_short, p); break; \
+            case 8: launch_chained(sr::short_range_kernel<RX_, 4, 0>, grid, block, 0, stream, bodies, entries, cell_start, cell_count, cell_mass, slots, a_short, p); break; \
+            case 11: launch_chained(sr::short_range_kernel<RX_, 5, 2>, grid, block, 0, stream, bodies, entries, cell_start, cell_count, cell_mass, slots, a_short, p); break; \
+            case 10: launch_chained(sr::short_range_kernel<RX_, 5, 0>, grid, block, 0, stream, bodies, entries, cell_start, cell_count, cell_mass, slots, a_short, p); break; \
+            case 13: launch_chained(sr::short_range_kernel<RX_, 6, 2>, grid, block, 0, stream, bodies, entries, cell_start, cell_count, cell_mass, slots, a_short, p); break; \
+            case 12: launch_chained(sr::short_range_kernel<RX_, 6, 0>, grid, block, 0, stream, bodies, entries, cell_start, cell_count, cell_mass, slots, a_short, p); break; \
             default: return cudaErrorInvalidValue;                                              \
         }                                                                                       \
         return cudaGetLastError();                                                              \

@@ -386,6 +386,7 @@ __global__ void __launch_bounds__(kSortThreads) lookback_scatter_kernel(
     uint32_t* __restrict__ keys_out, uint32_t* __restrict__ vals_out, int n, int shift, int bits,
     int tiles, const uint32_t* __restrict__ totals, uint32_t* counter, uint32_t* status,
     unsigned int* timeouts) {
+    grid_dependency_wait();
     radix_scatter_body<true, MAXR>(0, keys_in, vals_in, keys_out, vals_out, n, shift, bits,
                                    tiles, totals, counter, status, timeouts);
 }
@@ -397,6 +398,7 @@ __global__ void __launch_bounds__(kSortThreads) lookback_scatter_kernel(
 __global__ void __launch_bounds__(kSortThreads) lookback_totals_kernel(
     const uint32_t* __restrict__ keys, int n, int passes, int bits, int key_bits,
     uint32_t* totals) {
+    grid_dependency_wait();
     __shared__ uint32_t h[kSortMaxPasses][kLookbackMaxRadix];
     for (int i = threadIdx.x; i < kSortMaxPasses * kLookbackMaxRadix; i += blockDim.x)
         (&h[0][0])[i] = 0;
@@ -459,6 +461,7 @@ __device__ __forceinline__ uint32_t home_cell(float x, float y, int W, int H) {
 
 __global__ void cell_keys_kernel(const float4* __restrict__ bodies, int n, int W, int H,
                                  uint32_t* keys, uint32_t* vals) {
+    grid_dependency_wait();
     const int id = blockIdx.x * blockDim.x + threadIdx.x;
     if (id >= n) return;
     const float4 b = bodies[id];
@@ -504,6 +507,7 @@ __device__ __forceinline__ void morton_keys_body(int block, const float4* __rest
 
 __global__ void morton_keys_kernel(const float4* __restrict__ bodies, int n, int wbits, int hbits,
                                    uint32_t* keys, uint32_t* vals) {
+    grid_dependency_wait();
     morton_keys_body(blockIdx.x, bodies, n, wbits, hbits, keys, vals);
 }
 
@@ -528,6 +532,7 @@ __global__ void permute_kernel(const uint32_t* __restrict__ order, int n,
                                const float4* __restrict__ bodies, const float2* __restrict__ accel,
                                const float4* __restrict__ materials, float4* bodies_out,
                                float2* accel_out, float4* materials_out, uint32_t* destinations) {
+    grid_dependency_wait();
     permute_body(blockIdx.x, order, n, bodies, accel, materials, bodies_out, accel_out,
                  materials_out, destinations);
 }
@@ -611,6 +616,7 @@ __global__ void cell_build_kernel(const uint32_t* __restrict__ keys, const uint3
                                   const float4* __restrict__ materials, int* cell_start,
                                   int* cell_count, uint32_t* cell_mass, float4* entries,
                                   int fill_cells) {
+    grid_dependency_wait();
     cell_build_body(blockIdx.x, keys, ids, n, bodies, materials, cell_start, cell_count, cell_mass,
                     entries, fill_cells);
 }
@@ -739,7 +745,7 @@ cudaError_t radix_sort_pairs(uint32_t* keys, uint32_t* vals, const SortScratch& 
         cudaError_t e = cudaMemsetAsync(s.lookback, 0, words * sizeof(uint32_t), stream);
         if (e != cudaSuccess) return e;
         const int tblocks = min(tiles, 4 * 148);
-        lookback_totals_kernel<<<tblocks, kSortThreads, 0, stream>>>(kin, n, lb_passes, lb_bits,
+        launch_chained(lookback_totals_kernel, tblocks, kSortThreads, 0, stream, kin, n, lb_passes, lb_bits,
                                                                      key_bits, s.lookback);
         count_launches(1);
         for (int p = 0; p < lb_passes; ++p) {
@@ -749,11 +755,11 @@ cudaError_t radix_sort_pairs(uint32_t* keys, uint32_t* vals, const SortScratch& 
             uint32_t* counter = s.lookback + kSortMaxPasses * kLookbackMaxRadix + p;
             uint32_t* status = s.lookback + kLookbackHeader + (size_t)p * tiles * kLookbackMaxRadix;
             if (pbits > 8)
-                lookback_scatter_kernel<512><<<tiles, kSortThreads, 0, stream>>>(
+                launch_chained(lookback_scatter_kernel<512>, tiles, kSortThreads, 0, stream,
                     kin, vin, kout, vout, n, shift, pbits, tiles, totals, counter, status,
                     s.wait_timeouts);
             else
-                lookback_scatter_kernel<256><<<tiles, kSortThreads, 0, stream>>>(
+                launch_chained(lookback_scatter_kernel<256>, tiles, kSortThreads, 0, stream,
                     kin, vin, kout, vout, n, shift, pbits, tiles, totals, counter, status,
                     s.wait_timeouts);
             count_launches(1);
@@ -784,7 +790,7 @@ cudaError_t radix_sort_pairs(uint32_t* keys, uint32_t* vals, const SortScratch& 
 cudaError_t launch_cell_keys(const float4* bodies, int n, GridShape g, uint32_t* keys,
                              uint32_t* vals, cudaStream_t stream) {
     if (n <= 0) return cudaSuccess;
-    cell_keys_kernel<<<blocks_for(n, 256), 256, 0, stream>>>(bodies, n, g.W, g.H, keys, vals);
+    launch_chained(cell_keys_kernel, blocks_for(n, 256), 256, 0, stream, bodies, n, g.W, g.H, keys, vals);
     count_launches(1);
     return cudaGetLastError();
 }
@@ -792,7 +798,7 @@ cudaError_t launch_cell_keys(const float4* bodies, int n, GridShape g, uint32_t*
 cudaError_t launch_morton_keys(const float4* bodies, int n, int wbits, int hbits, uint32_t* keys,
                                uint32_t* vals, cudaStream_t stream) {
     if (n <= 0) return cudaSuccess;
-    morton_keys_kernel<<<blocks_for(n, 256), 256, 0, stream>>>(bodies, n, wbits, hbits, keys, vals);
+    launch_chained(morton_keys_kernel, blocks_for(n, 256), 256, 0, stream, bodies, n, wbits, hbits, keys, vals);
     count_launches(1);
     return cudaGetLastError();
 }
@@ -801,7 +807,7 @@ cudaError_t launch_permute(const uint32_t* order, int n, const float4* bodies, c
                            const float4* materials, float4* bodies_out, float2* accel_out,
                            float4* materials_out, uint32_t* destinations, cudaStream_t stream) {
     if (n <= 0) return cudaSuccess;
-    permute_kernel<<<blocks_for(n, 256), 256, 0, stream>>>(order, n, bodies, accel, materials,
+    launch_chained(permute_kernel, blocks_for(n, 256), 256, 0, stream, order, n, bodies, accel, materials,
                                                            bodies_out, accel_out, materials_out,
                                                            destinations);
     count_launches(1);
@@ -836,7 +842,7 @@ cudaError_t launch_cell_build(const uint32_t* keys, const uint32_t* ids, int n, 
             return cudaMemsetAsync(cell_start, 0, ((size_t)fill_cells + 1) * sizeof(int), stream);
         return cudaSuccess;
     }
-    cell_build_kernel<<<blocks_for(n, 256), 256, 0, stream>>>(keys, ids, n, bodies, materials,
+    launch_chained(cell_build_kernel, blocks_for(n, 256), 256, 0, stream, keys, ids, n, bodies, materials,
                                                               cell_start, cell_count, cell_mass,
                                                               entries, fill_cells);
     count_launches(1);
