@@ -90,10 +90,11 @@ __device__ __forceinline__ void dft<8>(float2 (&v)[8], bool inverse) {
 template <int R>
 __device__ __forceinline__ void stockham_pass(const float2* __restrict__ src, float2* __restrict__ dst,
                                               int L, int lines, int pitch, int Ns, int log_ns_r,
-                                              bool inverse, const float2* __restrict__ tw) {
+                                              bool inverse, const float2* __restrict__ tw,
+                                              int tw_log2) {
     const int per_line = L / R;
     const int total = lines * per_line;
-    const int shift = kTwiddleLog2 - log_ns_r;
+    const int shift = tw_log2 - log_ns_r;
     for (int t = threadIdx.x; t < total; t += blockDim.x) {
         const int line = t / per_line;
         const int j = t - line * per_line;
@@ -105,7 +106,7 @@ __device__ __forceinline__ void stockham_pass(const float2* __restrict__ src, fl
         for (int r = 0; r < R; ++r) {
             float2 x = s[j + r * per_line];
             if (r > 0 && k > 0) {
-                float2 w = __ldg(&tw[(k * r) << shift]);
+                float2 w = tw[(k * r) << shift];
                 if (inverse) w.y = -w.y;
                 x = cmulf(x, w);
             }
@@ -119,20 +120,23 @@ __device__ __forceinline__ void stockham_pass(const float2* __restrict__ src, fl
 }
 
 // Complex FFT of `lines` lines held in buffer a (ping-pong buffer b); returns
-// the buffer that holds the result. Ends with __syncthreads().
+// the buffer that holds the result. Ends with __syncthreads(). `tw` holds the
+// roots e^{-2 pi i m / 2^tw_log2}: the global 4096-root table (tw_log2 = 12)
+// or a CTA's copy of the L roots its lines use (tw_log2 = log2 L).
 __device__ float2* line_fft(float2* a, float2* b, int L, int log2L, int lines, int pitch,
-                            bool inverse, const float2* __restrict__ tw) {
+                            bool inverse, const float2* __restrict__ tw,
+                            int tw_log2 = kTwiddleLog2) {
     int Ns = 1, logNs = 0;
     while (Ns < L) {
         const int remaining = log2L - logNs;
         if (remaining >= 3) {
-            stockham_pass<8>(a, b, L, lines, pitch, Ns, logNs + 3, inverse, tw);
+            stockham_pass<8>(a, b, L, lines, pitch, Ns, logNs + 3, inverse, tw, tw_log2);
             Ns <<= 3; logNs += 3;
         } else if (remaining == 2) {
-            stockham_pass<4>(a, b, L, lines, pitch, Ns, logNs + 2, inverse, tw);
+            stockham_pass<4>(a, b, L, lines, pitch, Ns, logNs + 2, inverse, tw, tw_log2);
             Ns <<= 2; logNs += 2;
         } else {
-            stockham_pass<2>(a, b, L, lines, pitch, Ns, logNs + 1, inverse, tw);
+            stockham_pass<2>(a, b, L, lines, pitch, Ns, logNs + 1, inverse, tw, tw_log2);
             Ns <<= 1; logNs += 1;
         }
         __syncthreads();
@@ -148,6 +152,42 @@ __device__ __forceinline__ int ilog2(int v) { return 31 - __clz(v); }
 // otherwise wait out one memory latency per point.
 constexpr int kLoadBatch = 8;
 
+// Lines of up to this many points copy their roots into shared memory; the
+// table of a longer line would cost a CTA per SM, more than its L1 misses.
+constexpr int kStagedTwiddlesMax = 2048;
+__host__ __device__ __forceinline__ int staged_twiddles(int L) {
+    return L <= kStagedTwiddlesMax ? L : 0;
+}
+
+// The L roots e^{-2 pi i m / L} (L = 2^log2L) into shared memory, so that the
+// passes of a line transform read their twiddles there instead of waiting on
+// L1 misses to the global table. Values are the table's; a barrier must
+// follow before use. Returns the table to pass to line_fft with log2 L, or
+// the global table (log2 12) for lines longer than kStagedTwiddlesMax.
+__device__ __forceinline__ const float2* stage_twiddles(const float2* __restrict__ tw, float2* dst,
+                                                       int L, int log2L, int* tw_log2) {
+    if (!staged_twiddles(L)) {
+        *tw_log2 = kTwiddleLog2;
+        return tw;
+    }
+    *tw_log2 = log2L;
+    const int shift = kTwiddleLog2 - log2L;
+    for (int m0 = threadIdx.x; m0 < L; m0 += kLoadBatch * blockDim.x) {
+        float2 v[kLoadBatch];
+#pragma unroll
+        for (int u = 0; u < kLoadBatch; ++u) {
+            const int m = m0 + u * blockDim.x;
+            if (m < L) v[u] = __ldg(&tw[m << shift]);
+        }
+#pragma unroll
+        for (int u = 0; u < kLoadBatch; ++u) {
+            const int m = m0 + u * blockDim.x;
+            if (m < L) dst[m] = v[u];
+        }
+    }
+    return dst;
+}
+
 // ---------------------------------------------------------------- kernels
 // 1. forward rows: fft_init.comp (fixed point -> float) fused with the row
 // transform. Two rows per complex line.
@@ -162,6 +202,8 @@ __device__ __forceinline__ void fft_rows_forward_body(int block, const T* __rest
     const int pairs = min(pairs_per_cta, MH / 2 - pair0);
     float2* a = sm;
     float2* b = sm + pairs_per_cta * MW;
+    int twl;
+    const float2* tws = stage_twiddles(tw, sm + 2 * pairs_per_cta * MW, MW, ilog2(MW), &twl);
     const int total = pairs * MW;
     for (int t0 = threadIdx.x; t0 < total; t0 += kLoadBatch * blockDim.x) {
         T lo[kLoadBatch], hi[kLoadBatch];
@@ -183,7 +225,7 @@ __device__ __forceinline__ void fft_rows_forward_body(int block, const T* __rest
         }
     }
     __syncthreads();
-    float2* z = line_fft(a, b, MW, ilog2(MW), pairs, MW, false, tw);
+    float2* z = line_fft(a, b, MW, ilog2(MW), pairs, MW, false, tws, twl);
     const int SW = MW / 2 + 1;
     for (int t = threadIdx.x; t < pairs * SW; t += blockDim.x) {
         const int p = t / SW, kx = t - p * SW;
@@ -232,6 +274,8 @@ __device__ __forceinline__ void fft_columns_body(int block, const float2* __rest
     float2* A = sm;
     float2* B = sm + G * MH;
     float2* C = sm + 2 * G * MH;
+    int twl;
+    const float2* tws = stage_twiddles(tw, sm + 4 * G * MH, MH, logH, &twl);
     const int total = ncols * MH;
     for (int t0 = threadIdx.x; t0 < total; t0 += kLoadBatch * blockDim.x) {
         float2 v[kLoadBatch];
@@ -267,7 +311,7 @@ __device__ __forceinline__ void fft_columns_body(int block, const float2* __rest
         }
     }
     __syncthreads();
-    const float2* R = line_fft(A, B, MH, logH, ncols, MH, false, tw);
+    const float2* R = line_fft(A, B, MH, logH, ncols, MH, false, tws, twl);
     for (int t0 = threadIdx.x; t0 < total; t0 += kLoadBatch * blockDim.x) {
         if (!g_fits) {
 #pragma unroll
@@ -292,7 +336,7 @@ __device__ __forceinline__ void fft_columns_body(int block, const float2* __rest
         }
     }
     __syncthreads();
-    const float2* F = line_fft(C, A, MH, logH, 2 * ncols, MH, true, tw);
+    const float2* F = line_fft(C, A, MH, logH, 2 * ncols, MH, true, tws, twl);
     for (int t = threadIdx.x; t < ncols * MH; t += blockDim.x) {
         const int y = t / ncols, c = t - y * ncols;
         const float2 fx = F[c * MH + y], fy = F[(ncols + c) * MH + y];
@@ -396,6 +440,8 @@ __device__ __forceinline__ void fft_rows_inverse_body(int block, const float4* _
     const int SW = MW / 2 + 1;
     float2* a = sm;
     float2* b = sm + rows_per_cta * MW;
+    int twl;
+    const float2* tws = stage_twiddles(tw, sm + 2 * rows_per_cta * MW, MW, ilog2(MW), &twl);
     const int total = rows * SW;
     for (int t0 = threadIdx.x; t0 < total; t0 += kLoadBatch * blockDim.x) {
         float4 v[kLoadBatch];
@@ -424,7 +470,7 @@ __device__ __forceinline__ void fft_rows_inverse_body(int block, const float4* _
         }
     }
     __syncthreads();
-    const float2* z = line_fft(a, b, MW, ilog2(MW), rows, MW, true, tw);
+    const float2* z = line_fft(a, b, MW, ilog2(MW), rows, MW, true, tws, twl);
     for (int t = threadIdx.x; t < rows * MW; t += blockDim.x) {
         const int r = t / MW, x = t - r * MW;
         force[(size_t)(row0 + r) * MW + x] = z[r * MW + x];
@@ -591,7 +637,7 @@ cudaError_t launch_fft_forward_rows(const void* density, int deposit_mode, float
     int pairs_per_cta, threads;
     line_shape(pairs, g.MW, g.MW >= 4096 ? 1 : 4096 / g.MW, &pairs_per_cta, &threads, g.fft_lines);
     const int blocks = (pairs + pairs_per_cta - 1) / pairs_per_cta;
-    const size_t smem = (size_t)2 * pairs_per_cta * g.MW * sizeof(float2);
+    const size_t smem = ((size_t)2 * pairs_per_cta * g.MW + staged_twiddles(g.MW)) * sizeof(float2);
     if (deposit_mode == P3M_DEPOSIT_I64) {
         launch_chained(fft_rows_forward_kernel<long long>, blocks, threads, smem, stream,
             static_cast<const long long*>(density), inv_scale, g.MW, g.MH, pairs_per_cta, twiddles,
@@ -612,7 +658,7 @@ cudaError_t launch_fft_columns(const float2* half, const float2* green, float in
     column_shape(g.MW, g.MH, 4, &G, &threads, g.fft_lines);
     const int SW = g.MW / 2 + 1;
     const int blocks = (SW + G - 1) / G;
-    const size_t smem = (size_t)4 * G * g.MH * sizeof(float2);
+    const size_t smem = ((size_t)4 * G * g.MH + staged_twiddles(g.MH)) * sizeof(float2);
     launch_chained(fft_columns_kernel, blocks, threads, smem, stream, half, green, inv_total, g.MW, g.MH, G,
                                                       twiddles, cols);
     count_launches(1);
@@ -628,7 +674,7 @@ cudaError_t launch_fft_adjoint(const float* cotangent, const float2* green, floa
         int pairs_per_cta, threads;
         line_shape(pairs, g.MW, g.MW >= 4096 ? 1 : 4096 / g.MW, &pairs_per_cta, &threads, g.fft_lines);
         const int blocks = (pairs + pairs_per_cta - 1) / pairs_per_cta;
-        const size_t smem = (size_t)2 * pairs_per_cta * g.MW * sizeof(float2);
+        const size_t smem = ((size_t)2 * pairs_per_cta * g.MW + staged_twiddles(g.MW)) * sizeof(float2);
         fft_rows_forward_kernel<float><<<blocks, threads, smem, stream>>>(
             cotangent, 1.0f, g.MW, 2 * g.MH, pairs_per_cta, twiddles, half2);
         count_launches(1);
@@ -649,7 +695,7 @@ cudaError_t launch_fft_adjoint(const float* cotangent, const float2* green, floa
         int rows_per_cta, threads;
         line_shape(rows, g.MW, g.MW >= 4096 ? 1 : 4096 / g.MW, &rows_per_cta, &threads, g.fft_lines);
         const int blocks = (rows + rows_per_cta - 1) / rows_per_cta;
-        const size_t smem = (size_t)2 * rows_per_cta * g.MW * sizeof(float2);
+        const size_t smem = ((size_t)2 * rows_per_cta * g.MW + staged_twiddles(g.MW)) * sizeof(float2);
         launch_chained(fft_rows_inverse_kernel, blocks, threads, smem, stream, cols, g.MW, rows, rows_per_cta,
                                                                twiddles, mu2);
         count_launches(1);
@@ -673,11 +719,12 @@ void fft_batch_shape(const GridShape& g, int* rows_per_cta, int* cols_per_cta, i
     int col_cap = (128 * 1024) / (4 * g.MH * (int)sizeof(float2));
     if (col_cap > 16) col_cap = 16;
     *rows_per_cta = fill(g.MH / 2, g.MW, row_cap);
-    *rows_smem = (size_t)2 * *rows_per_cta * g.MW * sizeof(float2);
+    // + the staged twiddles of one line
+    *rows_smem = ((size_t)2 * *rows_per_cta * g.MW + staged_twiddles(g.MW)) * sizeof(float2);
     *cols_per_cta = fill(g.MW / 2 + 1, g.MH, col_cap);
-    *cols_smem = (size_t)4 * *cols_per_cta * g.MH * sizeof(float2);
+    *cols_smem = ((size_t)4 * *cols_per_cta * g.MH + staged_twiddles(g.MH)) * sizeof(float2);
     *inv_per_cta = fill(g.MH, g.MW, row_cap);
-    *inv_smem = (size_t)2 * *inv_per_cta * g.MW * sizeof(float2);
+    *inv_smem = ((size_t)2 * *inv_per_cta * g.MW + staged_twiddles(g.MW)) * sizeof(float2);
 }
 
 cudaError_t batched_fft_rows(const FftRowsArgs* a, BatchGrid g, int deposit_mode, size_t smem,
@@ -726,7 +773,7 @@ cudaError_t launch_fft_inverse_rows(const float4* cols, GridShape g, const float
     int rows_per_cta, threads;
     line_shape(g.MH, g.MW, g.MW >= 4096 ? 1 : 4096 / g.MW, &rows_per_cta, &threads, g.fft_lines);
     const int blocks = (g.MH + rows_per_cta - 1) / rows_per_cta;
-    const size_t smem = (size_t)2 * rows_per_cta * g.MW * sizeof(float2);
+    const size_t smem = ((size_t)2 * rows_per_cta * g.MW + staged_twiddles(g.MW)) * sizeof(float2);
     launch_chained(fft_rows_inverse_kernel, blocks, threads, smem, stream, cols, g.MW, g.MH, rows_per_cta,
                                                            twiddles, force);
     count_launches(1);
