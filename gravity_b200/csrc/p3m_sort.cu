@@ -228,14 +228,17 @@ __device__ __forceinline__ uint32_t lookback_exclusive(const uint32_t* status, i
 // (2^bits); a thread handles MAXR / 256 digits where that is above 1. The
 // per-warp digit counts and the tile staged in digit order share one shared
 // region: each key's slot is taken from the counts before the tile is staged.
-template <bool LOOKBACK, int MAXR>
+template <bool LOOKBACK, int MAXR, int THREADS = kSortThreads, int ITEMS = kSortItems>
 __device__ __forceinline__ void radix_scatter_body(
     int tile, const uint32_t* __restrict__ keys_in, const uint32_t* __restrict__ vals_in,
     uint32_t* __restrict__ keys_out, uint32_t* __restrict__ vals_out, int n, int shift, int bits,
     int tiles, const uint32_t* __restrict__ hist_scanned, uint32_t* counter = nullptr,
     uint32_t* status = nullptr, unsigned int* timeouts = nullptr) {
-    constexpr int kPer = MAXR > kSortThreads ? MAXR / kSortThreads : 1;
-    constexpr int kWarpHist = kSortWarps * MAXR;
+    constexpr int kWarps = THREADS / 32;
+    constexpr int kTile = THREADS * ITEMS;
+    static_assert(kTile == kSortTile, "tiles hold kSortTile keys");
+    constexpr int kPer = MAXR > THREADS ? MAXR / THREADS : 1;
+    constexpr int kWarpHist = kWarps * MAXR;
     constexpr int kShared = kWarpHist > 2 * kSortTile ? kWarpHist : 2 * kSortTile;
     __shared__ uint32_t shared[kShared];  // warp counts, then the staged tile
     __shared__ uint32_t tile_start[MAXR];
@@ -255,15 +258,15 @@ __device__ __forceinline__ void radix_scatter_body(
     const uint32_t mask = (uint32_t)radix - 1u;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int tile_base = tile * kSortTile;
-    const int sub_base = tile_base + warp * 32 * kSortItems;
+    const int sub_base = tile_base + warp * 32 * ITEMS;
     uint32_t* my_hist = warp_hist + warp * radix;
 
-    for (int i = threadIdx.x; i < kSortWarps * radix; i += blockDim.x) warp_hist[i] = 0;
+    for (int i = threadIdx.x; i < kWarps * radix; i += blockDim.x) warp_hist[i] = 0;
     __syncthreads();
 
-    uint32_t key[kSortItems], val[kSortItems], rank[kSortItems];
+    uint32_t key[ITEMS], val[ITEMS], rank[ITEMS];
 #pragma unroll
-    for (int j = 0; j < kSortItems; ++j) {
+    for (int j = 0; j < ITEMS; ++j) {
         const int idx = sub_base + j * 32 + lane;
         const bool valid = idx < n;
         key[j] = valid ? keys_in[idx] : 0u;
@@ -289,7 +292,7 @@ __device__ __forceinline__ void radix_scatter_body(
         const int d = threadIdx.x * kPer + q;
         if (d < radix) {
 #pragma unroll
-            for (int w = 0; w < kSortWarps; ++w) {
+            for (int w = 0; w < kWarps; ++w) {
                 const uint32_t t = warp_hist[w * radix + d];
                 warp_hist[w * radix + d] = count[q];
                 count[q] += t;
@@ -339,7 +342,7 @@ __device__ __forceinline__ void radix_scatter_body(
 
     // Each key's slot in the tile staged in digit order.
 #pragma unroll
-    for (int j = 0; j < kSortItems; ++j) {
+    for (int j = 0; j < ITEMS; ++j) {
         const int idx = sub_base + j * 32 + lane;
         if (idx < n) {
             const uint32_t d = (key[j] >> shift) & mask;
@@ -348,7 +351,7 @@ __device__ __forceinline__ void radix_scatter_body(
     }
     __syncthreads();  // the counts are read; their space becomes the staged tile
 #pragma unroll
-    for (int j = 0; j < kSortItems; ++j) {
+    for (int j = 0; j < ITEMS; ++j) {
         const int idx = sub_base + j * 32 + lane;
         if (idx < n) {
             s_keys[rank[j]] = key[j];
@@ -380,15 +383,21 @@ __global__ void __launch_bounds__(kSortThreads) radix_scatter_kernel(
 // One pass of the one-kernel-per-pass sort: `totals` = this pass's digit
 // totals, `status` = this pass's [tiles][kLookbackMaxRadix] look-back words.
 // MAXR: 256 for 8-bit digits, 512 for 9-bit ones.
+// 512 threads of 8 keys each: a sort of a few hundred thousand keys has one
+// tile per SM, and twice the warps hide more of each tile's latency.
+constexpr int kLookbackThreads = 512;
+constexpr int kLookbackItems = kSortTile / kLookbackThreads;
+
 template <int MAXR>
-__global__ void __launch_bounds__(kSortThreads) lookback_scatter_kernel(
+__global__ void __launch_bounds__(kLookbackThreads) lookback_scatter_kernel(
     const uint32_t* __restrict__ keys_in, const uint32_t* __restrict__ vals_in,
     uint32_t* __restrict__ keys_out, uint32_t* __restrict__ vals_out, int n, int shift, int bits,
     int tiles, const uint32_t* __restrict__ totals, uint32_t* counter, uint32_t* status,
     unsigned int* timeouts) {
     grid_dependency_wait();
-    radix_scatter_body<true, MAXR>(0, keys_in, vals_in, keys_out, vals_out, n, shift, bits,
-                                   tiles, totals, counter, status, timeouts);
+    radix_scatter_body<true, MAXR, kLookbackThreads, kLookbackItems>(
+        0, keys_in, vals_in, keys_out, vals_out, n, shift, bits, tiles, totals, counter, status,
+        timeouts);
 }
 
 // Digit totals of every pass in one read of the keys: per-CTA shared counts
@@ -755,11 +764,11 @@ cudaError_t radix_sort_pairs(uint32_t* keys, uint32_t* vals, const SortScratch& 
             uint32_t* counter = s.lookback + kSortMaxPasses * kLookbackMaxRadix + p;
             uint32_t* status = s.lookback + kLookbackHeader + (size_t)p * tiles * kLookbackMaxRadix;
             if (pbits > 8)
-                launch_chained(lookback_scatter_kernel<512>, tiles, kSortThreads, 0, stream,
+                launch_chained(lookback_scatter_kernel<512>, tiles, kLookbackThreads, 0, stream,
                     kin, vin, kout, vout, n, shift, pbits, tiles, totals, counter, status,
                     s.wait_timeouts);
             else
-                launch_chained(lookback_scatter_kernel<256>, tiles, kSortThreads, 0, stream,
+                launch_chained(lookback_scatter_kernel<256>, tiles, kLookbackThreads, 0, stream,
                     kin, vin, kout, vout, n, shift, pbits, tiles, totals, counter, status,
                     s.wait_timeouts);
             count_launches(1);
