@@ -417,8 +417,8 @@ __global__ void __launch_bounds__(kThreads) deposit_heavy_kernel(
 // non-zero cell with one global atomic into the cleared mesh. Deposits that
 // wrap across the mesh edge, or that fall beyond the window's capacity, go
 // straight to global memory.
-constexpr int kChunkEntries = 2048;
-constexpr int kWindowBytes = 96 * 1024;
+constexpr int kChunkEntries = 1024;
+constexpr int kWindowBytes = 48 * 1024;
 
 template <typename T>
 __device__ __forceinline__ void deposit_chunks_body(
