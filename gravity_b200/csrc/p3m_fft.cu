@@ -85,26 +85,37 @@ __device__ __forceinline__ void dft<8>(float2 (&v)[8], bool inverse) {
     }
 }
 
-// One Stockham pass of radix R over `lines` lines of length L (line pitch
-// `pitch`), src -> dst. Ns = product of earlier radices; log2(Ns*R) <= 12.
+// Position of point i of a line in shared memory: bits 0-3 XOR bits 4-7.
+// The passes write point (j - k) * R + k + r * Ns from lane j, strides that
+// would put a warp's stores on a few banks; the swizzle spreads every pass's
+// reads and writes over all banks. It permutes the points of each aligned
+// 256-point block (a line of 16 points or fewer is unchanged), so a line of
+// L = 2^n points stays in [0, L). Every access to a line buffer goes
+// through it.
+__device__ __forceinline__ int swz(int i) { return i ^ ((i >> 4) & 15); }
+
+// One Stockham pass of radix R over `lines` lines of length L = 2^log2L (line
+// pitch `pitch`), src -> dst. Ns = product of earlier radices; log2(Ns*R) <= 12.
 template <int R>
 __device__ __forceinline__ void stockham_pass(const float2* __restrict__ src, float2* __restrict__ dst,
-                                              int L, int lines, int pitch, int Ns, int log_ns_r,
+                                              int log2L, int lines, int pitch, int Ns, int log_ns_r,
                                               bool inverse, const float2* __restrict__ tw,
                                               int tw_log2) {
-    const int per_line = L / R;
-    const int total = lines * per_line;
+    constexpr int kLog2R = R == 8 ? 3 : (R == 4 ? 2 : 1);
+    const int log_per_line = log2L - kLog2R;
+    const int per_line = 1 << log_per_line;
+    const int total = lines << log_per_line;
     const int shift = tw_log2 - log_ns_r;
     for (int t = threadIdx.x; t < total; t += blockDim.x) {
-        const int line = t / per_line;
-        const int j = t - line * per_line;
+        const int line = t >> log_per_line;
+        const int j = t & (per_line - 1);
         const float2* s = src + line * pitch;
         float2* d = dst + line * pitch;
         const int k = j & (Ns - 1);
         float2 v[R];
 #pragma unroll
         for (int r = 0; r < R; ++r) {
-            float2 x = s[j + r * per_line];
+            float2 x = s[swz(j + r * per_line)];
             if (r > 0 && k > 0) {
                 float2 w = tw[(k * r) << shift];
                 if (inverse) w.y = -w.y;
@@ -115,7 +126,7 @@ __device__ __forceinline__ void stockham_pass(const float2* __restrict__ src, fl
         dft<R>(v, inverse);
         const int out = (j - k) * R + k;
 #pragma unroll
-        for (int r = 0; r < R; ++r) d[out + r * Ns] = v[r];
+        for (int r = 0; r < R; ++r) d[swz(out + r * Ns)] = v[r];
     }
 }
 
@@ -130,13 +141,13 @@ __device__ float2* line_fft(float2* a, float2* b, int L, int log2L, int lines, i
     while (Ns < L) {
         const int remaining = log2L - logNs;
         if (remaining >= 3) {
-            stockham_pass<8>(a, b, L, lines, pitch, Ns, logNs + 3, inverse, tw, tw_log2);
+            stockham_pass<8>(a, b, log2L, lines, pitch, Ns, logNs + 3, inverse, tw, tw_log2);
             Ns <<= 3; logNs += 3;
         } else if (remaining == 2) {
-            stockham_pass<4>(a, b, L, lines, pitch, Ns, logNs + 2, inverse, tw, tw_log2);
+            stockham_pass<4>(a, b, log2L, lines, pitch, Ns, logNs + 2, inverse, tw, tw_log2);
             Ns <<= 2; logNs += 2;
         } else {
-            stockham_pass<2>(a, b, L, lines, pitch, Ns, logNs + 1, inverse, tw, tw_log2);
+            stockham_pass<2>(a, b, log2L, lines, pitch, Ns, logNs + 1, inverse, tw, tw_log2);
             Ns <<= 1; logNs += 1;
         }
         __syncthreads();
@@ -220,8 +231,10 @@ __device__ __forceinline__ void fft_rows_forward_body(int block, const T* __rest
 #pragma unroll
         for (int u = 0; u < kLoadBatch; ++u) {
             const int t = t0 + u * blockDim.x;
-            if (t < total)
-                a[t] = make_float2((float)lo[u] * inv_scale, (float)hi[u] * inv_scale);
+            if (t < total) {
+                const int p = t / MW, x = t - p * MW;
+                a[p * MW + swz(x)] = make_float2((float)lo[u] * inv_scale, (float)hi[u] * inv_scale);
+            }
         }
     }
     __syncthreads();
@@ -229,8 +242,8 @@ __device__ __forceinline__ void fft_rows_forward_body(int block, const T* __rest
     const int SW = MW / 2 + 1;
     for (int t = threadIdx.x; t < pairs * SW; t += blockDim.x) {
         const int p = t / SW, kx = t - p * SW;
-        const float2 zk = z[p * MW + kx];
-        const float2 zn = z[p * MW + ((MW - kx) & (MW - 1))];
+        const float2 zk = z[p * MW + swz(kx)];
+        const float2 zn = z[p * MW + swz((MW - kx) & (MW - 1))];
         const float2 A = make_float2(0.5f * (zk.x + zn.x), 0.5f * (zk.y - zn.y));
         const float2 B = make_float2(0.5f * (zk.y + zn.y), 0.5f * (zn.x - zk.x));
         const size_t row = (size_t)(pair0 + p) * 2;
@@ -292,7 +305,7 @@ __device__ __forceinline__ void fft_columns_body(int block, const float2* __rest
             const int t = t0 + u * blockDim.x;
             if (t < total) {
                 const int y = t / ncols, c = t - y * ncols;
-                A[c * MH + y] = v[u];
+                A[c * MH + swz(y)] = v[u];
             }
         }
     }
@@ -328,10 +341,10 @@ __device__ __forceinline__ void fft_columns_body(int block, const float2* __rest
             const int t = t0 + u * blockDim.x;
             if (t < total) {
                 const int y = t / ncols, c = t - y * ncols;
-                const float2 rho = R[c * MH + y];
+                const float2 rho = R[c * MH + swz(y)];
                 const float gx = gv[u].x * inv_total, gy = gv[u].y * inv_total;
-                C[c * MH + y] = make_float2(-rho.y * gx, rho.x * gx);
-                C[(ncols + c) * MH + y] = make_float2(-rho.y * gy, rho.x * gy);
+                C[c * MH + swz(y)] = make_float2(-rho.y * gx, rho.x * gx);
+                C[(ncols + c) * MH + swz(y)] = make_float2(-rho.y * gy, rho.x * gy);
             }
         }
     }
@@ -339,7 +352,7 @@ __device__ __forceinline__ void fft_columns_body(int block, const float2* __rest
     const float2* F = line_fft(C, A, MH, logH, 2 * ncols, MH, true, tws, twl);
     for (int t = threadIdx.x; t < ncols * MH; t += blockDim.x) {
         const int y = t / ncols, c = t - y * ncols;
-        const float2 fx = F[c * MH + y], fy = F[(ncols + c) * MH + y];
+        const float2 fx = F[c * MH + swz(y)], fy = F[(ncols + c) * MH + swz(y)];
         cols[(size_t)y * SW + kx0 + c] = make_float4(fx.x, fx.y, fy.x, fy.y);
     }
 }
@@ -386,23 +399,23 @@ __global__ void __launch_bounds__(256) fft_columns_adjoint_kernel(const float2* 
     for (int t = threadIdx.x; t < 2 * ncols * MH; t += blockDim.x) {
         const int row = t / ncols, c = t - row * ncols;  // row = 2y + component
         const int y = row >> 1, comp = row & 1;
-        A[(comp * ncols + c) * MH + y] = half[(size_t)row * SW + kx0 + c];
+        A[(comp * ncols + c) * MH + swz(y)] = half[(size_t)row * SW + kx0 + c];
     }
     __syncthreads();
     float2* R = line_fft(A, B, MH, logH, 2 * ncols, MH, false, tw);
     float2* C = R == A ? B : A;
     for (int t = threadIdx.x; t < ncols * MH; t += blockDim.x) {
         const int y = t / ncols, c = t - y * ncols;
-        const float2 X = R[c * MH + y], Y = R[(ncols + c) * MH + y];
+        const float2 X = R[c * MH + swz(y)], Y = R[(ncols + c) * MH + swz(y)];
         const float2 g = __ldg(&green[(size_t)y * SW + kx0 + c]);
         const float sx = X.x * g.x + Y.x * g.y, sy = X.y * g.x + Y.y * g.y;
-        C[c * MH + y] = make_float2(sy * inv_total, -sx * inv_total);  // -i (gx X + gy Y) / M
+        C[c * MH + swz(y)] = make_float2(sy * inv_total, -sx * inv_total);  // -i (gx X + gy Y) / M
     }
     __syncthreads();
     const float2* F = line_fft(C, R, MH, logH, ncols, MH, true, tw);
     for (int t = threadIdx.x; t < ncols * MH; t += blockDim.x) {
         const int y = t / ncols, c = t - y * ncols;
-        cols[((size_t)(y >> 1) * SW + kx0 + c) * 2 + (y & 1)] = F[c * MH + y];
+        cols[((size_t)(y >> 1) * SW + kx0 + c) * 2 + (y & 1)] = F[c * MH + swz(y)];
     }
 }
 
@@ -418,13 +431,13 @@ __global__ void __launch_bounds__(256) fft_columns_forward_kernel(float2* half, 
     float2* B = sm + G * MH;
     for (int t = threadIdx.x; t < ncols * MH; t += blockDim.x) {
         const int y = t / ncols, c = t - y * ncols;
-        A[c * MH + y] = half[(size_t)y * SW + kx0 + c];
+        A[c * MH + swz(y)] = half[(size_t)y * SW + kx0 + c];
     }
     __syncthreads();
     const float2* R = line_fft(A, B, MH, ilog2(MH), ncols, MH, false, tw);
     for (int t = threadIdx.x; t < ncols * MH; t += blockDim.x) {
         const int y = t / ncols, c = t - y * ncols;
-        half[(size_t)y * SW + kx0 + c] = R[c * MH + y];
+        half[(size_t)y * SW + kx0 + c] = R[c * MH + swz(y)];
     }
 }
 
@@ -461,10 +474,10 @@ __device__ __forceinline__ void fft_rows_inverse_body(int block, const float4* _
                 const float4 q = v[u];
                 if (kx == 0 || kx == MW / 2) {
                     // DC and Nyquist bins of a real row are real.
-                    a[r * MW + kx] = make_float2(q.x, q.z);
+                    a[r * MW + swz(kx)] = make_float2(q.x, q.z);
                 } else {
-                    a[r * MW + kx] = make_float2(q.x - q.w, q.y + q.z);
-                    a[r * MW + (MW - kx)] = make_float2(q.x + q.w, q.z - q.y);
+                    a[r * MW + swz(kx)] = make_float2(q.x - q.w, q.y + q.z);
+                    a[r * MW + swz(MW - kx)] = make_float2(q.x + q.w, q.z - q.y);
                 }
             }
         }
@@ -473,7 +486,7 @@ __device__ __forceinline__ void fft_rows_inverse_body(int block, const float4* _
     const float2* z = line_fft(a, b, MW, ilog2(MW), rows, MW, true, tws, twl);
     for (int t = threadIdx.x; t < rows * MW; t += blockDim.x) {
         const int r = t / MW, x = t - r * MW;
-        force[(size_t)(row0 + r) * MW + x] = z[r * MW + x];
+        force[(size_t)(row0 + r) * MW + x] = z[r * MW + swz(x)];
     }
 }
 
