@@ -260,13 +260,15 @@ int check_n(p3m_ctx* ctx, int n) {
 }
 
 // Cell lists from keys already written in descending ID order.
-int lists_from_keys(p3m_ctx* ctx, int n) {
+// totals_ready: radix_sort_prepare ran and the keys' producer (the drift)
+// added their digit totals.
+int lists_from_keys(p3m_ctx* ctx, int n, bool totals_ready = false) {
     StageScope scope(ctx, P3M_STAGE_CELL_LISTS);
     const long long P = (long long)phys_cells(ctx);
     uint32_t* sk = ctx->keys;
     uint32_t* sv = ctx->vals;
     P3M_CUDA(ctx, p3m::radix_sort_pairs(ctx->keys, ctx->vals, ctx->sort, n, bits_for(P),
-                                        ctx->stream, &sk, &sv));
+                                        ctx->stream, &sk, &sv, totals_ready));
     ctx->sorted_keys = sk;
     ctx->sorted_ids = sv;
     P3M_CUDA(ctx, cudaMemsetAsync(ctx->cell_count, 0, P * sizeof(int), ctx->stream));
@@ -369,12 +371,15 @@ int apply_kick(p3m_ctx* ctx, int n, int initial, bool with_short_range = true) {
 int sort_bodies(p3m_ctx* ctx, int n) {
     if (n <= 0) return P3M_OK;
     StageScope scope(ctx, P3M_STAGE_SPATIAL_SORT);
+    const int key_bits = ctx->sort_wbits + ctx->sort_hbits;
+    p3m::SortTotals totals;  // the key kernel adds the sort's digit totals
+    P3M_CUDA(ctx, p3m::radix_sort_prepare(ctx->sort, n, key_bits, ctx->stream, &totals));
     P3M_CUDA(ctx, p3m::launch_morton_keys(ctx->bodies, n, ctx->sort_wbits, ctx->sort_hbits,
-                                          ctx->keys, ctx->vals, ctx->stream));
+                                          ctx->keys, ctx->vals, ctx->stream, totals));
     uint32_t* sk = ctx->keys;
     uint32_t* sv = ctx->vals;
-    P3M_CUDA(ctx, p3m::radix_sort_pairs(ctx->keys, ctx->vals, ctx->sort, n,
-                                        ctx->sort_wbits + ctx->sort_hbits, ctx->stream, &sk, &sv));
+    P3M_CUDA(ctx, p3m::radix_sort_pairs(ctx->keys, ctx->vals, ctx->sort, n, key_bits, ctx->stream,
+                                        &sk, &sv, totals.totals != nullptr));
     P3M_CUDA(ctx, p3m::launch_permute(sv, n, ctx->bodies, ctx->accel, ctx->materials,
                                       ctx->bodies_alt, ctx->accel_alt, ctx->materials_alt,
                                       ctx->destinations, ctx->stream));
@@ -407,14 +412,18 @@ int enqueue_step(p3m_ctx* ctx, int n, bool do_sort) {
     // writes the home-cell keys.
     const float dt = ctx->cfg.time_step;
     const float drift_dt = dt / (float)ctx->cfg.drift_substeps;
+    p3m::SortTotals totals;  // the drift adds the cell sort's digit totals
     {
         StageScope scope(ctx, P3M_STAGE_DRIFT);
+        if (ctx->mutual)
+            P3M_CUDA(ctx, p3m::radix_sort_prepare(ctx->sort, n, bits_for(phys_cells(ctx)),
+                                                  ctx->stream, &totals));
         P3M_CUDA(ctx, p3m::launch_drift(ctx->bodies, ctx->accel, n, 0.5f * dt, drift_dt,
                                         ctx->cfg.drift_substeps, ctx->grid, ctx->keys, ctx->vals,
-                                        ctx->status, ctx->stream));
+                                        ctx->status, ctx->stream, totals));
     }
     if (ctx->mutual) {
-        int st = lists_from_keys(ctx, n);
+        int st = lists_from_keys(ctx, n, totals.totals != nullptr);
         if (st != P3M_OK) return st;
         // The short range reads only the lists: outside the profiler it runs
         // on the side stream beside the deposit and FFT.

@@ -15,14 +15,15 @@ namespace {
 
 __device__ __forceinline__ float fractf(float v) { return v - floorf(v); }
 
-__device__ __forceinline__ void drift_body(int block, float4* __restrict__ bodies,
-                                           const float2* __restrict__ accel, int n,
-                                           float half_kick, float drift_dt, int substeps,
-                                           int bounded, int W, int H, uint32_t* __restrict__ keys,
-                                           uint32_t* __restrict__ vals,
-                                           unsigned int* __restrict__ nonfinite) {
-    const int id = block * blockDim.x + threadIdx.x;
-    if (id >= n) return;
+// Drifts body `id` (when id < n) and writes its cell key; returns the key.
+__device__ __forceinline__ uint32_t drift_one(int id, float4* __restrict__ bodies,
+                                              const float2* __restrict__ accel, int n,
+                                              float half_kick, float drift_dt, int substeps,
+                                              int bounded, int W, int H,
+                                              uint32_t* __restrict__ keys,
+                                              uint32_t* __restrict__ vals,
+                                              unsigned int* __restrict__ nonfinite) {
+    if (id >= n) return 0u;
     float4 b = bodies[id];
     const float2 a = accel[id];
     for (int s = 0; s < substeps; ++s) {
@@ -44,22 +45,42 @@ __device__ __forceinline__ void drift_body(int block, float4* __restrict__ bodie
     bodies[id] = b;
     if (nonfinite && !(isfinite(b.x) && isfinite(b.y) && isfinite(b.z) && isfinite(b.w)))
         atomicAdd(nonfinite, 1u);
+    uint32_t key = 0u;
     if (keys) {
         const int hx = wrap_index(float_to_int(floorf(b.x * (float)W)), W);
         const int hy = wrap_index(float_to_int(floorf(b.y * (float)H)), H);
         const int slot = n - 1 - id;  // descending ID order for the cell sort
-        keys[slot] = (uint32_t)hx + (uint32_t)hy * (uint32_t)W;
+        key = (uint32_t)hx + (uint32_t)hy * (uint32_t)W;
+        keys[slot] = key;
         vals[slot] = (uint32_t)id;
     }
+    return key;
 }
 
+__device__ __forceinline__ void drift_body(int block, float4* __restrict__ bodies,
+                                           const float2* __restrict__ accel, int n,
+                                           float half_kick, float drift_dt, int substeps,
+                                           int bounded, int W, int H, uint32_t* __restrict__ keys,
+                                           uint32_t* __restrict__ vals,
+                                           unsigned int* __restrict__ nonfinite) {
+    drift_one(block * blockDim.x + threadIdx.x, bodies, accel, n, half_kick, drift_dt, substeps,
+              bounded, W, H, keys, vals, nonfinite);
+}
+
+// The drift, and (totals.totals set) the digit totals of the cell keys for
+// the look-back sort that follows.
 __global__ void drift_kernel(float4* __restrict__ bodies, const float2* __restrict__ accel, int n,
                              float half_kick, float drift_dt, int substeps, int bounded, int W,
                              int H, uint32_t* __restrict__ keys, uint32_t* __restrict__ vals,
-                             unsigned int* __restrict__ nonfinite) {
+                             unsigned int* __restrict__ nonfinite, SortTotals totals) {
     grid_dependency_wait();
-    drift_body(blockIdx.x, bodies, accel, n, half_kick, drift_dt, substeps, bounded, W, H, keys,
-               vals, nonfinite);
+    const int id = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t key = drift_one(id, bodies, accel, n, half_kick, drift_dt, substeps, bounded,
+                                   W, H, keys, vals, nonfinite);
+    if (totals.totals && keys) {
+        __shared__ uint32_t sh[kSortMaxPasses * kLookbackMaxRadix];
+        add_digit_totals(totals, id < n, key, sh);
+    }
 }
 
 __global__ void drift_batched_kernel(const DriftArgs* __restrict__ args, const int* __restrict__ first,
@@ -81,11 +102,10 @@ cudaError_t batched_drift(const DriftArgs* a, BatchGrid g, cudaStream_t s) {
 
 cudaError_t launch_drift(float4* bodies, const float2* accel, int n, float half_kick, float drift_dt,
                          int substeps, GridShape g, uint32_t* keys, uint32_t* vals,
-                         unsigned int* nonfinite, cudaStream_t stream) {
+                         unsigned int* nonfinite, cudaStream_t stream, SortTotals totals) {
     if (n <= 0) return cudaSuccess;
-    launch_chained(drift_kernel, (n + 255) / 256, 256, 0, stream, bodies, accel, n, half_kick, drift_dt,
-                                                      substeps, g.bounded, g.W, g.H, keys, vals,
-                                                      nonfinite);
+    launch_chained(drift_kernel, (n + 255) / 256, 256, 0, stream, bodies, accel, n, half_kick,
+                   drift_dt, substeps, g.bounded, g.W, g.H, keys, vals, nonfinite, totals);
     count_launches(1);
     return cudaGetLastError();
 }

@@ -92,13 +92,54 @@ size_t sort_hist_entries(int capacity);
 size_t sort_block_sum_entries(int capacity);
 size_t sort_lookback_words(int capacity);
 
+// Digit totals of a look-back sort, added by the kernel that writes its keys
+// (the drift for the cell sort, the Morton-key kernel for the reorder)
+// instead of by a separate pass over the keys. totals == nullptr: the sort
+// counts them itself.
+struct SortTotals {
+    uint32_t* totals = nullptr;  // [pass][kLookbackMaxRadix] digit counts, cleared
+    int passes = 0, bits = 0, key_bits = 0;
+};
+constexpr int kLookbackMaxRadix = 512;  // digits of up to 9 bits
+
+// Clears the look-back words of a sort of n keys over key_bits bits (one
+// memset) and says where the keys' producer adds their digit totals. Leaves
+// out->totals null (nothing issued; the sort counts its digits itself) from
+// 2^21 keys, and when that sort does not take the look-back form.
+cudaError_t radix_sort_prepare(const SortScratch& s, int n, int key_bits, cudaStream_t stream,
+                               SortTotals* out);
+
+// Adds this thread's key (when `valid`) to the digit totals: counts per pass
+// in shared memory (warp-aggregated), then one global atomic per CTA and
+// non-zero digit. Every thread of the CTA calls it; `sh` holds
+// kSortMaxPasses * kLookbackMaxRadix words.
+__device__ __forceinline__ void add_digit_totals(const SortTotals& st, bool valid, uint32_t key,
+                                                 uint32_t* sh) {
+    const int bins = st.passes * kLookbackMaxRadix;
+    for (int i = threadIdx.x; i < bins; i += blockDim.x) sh[i] = 0u;
+    __syncthreads();
+    for (int p = 0; p < st.passes; ++p) {
+        const int pb = min(st.bits, st.key_bits - p * st.bits);
+        const uint32_t d = valid ? (key >> (p * st.bits)) & ((1u << pb) - 1u) : 0xffffffffu;
+        const unsigned peers = __match_any_sync(0xffffffffu, d);
+        const int lane = threadIdx.x & 31;
+        if (valid && lane == __ffs(peers) - 1)
+            atomicAdd(&sh[p * kLookbackMaxRadix + d], (uint32_t)__popc(peers));
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < bins; i += blockDim.x)
+        if (sh[i]) atomicAdd(&st.totals[i], sh[i]);
+}
+
 // Stable LSD radix sort of (keys, vals) on bits [0, key_bits). Passes
 // alternate between the inputs and the scratch pair; *out_keys/*out_vals
 // name the pair that holds the result. Launches only; no allocation, no
 // synchronisation.
+// totals_ready: radix_sort_prepare ran for this sort and the keys' producer
+// added the digit totals.
 cudaError_t radix_sort_pairs(uint32_t* keys, uint32_t* vals, const SortScratch& s, int n,
                              int key_bits, cudaStream_t stream, uint32_t** out_keys,
-                             uint32_t** out_vals);
+                             uint32_t** out_vals, bool totals_ready = false);
 
 // Exclusive scan of n uint32 in place (n <= 4096 * 4096).
 cudaError_t exclusive_scan_u32(uint32_t* data, int n, uint32_t* block_sums,
@@ -114,15 +155,19 @@ struct GridShape {
 
 // Half kick + drift substeps (collision_build.comp:40-51), then the home-cell
 // key of each body, written in descending ID order for the cell sort.
+// With totals.totals set (radix_sort_prepare), also adds the keys' digit
+// totals for the look-back cell sort.
 cudaError_t launch_drift(float4* bodies, const float2* accel, int n, float half_kick,
                          float drift_dt, int substeps, GridShape g, uint32_t* keys,
-                         uint32_t* vals, unsigned int* nonfinite, cudaStream_t stream);
+                         uint32_t* vals, unsigned int* nonfinite, cudaStream_t stream,
+                         SortTotals totals = SortTotals());
 // Home-cell keys of the current positions (no drift).
 cudaError_t launch_cell_keys(const float4* bodies, int n, GridShape g, uint32_t* keys,
                              uint32_t* vals, cudaStream_t stream);
 // Morton tile keys (spatial_sort_key.glsl), ascending ID order.
 cudaError_t launch_morton_keys(const float4* bodies, int n, int wbits, int hbits,
-                               uint32_t* keys, uint32_t* vals, cudaStream_t stream);
+                               uint32_t* keys, uint32_t* vals, cudaStream_t stream,
+                               SortTotals totals = SortTotals());
 // Permutation of the Morton reorder (spatial_sort_scatter / _materials.comp).
 cudaError_t launch_permute(const uint32_t* order, int n, const float4* bodies, const float2* accel,
                            const float4* materials, float4* bodies_out, float2* accel_out,

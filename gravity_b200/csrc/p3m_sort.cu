@@ -164,8 +164,6 @@ constexpr uint32_t kLookbackInclusive = 2u << 30;
 constexpr uint32_t kLookbackValue = (1u << 30) - 1u;
 constexpr int kLookbackWindow = 16;    // predecessors read per round trip
 constexpr int kLookbackSpins = 200000; // polls of one word before giving up
-// Digits of the look-back sort: 8 bits, or 9 where that saves a pass.
-constexpr int kLookbackMaxRadix = 512;
 constexpr int kLookbackHeader = kSortMaxPasses * kLookbackMaxRadix + 32;  // totals + counters
 
 __device__ __forceinline__ uint32_t load_relaxed(const uint32_t* p) {
@@ -500,24 +498,42 @@ __device__ __forceinline__ uint32_t tile_coord(float p, int size) {
     return (uint32_t)min(max(t, 0), size - 1);
 }
 
+__device__ __forceinline__ uint32_t morton_key(float4 b, int wbits, int hbits) {
+    const uint32_t tx = tile_coord(b.x, 1 << wbits), ty = tile_coord(b.y, 1 << hbits);
+    const int common = min(wbits, hbits);
+    const uint32_t low = (1u << common) - 1u;
+    const uint32_t morton = spread_bits(tx & low) | (spread_bits(ty & low) << 1);
+    return morton | (((tx | ty) >> common) << (2 * common));
+}
+
 __device__ __forceinline__ void morton_keys_body(int block, const float4* __restrict__ bodies, int n,
                                                  int wbits, int hbits, uint32_t* keys,
                                                  uint32_t* vals) {
     const int id = block * blockDim.x + threadIdx.x;
     if (id >= n) return;
-    const float4 b = bodies[id];
-    const uint32_t tx = tile_coord(b.x, 1 << wbits), ty = tile_coord(b.y, 1 << hbits);
-    const int common = min(wbits, hbits);
-    const uint32_t low = (1u << common) - 1u;
-    const uint32_t morton = spread_bits(tx & low) | (spread_bits(ty & low) << 1);
-    keys[id] = morton | (((tx | ty) >> common) << (2 * common));
+    keys[id] = morton_key(bodies[id], wbits, hbits);
     vals[id] = (uint32_t)id;
 }
 
+// The Morton keys, and (totals.totals set) their digit totals for the
+// look-back sort that follows.
 __global__ void morton_keys_kernel(const float4* __restrict__ bodies, int n, int wbits, int hbits,
-                                   uint32_t* keys, uint32_t* vals) {
+                                   uint32_t* keys, uint32_t* vals, SortTotals totals) {
     grid_dependency_wait();
-    morton_keys_body(blockIdx.x, bodies, n, wbits, hbits, keys, vals);
+    if (!totals.totals) {
+        morton_keys_body(blockIdx.x, bodies, n, wbits, hbits, keys, vals);
+        return;
+    }
+    __shared__ uint32_t sh[kSortMaxPasses * kLookbackMaxRadix];
+    const int id = blockIdx.x * blockDim.x + threadIdx.x;
+    const bool valid = id < n;
+    uint32_t key = 0;
+    if (valid) {
+        key = morton_key(bodies[id], wbits, hbits);
+        keys[id] = key;
+        vals[id] = (uint32_t)id;
+    }
+    add_digit_totals(totals, valid, key, sh);
 }
 
 // spatial_sort_scatter.comp:14-28 and spatial_sort_materials.comp:9-13: a
@@ -725,9 +741,51 @@ cudaError_t exclusive_scan_u32(uint32_t* data, int n, uint32_t* block_sums, cuda
     return cudaGetLastError();
 }
 
+// Passes and digit width of the look-back form, or false when a sort of n
+// keys does not take it. With no per-pass histogram or scan to pay for,
+// 9-bit digits are used where they save a pass (17 or 18 key bits: 2 passes
+// instead of 3).
+static bool lookback_plan(const SortScratch& s, int n, int key_bits, int* passes, int* bits) {
+    int p = (key_bits + 7) / 8;
+    if (!s.lookback || !s.wait_timeouts || n <= 1 || n >= (1 << 30) || key_bits <= 0 ||
+        p > kSortMaxPasses)
+        return false;
+    if (p > 1 && (key_bits + 8) / 9 < p) p = (key_bits + 8) / 9;
+    *passes = p;
+    *bits = (key_bits + p - 1) / p;
+    return true;
+}
+
+static size_t lookback_words(int n, int passes) {
+    return (size_t)kLookbackHeader + (size_t)passes * blocks_for(n, kSortTile) * kLookbackMaxRadix;
+}
+
+// Below this many keys the producer adds the digit totals: the separate
+// totals kernel's launch is then the larger cost. Above it, a producer CTA's
+// per-pass bins and the global atomics on shared high digits cost more than
+// one streaming read of the keys.
+constexpr int kProducerTotalsMaxKeys = 1 << 21;
+
+cudaError_t radix_sort_prepare(const SortScratch& s, int n, int key_bits, cudaStream_t stream,
+                               SortTotals* out) {
+    *out = SortTotals();
+    int passes, bits;
+    if (n > s.capacity || n >= kProducerTotalsMaxKeys ||
+        !lookback_plan(s, n, key_bits, &passes, &bits))
+        return cudaSuccess;
+    cudaError_t e =
+        cudaMemsetAsync(s.lookback, 0, lookback_words(n, passes) * sizeof(uint32_t), stream);
+    if (e != cudaSuccess) return e;
+    out->totals = s.lookback;
+    out->passes = passes;
+    out->bits = bits;
+    out->key_bits = key_bits;
+    return cudaSuccess;
+}
+
 cudaError_t radix_sort_pairs(uint32_t* keys, uint32_t* vals, const SortScratch& s, int n,
                              int key_bits, cudaStream_t stream, uint32_t** out_keys,
-                             uint32_t** out_vals) {
+                             uint32_t** out_vals, bool totals_ready) {
     *out_keys = keys;
     *out_vals = vals;
     if (n <= 1 || key_bits <= 0) return cudaSuccess;
@@ -739,24 +797,20 @@ cudaError_t radix_sort_pairs(uint32_t* keys, uint32_t* vals, const SortScratch& 
     uint32_t* vin = vals;
     uint32_t* kout = s.keys_alt;
     uint32_t* vout = s.vals_alt;
-    if (s.lookback && s.wait_timeouts && n < (1 << 30) && passes <= kSortMaxPasses) {
-        // One kernel per pass: the digit totals of all passes first, then each
-        // pass's tiles find their offsets by look-back. With no per-pass
-        // histogram or scan to pay for, 9-bit digits are used where they save
-        // a pass (17 or 18 key bits: 2 passes instead of 3).
-        int lb_passes = passes, lb_bits = bits;
-        if (passes > 1 && (key_bits + 8) / 9 < passes) {
-            lb_passes = (key_bits + 8) / 9;
-            lb_bits = (key_bits + lb_passes - 1) / lb_passes;
+    int lb_passes, lb_bits;
+    if (lookback_plan(s, n, key_bits, &lb_passes, &lb_bits)) {
+        // One kernel per pass: the digit totals of all passes first (here, or
+        // by the keys' producer after radix_sort_prepare), then each pass's
+        // tiles find their offsets by look-back.
+        if (!totals_ready) {
+            cudaError_t e = cudaMemsetAsync(s.lookback, 0,
+                                            lookback_words(n, lb_passes) * sizeof(uint32_t), stream);
+            if (e != cudaSuccess) return e;
+            const int tblocks = min(tiles, 4 * 148);
+            launch_chained(lookback_totals_kernel, tblocks, kSortThreads, 0, stream, kin, n,
+                           lb_passes, lb_bits, key_bits, s.lookback);
+            count_launches(1);
         }
-        const size_t words =
-            (size_t)kLookbackHeader + (size_t)lb_passes * tiles * kLookbackMaxRadix;
-        cudaError_t e = cudaMemsetAsync(s.lookback, 0, words * sizeof(uint32_t), stream);
-        if (e != cudaSuccess) return e;
-        const int tblocks = min(tiles, 4 * 148);
-        launch_chained(lookback_totals_kernel, tblocks, kSortThreads, 0, stream, kin, n, lb_passes, lb_bits,
-                                                                     key_bits, s.lookback);
-        count_launches(1);
         for (int p = 0; p < lb_passes; ++p) {
             const int shift = p * lb_bits;
             const int pbits = min(lb_bits, key_bits - shift);
@@ -805,9 +859,10 @@ cudaError_t launch_cell_keys(const float4* bodies, int n, GridShape g, uint32_t*
 }
 
 cudaError_t launch_morton_keys(const float4* bodies, int n, int wbits, int hbits, uint32_t* keys,
-                               uint32_t* vals, cudaStream_t stream) {
+                               uint32_t* vals, cudaStream_t stream, SortTotals totals) {
     if (n <= 0) return cudaSuccess;
-    launch_chained(morton_keys_kernel, blocks_for(n, 256), 256, 0, stream, bodies, n, wbits, hbits, keys, vals);
+    launch_chained(morton_keys_kernel, blocks_for(n, 256), 256, 0, stream, bodies, n, wbits, hbits,
+                   keys, vals, totals);
     count_launches(1);
     return cudaGetLastError();
 }
