@@ -214,7 +214,8 @@ __device__ __forceinline__ void fft_rows_forward_body(int block, const T* __rest
     float2* a = sm;
     float2* b = sm + pairs_per_cta * MW;
     int twl;
-    const float2* tws = stage_twiddles(tw, sm + 2 * pairs_per_cta * MW, MW, ilog2(MW), &twl);
+    const int logW = ilog2(MW);
+    const float2* tws = stage_twiddles(tw, sm + 2 * pairs_per_cta * MW, MW, logW, &twl);
     const int total = pairs * MW;
     for (int t0 = threadIdx.x; t0 < total; t0 += kLoadBatch * blockDim.x) {
         T lo[kLoadBatch], hi[kLoadBatch];
@@ -222,7 +223,7 @@ __device__ __forceinline__ void fft_rows_forward_body(int block, const T* __rest
         for (int u = 0; u < kLoadBatch; ++u) {
             const int t = t0 + u * blockDim.x;
             if (t < total) {
-                const int p = t / MW, x = t - p * MW;
+                const int p = t >> logW, x = t & (MW - 1);
                 const size_t row = (size_t)(pair0 + p) * 2;
                 lo[u] = density[row * MW + x];
                 hi[u] = density[(row + 1) * MW + x];
@@ -232,23 +233,24 @@ __device__ __forceinline__ void fft_rows_forward_body(int block, const T* __rest
         for (int u = 0; u < kLoadBatch; ++u) {
             const int t = t0 + u * blockDim.x;
             if (t < total) {
-                const int p = t / MW, x = t - p * MW;
+                const int p = t >> logW, x = t & (MW - 1);
                 a[p * MW + swz(x)] = make_float2((float)lo[u] * inv_scale, (float)hi[u] * inv_scale);
             }
         }
     }
     __syncthreads();
-    float2* z = line_fft(a, b, MW, ilog2(MW), pairs, MW, false, tws, twl);
+    float2* z = line_fft(a, b, MW, logW, pairs, MW, false, tws, twl);
     const int SW = MW / 2 + 1;
-    for (int t = threadIdx.x; t < pairs * SW; t += blockDim.x) {
-        const int p = t / SW, kx = t - p * SW;
-        const float2 zk = z[p * MW + swz(kx)];
-        const float2 zn = z[p * MW + swz((MW - kx) & (MW - 1))];
-        const float2 A = make_float2(0.5f * (zk.x + zn.x), 0.5f * (zk.y - zn.y));
-        const float2 B = make_float2(0.5f * (zk.y + zn.y), 0.5f * (zn.x - zk.x));
+    for (int p = 0; p < pairs; ++p) {
         const size_t row = (size_t)(pair0 + p) * 2;
-        half[row * SW + kx] = A;
-        half[(row + 1) * SW + kx] = B;
+        for (int kx = threadIdx.x; kx < SW; kx += blockDim.x) {
+            const float2 zk = z[p * MW + swz(kx)];
+            const float2 zn = z[p * MW + swz((MW - kx) & (MW - 1))];
+            const float2 A = make_float2(0.5f * (zk.x + zn.x), 0.5f * (zk.y - zn.y));
+            const float2 B = make_float2(0.5f * (zk.y + zn.y), 0.5f * (zn.x - zk.x));
+            half[row * SW + kx] = A;
+            half[(row + 1) * SW + kx] = B;
+        }
     }
 }
 
@@ -296,7 +298,7 @@ __device__ __forceinline__ void fft_columns_body(int block, const float2* __rest
         for (int u = 0; u < kLoadBatch; ++u) {
             const int t = t0 + u * blockDim.x;
             if (t < total) {
-                const int y = t / ncols, c = t - y * ncols;
+                const int c = t >> logH, y = t & (MH - 1);
                 v[u] = half[(size_t)y * SW + kx0 + c];
             }
         }
@@ -304,7 +306,7 @@ __device__ __forceinline__ void fft_columns_body(int block, const float2* __rest
         for (int u = 0; u < kLoadBatch; ++u) {
             const int t = t0 + u * blockDim.x;
             if (t < total) {
-                const int y = t / ncols, c = t - y * ncols;
+                const int c = t >> logH, y = t & (MH - 1);
                 A[c * MH + swz(y)] = v[u];
             }
         }
@@ -318,7 +320,7 @@ __device__ __forceinline__ void fft_columns_body(int block, const float2* __rest
         for (int u = 0; u < kLoadBatch; ++u) {
             const int t = threadIdx.x + u * blockDim.x;
             if (t < total) {
-                const int y = t / ncols, c = t - y * ncols;
+                const int c = t >> logH, y = t & (MH - 1);
                 gv[u] = __ldg(&green[(size_t)y * SW + kx0 + c]);
             }
         }
@@ -331,7 +333,7 @@ __device__ __forceinline__ void fft_columns_body(int block, const float2* __rest
             for (int u = 0; u < kLoadBatch; ++u) {
                 const int t = t0 + u * blockDim.x;
                 if (t < total) {
-                    const int y = t / ncols, c = t - y * ncols;
+                    const int c = t >> logH, y = t & (MH - 1);
                     gv[u] = __ldg(&green[(size_t)y * SW + kx0 + c]);
                 }
             }
@@ -340,7 +342,7 @@ __device__ __forceinline__ void fft_columns_body(int block, const float2* __rest
         for (int u = 0; u < kLoadBatch; ++u) {
             const int t = t0 + u * blockDim.x;
             if (t < total) {
-                const int y = t / ncols, c = t - y * ncols;
+                const int c = t >> logH, y = t & (MH - 1);
                 const float2 rho = R[c * MH + swz(y)];
                 const float gx = gv[u].x * inv_total, gy = gv[u].y * inv_total;
                 C[c * MH + swz(y)] = make_float2(-rho.y * gx, rho.x * gx);
@@ -351,7 +353,7 @@ __device__ __forceinline__ void fft_columns_body(int block, const float2* __rest
     __syncthreads();
     const float2* F = line_fft(C, A, MH, logH, 2 * ncols, MH, true, tws, twl);
     for (int t = threadIdx.x; t < ncols * MH; t += blockDim.x) {
-        const int y = t / ncols, c = t - y * ncols;
+        const int c = t >> logH, y = t & (MH - 1);
         const float2 fx = F[c * MH + swz(y)], fy = F[(ncols + c) * MH + swz(y)];
         cols[(size_t)y * SW + kx0 + c] = make_float4(fx.x, fx.y, fy.x, fy.y);
     }
@@ -455,37 +457,35 @@ __device__ __forceinline__ void fft_rows_inverse_body(int block, const float4* _
     float2* b = sm + rows_per_cta * MW;
     int twl;
     const float2* tws = stage_twiddles(tw, sm + 2 * rows_per_cta * MW, MW, ilog2(MW), &twl);
-    const int total = rows * SW;
-    for (int t0 = threadIdx.x; t0 < total; t0 += kLoadBatch * blockDim.x) {
-        float4 v[kLoadBatch];
+    for (int r = 0; r < rows; ++r) {
+        for (int k0 = threadIdx.x; k0 < SW; k0 += kLoadBatch * blockDim.x) {
+            float4 v[kLoadBatch];
 #pragma unroll
-        for (int u = 0; u < kLoadBatch; ++u) {
-            const int t = t0 + u * blockDim.x;
-            if (t < total) {
-                const int r = t / SW, kx = t - r * SW;
-                v[u] = cols[(size_t)(row0 + r) * SW + kx];  // (Fx.re, Fx.im, Fy.re, Fy.im)
+            for (int u = 0; u < kLoadBatch; ++u) {
+                const int kx = k0 + u * blockDim.x;
+                if (kx < SW) v[u] = cols[(size_t)(row0 + r) * SW + kx];  // (Fx.re, Fx.im, Fy.re, Fy.im)
             }
-        }
 #pragma unroll
-        for (int u = 0; u < kLoadBatch; ++u) {
-            const int t = t0 + u * blockDim.x;
-            if (t < total) {
-                const int r = t / SW, kx = t - r * SW;
-                const float4 q = v[u];
-                if (kx == 0 || kx == MW / 2) {
-                    // DC and Nyquist bins of a real row are real.
-                    a[r * MW + swz(kx)] = make_float2(q.x, q.z);
-                } else {
-                    a[r * MW + swz(kx)] = make_float2(q.x - q.w, q.y + q.z);
-                    a[r * MW + swz(MW - kx)] = make_float2(q.x + q.w, q.z - q.y);
+            for (int u = 0; u < kLoadBatch; ++u) {
+                const int kx = k0 + u * blockDim.x;
+                if (kx < SW) {
+                    const float4 q = v[u];
+                    if (kx == 0 || kx == MW / 2) {
+                        // DC and Nyquist bins of a real row are real.
+                        a[r * MW + swz(kx)] = make_float2(q.x, q.z);
+                    } else {
+                        a[r * MW + swz(kx)] = make_float2(q.x - q.w, q.y + q.z);
+                        a[r * MW + swz(MW - kx)] = make_float2(q.x + q.w, q.z - q.y);
+                    }
                 }
             }
         }
     }
     __syncthreads();
-    const float2* z = line_fft(a, b, MW, ilog2(MW), rows, MW, true, tws, twl);
+    const int logW = ilog2(MW);
+    const float2* z = line_fft(a, b, MW, logW, rows, MW, true, tws, twl);
     for (int t = threadIdx.x; t < rows * MW; t += blockDim.x) {
-        const int r = t / MW, x = t - r * MW;
+        const int r = t >> logW, x = t & (MW - 1);
         force[(size_t)(row0 + r) * MW + x] = z[r * MW + swz(x)];
     }
 }
