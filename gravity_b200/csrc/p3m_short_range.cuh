@@ -199,6 +199,112 @@ __device__ __forceinline__ StageBox stage_slots(bool valid, int hx, int hy,
     return box;
 }
 
+// The stencil sum of one target (its position t, ID id, home cell hx, hy),
+// accumulated per packed half: the two slots of a non-home cell (EXACT = 2),
+// two list entries at a time in a walked cell, and a monopole in .x.
+// STAGED: the slots come from the CTA's shared-memory box (base `sbase`, row
+// pitch `bw`), else from the global table. The two instantiations keep the
+// CTA-uniform choice out of the unrolled 49-cell loop.
+template <int RX, int RY, int EXACT, bool STAGED>
+__device__ __forceinline__ void stencil_sum(
+    float4 t, uint32_t id, int hx, int hy, const PairConst& k, const KickParams& p,
+    const float4* __restrict__ entries, const int* __restrict__ cell_start,
+    const int* __restrict__ cell_count, const uint32_t* __restrict__ cell_mass,
+    const float4* __restrict__ slots, const float2* __restrict__ slots_b, const float4* st_a,
+    const float2* st_b, int sbase, int bw, float2& acc_x, float2& acc_y) {
+    const float inv_w = 1.0f / (float)p.W, inv_h = 1.0f / (float)p.H;
+    // Per stencil column: wrapped column, periodic image shift, validity.
+    // off_x: the image shift less the target's x, so that a source at x on
+    // that column is at dx = x + off_x (exactly x - t.x where no wrap).
+    int col[2 * RX + 1];
+    float shift_x[2 * RX + 1];
+    float off_x[2 * RX + 1];
+    bool ok_x[2 * RX + 1];
+#pragma unroll
+    for (int a = 0; a < 2 * RX + 1; ++a) {
+        const int cx = hx + a - RX;
+        const int wx = wrap_index(cx, p.W);
+        col[a] = wx;
+        shift_x[a] = (float)(cx - wx) * inv_w;
+        off_x[a] = shift_x[a] - t.x;
+        ok_x[a] = !p.bounded || (cx >= 0 && cx < p.W);
+    }
+    const float2 neg_t = make_float2(-t.x, -t.y);
+    float2 ax2 = make_float2(0.0f, 0.0f), ay2 = make_float2(0.0f, 0.0f);
+#pragma unroll
+    for (int b = 0; b < 2 * RY + 1; ++b) {
+        const int cy = hy + b - RY;
+        if (p.bounded && (cy < 0 || cy >= p.H)) continue;
+        const int wy = wrap_index(cy, p.H);
+        const int row = wy * p.W;
+        const float shift_y = (float)(cy - wy) * inv_h;
+        const float cyr = ((float)wy + 0.5f) * inv_h;  // wrapped row centre
+        const float off_y = shift_y - t.y;
+#pragma unroll
+        for (int a = 0; a < 2 * RX + 1; ++a) {
+            if (!ok_x[a]) continue;
+            const int index = row + col[a];
+            const bool home = (a == RX) && (b == RY);
+            if (EXACT == 2 && !home) {
+                // The cell's two slots, prepared once per step (cell_slots):
+                // (x0, y0, G m0 / M_tot, x1) and (y1, G m1 / M_tot).
+                float4 s0;
+                float2 s1;
+                if (STAGED) {
+                    const int si = sbase + b * bw + a;
+                    s0 = st_a[si];
+                    s1 = st_b[si];
+                } else {
+                    s0 = __ldg(&slots[index]);
+                    s1 = __ldg(&slots_b[index]);
+                }
+                const float2 ox = make_float2(off_x[a], off_x[a]);
+                const float2 oy = make_float2(off_y, off_y);
+                pair_add2_gm(k, __fadd2_rn(make_float2(s0.x, s0.w), ox),
+                             __fadd2_rn(make_float2(s0.y, s1.x), oy), make_float2(s0.z, s1.y),
+                             ax2, ay2);
+                continue;
+            }
+            const int count = __ldg(&cell_count[index]);
+            if (count == 0) continue;
+            if (!home && count > p.exact) {
+                const float mass = (float)__ldg(&cell_mass[index]) * (1.0f / kCellMassUnits);
+                const float dx = ((float)col[a] + 0.5f) * inv_w + shift_x[a] - t.x;
+                float ax = ax2.x, ay = ay2.x;
+                pair_add(k, dx, (cyr + shift_y) - t.y, mass, ax, ay);
+                ax2.x = ax;
+                ay2.x = ay;
+            } else {
+                // The list walk, two entries at a time; the target itself and
+                // the filler of an odd count have mass 0 and add nothing.
+                const int limit = home ? p.home_limit : p.exact;
+                const int walk = count < limit ? count : limit;
+                const int start = __ldg(&cell_start[index]);
+                const float2 sx = make_float2(shift_x[a], shift_x[a]);
+                const float2 sy = make_float2(shift_y, shift_y);
+                for (int e = 0; e < walk; e += 2) {
+                    const float4 o0 = __ldg(&entries[start + e]);
+                    const bool has1 = e + 1 < walk;
+                    const float4 o1 = has1 ? __ldg(&entries[start + e + 1]) : o0;
+                    const float m0 = __float_as_uint(o0.w) != id ? o0.z : 0.0f;
+                    const float m1 = has1 && __float_as_uint(o1.w) != id ? o1.z : 0.0f;
+                    // (o + shift) - t, rounded as the scalar form does.
+                    const float2 dx = __fadd2_rn(__fadd2_rn(make_float2(o0.x, o1.x), sx),
+                                                 make_float2(neg_t.x, neg_t.x));
+                    const float2 dy = __fadd2_rn(__fadd2_rn(make_float2(o0.y, o1.y), sy),
+                                                 make_float2(neg_t.y, neg_t.y));
+                    pair_add2_gm(k, dx, dy,
+                                 __fmul2_rn(make_float2(k.g_over_m, k.g_over_m),
+                                            make_float2(m0, m1)),
+                                 ax2, ay2);
+                }
+            }
+        }
+    }
+    acc_x = ax2;
+    acc_y = ay2;
+}
+
 template <int RX, int RY, int EXACT>
 __device__ __forceinline__ void short_range_body(
     int block, const float4* __restrict__ bodies, const float4* __restrict__ entries,
@@ -232,77 +338,16 @@ __device__ __forceinline__ void short_range_body(
         if (box.staged) sbase = (hy - RY - box.y0) * box.w + (hx - RX - box.x0);
     }
 
-    // Per stencil column: wrapped column, periodic image shift, validity.
-    // off_x: the image shift less the target's x, so that a source at x on
-    // that column is at dx = x + off_x (exactly x - t.x where no wrap).
-    int col[2 * RX + 1];
-    float shift_x[2 * RX + 1];
-    float off_x[2 * RX + 1];
-    bool ok_x[2 * RX + 1];
-#pragma unroll
-    for (int a = 0; a < 2 * RX + 1; ++a) {
-        const int cx = hx + a - RX;
-        const int wx = wrap_index(cx, p.W);
-        col[a] = wx;
-        shift_x[a] = (float)(cx - wx) * inv_w;
-        off_x[a] = shift_x[a] - t.x;
-        ok_x[a] = !p.bounded || (cx >= 0 && cx < p.W);
-    }
-    float ax = 0.0f, ay = 0.0f;
-    float2 ax2 = make_float2(0.0f, 0.0f), ay2 = make_float2(0.0f, 0.0f);  // per slot
-#pragma unroll
-    for (int b = 0; b < 2 * RY + 1; ++b) {
-        const int cy = hy + b - RY;
-        if (p.bounded && (cy < 0 || cy >= p.H)) continue;
-        const int wy = wrap_index(cy, p.H);
-        const int row = wy * p.W;
-        const float shift_y = (float)(cy - wy) * inv_h;
-        const float cyr = ((float)wy + 0.5f) * inv_h;  // wrapped row centre
-        const float off_y = shift_y - t.y;
-#pragma unroll
-        for (int a = 0; a < 2 * RX + 1; ++a) {
-            if (!ok_x[a]) continue;
-            const int index = row + col[a];
-            const bool home = (a == RX) && (b == RY);
-            if (EXACT == 2 && !home) {
-                // The cell's two slots, prepared once per step (cell_slots):
-                // (x0, y0, G m0 / M_tot, x1) and (y1, G m1 / M_tot).
-                float4 s0;
-                float2 s1;
-                if (box.staged) {
-                    const int si = sbase + b * box.w + a;
-                    s0 = st_a[si];
-                    s1 = st_b[si];
-                } else {
-                    s0 = __ldg(&slots[index]);
-                    s1 = __ldg(&slots_b[index]);
-                }
-                const float2 ox = make_float2(off_x[a], off_x[a]);
-                const float2 oy = make_float2(off_y, off_y);
-                pair_add2_gm(k, __fadd2_rn(make_float2(s0.x, s0.w), ox),
-                             __fadd2_rn(make_float2(s0.y, s1.x), oy), make_float2(s0.z, s1.y),
-                             ax2, ay2);
-                continue;
-            }
-            const int count = __ldg(&cell_count[index]);
-            if (count == 0) continue;
-            if (!home && count > p.exact) {
-                const float mass = (float)__ldg(&cell_mass[index]) * (1.0f / kCellMassUnits);
-                const float dx = ((float)col[a] + 0.5f) * inv_w + shift_x[a] - t.x;
-                pair_add(k, dx, (cyr + shift_y) - t.y, mass, ax, ay);
-            } else {
-                const int limit = home ? p.home_limit : p.exact;
-                const int walk = count < limit ? count : limit;
-                const int start = __ldg(&cell_start[index]);
-                for (int e = 0; e < walk; ++e) {
-                    const float4 o = __ldg(&entries[start + e]);
-                    if (__float_as_uint(o.w) != id)
-                        pair_add(k, (o.x + shift_x[a]) - t.x, (o.y + shift_y) - t.y, o.z, ax, ay);
-                }
-            }
-        }
-    }
-    a_short[id] = make_float2(ax + (ax2.x + ax2.y), ay + (ay2.x + ay2.y));
+    float2 acc_x, acc_y;
+    if (EXACT == 2 && box.staged)
+        stencil_sum<RX, RY, EXACT, true>(t, id, hx, hy, k, p, entries, cell_start, cell_count,
+                                         cell_mass, slots, slots_b, st_a, st_b, sbase, box.w,
+                                         acc_x, acc_y);
+    else
+        stencil_sum<RX, RY, EXACT, false>(t, id, hx, hy, k, p, entries, cell_start, cell_count,
+                                          cell_mass, slots, slots_b, st_a, st_b, sbase, box.w,
+                                          acc_x, acc_y);
+    a_short[id] = make_float2(acc_x.x + acc_x.y, acc_y.x + acc_y.y);
 }
 
 template <int RX, int RY, int EXACT>
