@@ -1874,12 +1874,23 @@ struct p3m_adjoint_store {
     float* cot = nullptr;           // 2*MH x MW
     float2* half2 = nullptr;        // 2*MH x (MW/2+1)
     float2* mu2 = nullptr;          // MH/2 x MW
+    // One captured reverse step per slot (its pointers are the slot's), with
+    // the parameters it was captured with; re-captured when they change.
+    struct ReverseGraph {
+        cudaGraphExec_t exec = nullptr;
+        p3m::AdjointParams p{};
+        const void* buffers[4] = {};  // the context buffers it reads
+        long long kernels = 0;
+    };
+    std::vector<ReverseGraph> reverse_graphs;
 };
 
 namespace {
 
 void adjoint_free(p3m_ctx* ctx) {
     if (!ctx->adjoint) return;
+    for (auto& g : ctx->adjoint->reverse_graphs)
+        if (g.exec) cudaGraphExecDestroy(g.exec);
     for (void* b : ctx->adjoint->blocks) cudaFree(b);
     delete ctx->adjoint;
     ctx->adjoint = nullptr;
@@ -1939,15 +1950,45 @@ int adjoint_prepare(p3m_ctx* ctx, int n, int steps, int interval) {
     P3M_CUDA(ctx, cudaMemcpyAsync((dst), (src), (bytes), cudaMemcpyDeviceToDevice, (ctx)->stream))
 
 // Keeps what the reverse step at the current state needs.
+// Up to six device-to-device copies in one launch (16-byte words; every
+// segment here starts on a 16-byte boundary and is a multiple of 16 bytes).
+struct CopySegments {
+    uint4* dst[6];
+    const uint4* src[6];
+    long long words[6];
+    int count;
+};
+
+__global__ void __launch_bounds__(256) copy_segments_kernel(CopySegments c) {
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (int k = 0; k < c.count; ++k)
+        for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < c.words[k];
+             i += stride)
+            c.dst[k][i] = c.src[k][i];
+}
+
+// The state a reverse step needs, saved into recompute slot `slot` with one
+// kernel (a backward pass saves a slot per step: six copies each would be
+// six launches).
 int adjoint_save_slot(p3m_ctx* ctx, int slot) {
     p3m_adjoint_store* a = ctx->adjoint;
     const size_t n = (size_t)a->n, P = a->P, M = a->M, s = (size_t)slot;
-    P3M_COPY(ctx, a->slot_bodies + s * n, ctx->bodies, n * sizeof(float4));
-    P3M_COPY(ctx, a->slot_entries + s * n, ctx->entries, n * sizeof(float4));
-    P3M_COPY(ctx, a->slot_start + s * P, ctx->cell_start, P * sizeof(int));
-    P3M_COPY(ctx, a->slot_count + s * P, ctx->cell_count, P * sizeof(int));
-    P3M_COPY(ctx, a->slot_mass + s * P, ctx->cell_mass, P * sizeof(uint32_t));
-    P3M_COPY(ctx, a->slot_force + s * M, ctx->force, M * sizeof(float2));
+    CopySegments c{};
+    auto add = [&](void* dst, const void* src, size_t bytes) {
+        c.dst[c.count] = static_cast<uint4*>(dst);
+        c.src[c.count] = static_cast<const uint4*>(src);
+        c.words[c.count] = (long long)(bytes / sizeof(uint4));
+        ++c.count;
+    };
+    add(a->slot_bodies + s * n, ctx->bodies, n * sizeof(float4));
+    add(a->slot_entries + s * n, ctx->entries, n * sizeof(float4));
+    add(a->slot_start + s * P, ctx->cell_start, P * sizeof(int));  // P is a multiple of 16
+    add(a->slot_count + s * P, ctx->cell_count, P * sizeof(int));
+    add(a->slot_mass + s * P, ctx->cell_mass, P * sizeof(uint32_t));
+    add(a->slot_force + s * M, ctx->force, M * sizeof(float2));
+    copy_segments_kernel<<<4 * 148, 256, 0, ctx->stream>>>(c);
+    p3m::count_launches(1);
+    P3M_CUDA(ctx, cudaGetLastError());
     return P3M_OK;
 }
 
@@ -1981,7 +2022,7 @@ p3m::AdjointParams adjoint_params(const p3m_ctx* ctx, int n) {
 }
 
 // One reverse step against recompute slot `slot`.
-int adjoint_reverse(p3m_ctx* ctx, int slot, const p3m::AdjointParams& p) {
+int adjoint_reverse_enqueue(p3m_ctx* ctx, int slot, const p3m::AdjointParams& p) {
     p3m_adjoint_store* a = ctx->adjoint;
     const size_t n = (size_t)a->n, P = a->P, M = a->M, s = (size_t)slot;
     const float4* bodies = a->slot_bodies + s * n;
@@ -1999,6 +2040,48 @@ int adjoint_reverse(p3m_ctx* ctx, int slot, const p3m::AdjointParams& p) {
     P3M_CUDA(ctx, p3m::launch_adjoint_gather(bodies, ctx->materials, a->wa, a->mu2,
                                              a->slot_force + s * M, a->g_short, a->lam, a->lam_a,
                                              p, ctx->stream));
+    return P3M_OK;
+}
+
+// One reverse step (two clears and six kernels), replayed from a CUDA graph
+// captured once per slot: a backward pass runs hundreds of them, each too
+// short to hide eight launches.
+int adjoint_reverse(p3m_ctx* ctx, int slot, const p3m::AdjointParams& p) {
+    p3m_adjoint_store* a = ctx->adjoint;
+    if (!ctx->use_graphs || ctx->profiling) return adjoint_reverse_enqueue(ctx, slot, p);
+    if ((int)a->reverse_graphs.size() < a->slots) a->reverse_graphs.resize(a->slots);
+    auto& g = a->reverse_graphs[slot];
+    const void* buffers[4] = {ctx->materials, ctx->green, ctx->cols, ctx->twiddles};
+    if (g.exec && std::memcmp(&g.p, &p, sizeof(p)) == 0 &&
+        std::memcmp(g.buffers, buffers, sizeof(buffers)) == 0) {
+        P3M_CUDA(ctx, cudaGraphLaunch(g.exec, ctx->stream));
+        p3m::count_launches((int)g.kernels);
+        return P3M_OK;
+    }
+    if (g.exec) {
+        cudaGraphExecDestroy(g.exec);
+        g.exec = nullptr;
+    }
+    const long long k0 = p3m_kernel_launches();
+    P3M_CUDA(ctx, cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+    const int st = adjoint_reverse_enqueue(ctx, slot, p);
+    cudaGraph_t graph = nullptr;
+    cudaError_t e = cudaStreamEndCapture(ctx->stream, &graph);
+    if (st != P3M_OK || e != cudaSuccess) {
+        if (graph) cudaGraphDestroy(graph);
+        if (st != P3M_OK) return st;
+        return fail_cuda(ctx, "cudaStreamEndCapture", e);
+    }
+    g.kernels = p3m_kernel_launches() - k0;
+    e = cudaGraphInstantiate(&g.exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (e != cudaSuccess) {
+        g.exec = nullptr;
+        return fail_cuda(ctx, "cudaGraphInstantiate", e);
+    }
+    g.p = p;
+    std::memcpy(g.buffers, buffers, sizeof(buffers));
+    P3M_CUDA(ctx, cudaGraphLaunch(g.exec, ctx->stream));
     return P3M_OK;
 }
 
