@@ -88,8 +88,10 @@ def mesh_sizes(sc):
 
 
 def stage_bytes(sc, stage: str, radix_passes: int) -> float:
-    """Algorithmic bytes of one launch of a stage (the per-unit figures are
-    listed in DESIGN.md, section "Kernels and their rooflines")."""
+    """Algorithmic bytes of one launch of a stage: the compulsory traffic of
+    its inputs and outputs for N bodies, P physical cells, M mesh cells and
+    p radix passes (body records 16 B, accelerations 8 B, cell tables 4 B per
+    word, mesh words 4 or 8 B)."""
     n = sc.n
     P, M = mesh_sizes(sc)
     i64 = sc.config.deposit_mode == 1
