@@ -398,25 +398,58 @@ __global__ void __launch_bounds__(256) fft_columns_adjoint_kernel(const float2* 
     const int logH = ilog2(MH);
     float2* A = sm;               // 2G lines: X columns, then Y columns
     float2* B = sm + 2 * G * MH;  // 2G lines
-    for (int t = threadIdx.x; t < 2 * ncols * MH; t += blockDim.x) {
-        const int row = t / ncols, c = t - row * ncols;  // row = 2y + component
-        const int y = row >> 1, comp = row & 1;
-        A[(comp * ncols + c) * MH + swz(y)] = half[(size_t)row * SW + kx0 + c];
+    int twl;
+    const float2* tws = stage_twiddles(tw, sm + 4 * G * MH, MH, logH, &twl);
+    // Line l = comp * ncols + c holds component comp of column c; a thread
+    // takes points of one line at a time (shifts, no division).
+    const int total2 = 2 * ncols * MH;
+    for (int t0 = threadIdx.x; t0 < total2; t0 += kLoadBatch * blockDim.x) {
+        float2 v[kLoadBatch];
+#pragma unroll
+        for (int u = 0; u < kLoadBatch; ++u) {
+            const int t = t0 + u * blockDim.x;
+            if (t < total2) {
+                const int l = t >> logH, y = t & (MH - 1);
+                const int comp = l >= ncols ? 1 : 0, c = l - comp * ncols;
+                v[u] = half[(size_t)(2 * y + comp) * SW + kx0 + c];
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < kLoadBatch; ++u) {
+            const int t = t0 + u * blockDim.x;
+            if (t < total2) A[(t >> logH) * MH + swz(t & (MH - 1))] = v[u];
+        }
     }
     __syncthreads();
-    float2* R = line_fft(A, B, MH, logH, 2 * ncols, MH, false, tw);
+    float2* R = line_fft(A, B, MH, logH, 2 * ncols, MH, false, tws, twl);
     float2* C = R == A ? B : A;
-    for (int t = threadIdx.x; t < ncols * MH; t += blockDim.x) {
-        const int y = t / ncols, c = t - y * ncols;
-        const float2 X = R[c * MH + swz(y)], Y = R[(ncols + c) * MH + swz(y)];
-        const float2 g = __ldg(&green[(size_t)y * SW + kx0 + c]);
-        const float sx = X.x * g.x + Y.x * g.y, sy = X.y * g.x + Y.y * g.y;
-        C[c * MH + swz(y)] = make_float2(sy * inv_total, -sx * inv_total);  // -i (gx X + gy Y) / M
+    const int total = ncols * MH;
+    for (int t0 = threadIdx.x; t0 < total; t0 += kLoadBatch * blockDim.x) {
+        float2 gv[kLoadBatch];
+#pragma unroll
+        for (int u = 0; u < kLoadBatch; ++u) {
+            const int t = t0 + u * blockDim.x;
+            if (t < total) {
+                const int c = t >> logH, y = t & (MH - 1);
+                gv[u] = __ldg(&green[(size_t)y * SW + kx0 + c]);
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < kLoadBatch; ++u) {
+            const int t = t0 + u * blockDim.x;
+            if (t < total) {
+                const int c = t >> logH, y = t & (MH - 1);
+                const float2 X = R[c * MH + swz(y)], Y = R[(ncols + c) * MH + swz(y)];
+                const float2 g = gv[u];
+                const float sx = X.x * g.x + Y.x * g.y, sy = X.y * g.x + Y.y * g.y;
+                C[c * MH + swz(y)] = make_float2(sy * inv_total, -sx * inv_total);  // -i (gx X + gy Y) / M
+            }
+        }
     }
     __syncthreads();
-    const float2* F = line_fft(C, R, MH, logH, ncols, MH, true, tw);
-    for (int t = threadIdx.x; t < ncols * MH; t += blockDim.x) {
-        const int y = t / ncols, c = t - y * ncols;
+    const float2* F = line_fft(C, R, MH, logH, ncols, MH, true, tws, twl);
+    for (int t = threadIdx.x; t < total; t += blockDim.x) {
+        const int c = t >> logH, y = t & (MH - 1);
         cols[((size_t)(y >> 1) * SW + kx0 + c) * 2 + (y & 1)] = F[c * MH + swz(y)];
     }
 }
@@ -697,7 +730,7 @@ cudaError_t launch_fft_adjoint(const float* cotangent, const float2* green, floa
         column_shape(g.MW, g.MH, 4, &G, &threads, g.fft_lines);
         const int SW = g.MW / 2 + 1;
         const int blocks = (SW + G - 1) / G;
-        const size_t smem = (size_t)4 * G * g.MH * sizeof(float2);
+        const size_t smem = ((size_t)4 * G * g.MH + staged_twiddles(g.MH)) * sizeof(float2);
         fft_columns_adjoint_kernel<<<blocks, threads, smem, stream>>>(
             half2, green, inv_total, g.MW, g.MH, G, twiddles, reinterpret_cast<float2*>(cols));
         count_launches(1);
