@@ -220,7 +220,7 @@ void free_all(p3m_ctx* ctx) {
                     ctx->materials_alt, ctx->destinations, ctx->status, ctx->keys, ctx->vals,
                     ctx->sort.keys_alt, ctx->sort.vals_alt, ctx->sort.hist, ctx->sort.block_sums,
                     ctx->sort.lookback,
-                    ctx->cell_start, ctx->cell_count, ctx->cell_mass, ctx->entries, ctx->cell_slots,
+                    ctx->cell_start, ctx->cell_count, ctx->entries, ctx->cell_slots,
                     ctx->a_short, ctx->deposit_work, ctx->density,
                     ctx->half, ctx->cols, ctx->force, ctx->green, ctx->twiddles};
     for (void* p : ptrs)
@@ -271,8 +271,8 @@ int lists_from_keys(p3m_ctx* ctx, int n, bool totals_ready = false) {
                                         ctx->stream, &sk, &sv, totals_ready));
     ctx->sorted_keys = sk;
     ctx->sorted_ids = sv;
-    P3M_CUDA(ctx, cudaMemsetAsync(ctx->cell_count, 0, P * sizeof(int), ctx->stream));
-    P3M_CUDA(ctx, cudaMemsetAsync(ctx->cell_mass, 0, P * sizeof(uint32_t), ctx->stream));
+    // Counts and masses are one block (cell_mass follows cell_count): one clear.
+    P3M_CUDA(ctx, cudaMemsetAsync(ctx->cell_count, 0, 2 * P * sizeof(int), ctx->stream));
     P3M_CUDA(ctx, p3m::launch_cell_build(sk, sv, n, ctx->bodies, ctx->materials, ctx->cell_start,
                                          ctx->cell_count, ctx->cell_mass, ctx->entries,
                                          p3m::deposit_uses_cell_starts(n) ? (int)P : 0,
@@ -665,8 +665,8 @@ int p3m_create(const p3m_config* config, p3m_ctx** out) {
     ALLOC(ctx->sort.block_sums, p3m::sort_block_sum_entries((int)cap));
     ALLOC(ctx->sort.lookback, p3m::sort_lookback_words((int)cap));
     ALLOC(ctx->cell_start, P + 1);
-    ALLOC(ctx->cell_count, P);
-    ALLOC(ctx->cell_mass, P);
+    ALLOC(ctx->cell_count, 2 * P);  // counts, then the masses (cleared together)
+    ctx->cell_mass = reinterpret_cast<uint32_t*>(ctx->cell_count + P);
     ALLOC(ctx->cell_slots, (3 * P + 1) / 2);  // float4 plane + float2 plane
     ALLOC(ctx->entries, cap);
     ALLOC(ctx->a_short, cap);
