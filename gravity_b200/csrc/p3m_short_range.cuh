@@ -88,9 +88,10 @@ __device__ __forceinline__ float fast_rcp(float x) {
     return y;
 }
 
-// A cell's two slots at once with Blackwell's packed FP32x2 arithmetic (each
-// half rounded as one scalar operation): the pair term of pair_add_gm for
-// source 0 in .x and source 1 in .y, accumulated into (ax, ay) per slot.
+// Two sources at once with Blackwell's packed FP32x2 arithmetic (each half
+// rounded as one scalar operation): the pair term of pair_add with the
+// source's G m / M_tot already formed (`gm`), source 0 in .x and source 1 in
+// .y, accumulated into (ax, ay) per half.
 __device__ __forceinline__ void pair_add2_gm(const PairConst& k, float2 dx, float2 dy, float2 gm,
                                              float2& ax, float2& ay) {
     const float2 px = __fmul2_rn(dx, make_float2(k.aspect, k.aspect));
@@ -102,17 +103,6 @@ __device__ __forceinline__ void pair_add2_gm(const PairConst& k, float2 dx, floa
     const float2 phys = __fmul2_rn(num, inv);
     ax = __ffma2_rn(phys, dx, ax);
     ay = __ffma2_rn(phys, dy, ay);
-}
-
-// pair_add with the source's G m / M_tot already formed (a cell slot).
-__device__ __forceinline__ void pair_add_gm(const PairConst& k, float dx, float dy, float gm,
-                                            float& ax, float& ay) {
-    const float px = dx * k.aspect;
-    const float r2 = fmaf(px, px, dy * dy);
-    const float w = fast_exp2(r2 * k.neg_log2e_over_2s2);
-    const float phys = __fdividef(gm * w, fmaxf(r2, k.min_dist2));
-    ax = fmaf(phys, dx, ax);
-    ay = fmaf(phys, dy, ay);
 }
 
 // Cells of the slot table a CTA stages in shared memory (24 bytes each): the
@@ -317,7 +307,6 @@ __device__ __forceinline__ void short_range_body(
     const float4 t = valid ? bodies[i] : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
     const uint32_t id = (uint32_t)i;
     const PairConst k = pair_const(p);
-    const float inv_w = 1.0f / (float)p.W, inv_h = 1.0f / (float)p.H;
     const float2* __restrict__ slots_b =
         reinterpret_cast<const float2*>(slots + (size_t)p.W * p.H);
     const int hx = guard_coord(float_to_int(floorf(t.x * (float)p.W)), p.W);

@@ -102,7 +102,6 @@ __global__ void __launch_bounds__(kScanThreads) scan_add_kernel(uint32_t* data, 
 }
 
 // ------------------------------------------------------------ radix sort
-constexpr int kSortWarps = kSortThreads / 32;
 
 // Per-tile digit histogram, written digit-major (hist[d * tiles + tile]) so
 // that one exclusive scan of the whole array yields every tile's output base
