@@ -338,13 +338,17 @@ p3m::KickParams kick_params(const p3m_ctx* ctx, int n, int initial) {
     p.min_frac = ctx->cfg.minimum_distance_cell_fraction; p.dt = ctx->cfg.time_step;
     p.field_x = ctx->field_x; p.field_y = ctx->field_y;
     p.sr_threads = ctx->tune_sr_threads;
+    // Two-slot form for exact limit 2 unless the simulation is sparse (under
+    // one body per two cells): the slot table of mostly empty cells then
+    // costs more than the list walk it saves.
+    p.slot_form = p.exact == 2 && 2 * (long long)n >= (long long)phys_cells(ctx);
     return p;
 }
 
 // The short range over the current cell lists; with exact limit 2 it reads
 // the per-cell slot table, built first on the same stream.
 int short_range(p3m_ctx* ctx, const p3m::KickParams& p, cudaStream_t stream) {
-    if (p.exact == 2 && p.n > 0)
+    if (p.slot_form && p.n > 0)
         P3M_CUDA(ctx, p3m::launch_cell_slots(ctx->cell_start, ctx->cell_count, ctx->cell_mass,
                                              ctx->entries, ctx->grid.W, ctx->grid.H,
                                              p.gravity, p.total_mass, ctx->cell_slots, stream));
@@ -1397,13 +1401,15 @@ int build_fused(p3m_batch* b, const std::vector<char>& sort, p3m_batch::Plan& pl
             if (e == cudaSuccess) e = cudaStreamWaitEvent(side, fork_ev, 0);
             return e;
         });
-        // The two-slot form (exact limit 2) first builds each cell's slots.
+        // The two-slot form first builds each cell's slots (kick_params says
+        // which simulations take it).
+        auto slot_form = [&](int i) { return kick_params(b->sims[i], b->n[i], 0).slot_form != 0; };
         {
             std::vector<p3m::SlotsArgs> sl;
             std::vector<int> slb;
             for (int i : mut) {
                 p3m_ctx* c = b->sims[i];
-                if (c->cfg.exact_neighbor_body_limit != 2) continue;
+                if (!slot_form(i)) continue;
                 const p3m::KickParams kp = kick_params(c, b->n[i], 0);
                 sl.push_back({c->cell_start, c->cell_count, c->cell_mass, c->entries,
                               c->cell_slots, c->grid.W, c->grid.H, kp.gravity, kp.total_mass});
@@ -1414,12 +1420,10 @@ int build_fused(p3m_batch* b, const std::vector<char>& sort, p3m_batch::Plan& pl
                     return p3m::batched_cell_slots(a, g, side);
                 });
         }
-        // (The branch-free two-slot form of exact limit 2 also beats the list
-        // walk on sparse simulations: measured on the batch workload.)
         std::map<int, std::vector<int>> groups;  // rx * 64 + ry * 2 + two-slot form
         for (int i : mut) {
             const p3m_ctx* c = b->sims[i];
-            groups[c->rx * 64 + c->ry * 2 + (c->cfg.exact_neighbor_body_limit == 2 ? 1 : 0)].push_back(i);
+            groups[c->rx * 64 + c->ry * 2 + (slot_form(i) ? 1 : 0)].push_back(i);
         }
         for (const auto& kv : groups) {
             std::vector<p3m::ShortRangeArgs> sa;

@@ -217,6 +217,9 @@ cudaError_t build_green(GridShape g, GreenParams p, double2* work, float2* green
 struct KickParams {
     int n, W, H, MW, MH, bounded, rx, ry, exact, home_limit, initial, mutual;
     int sr_threads;  // block size of the short-range kernel (64..256)
+    // The short range's two-slot form (exact limit 2, at least one body per
+    // two cells: it reads the per-cell slot table); else the list walk.
+    int slot_form;
     float aspect, gravity, sigma_cells, total_mass, min_frac, dt, field_x, field_y;
 };
 // Short-range correction over the cell stencil (kick.comp:122-151), one

@@ -396,7 +396,7 @@ P3M_DECLARE_SHORT_RANGE_RX(6)
                                            cudaStream_t stream) {                               \
         const int threads_ = p.sr_threads > 0 ? p.sr_threads : 256;                               \
         const dim3 grid((p.n + threads_ - 1) / threads_), block(threads_);                      \
-        switch (p.ry * 2 + (p.exact == 2 ? 1 : 0)) {                                            \
+        switch (p.ry * 2 + (p.slot_form ? 1 : 0)) {                                             \
             case 3: launch_chained(sr::short_range_kernel<RX_, 1, 2>, grid, block, 0, stream, bodies, entries, cell_start, cell_count, cell_mass, slots, a_short, p); break; \
             case 2: launch_chained(sr::short_range_kernel<RX_, 1, 0>, grid, block, 0, stream, bodies, entries, cell_start, cell_count, cell_mass, slots, a_short, p); break; \
             case 5: launch_chained(sr::short_range_kernel<RX_, 2, 2>, grid, block, 0, stream, bodies, entries, cell_start, cell_count, cell_mass, slots, a_short, p); break; \
