@@ -240,14 +240,20 @@ def dist_env():
 
 
 def init_dist(ws: int, local: int):
+    """One process per GPU over NCCL (barrier and max-over-ranks timing only:
+    the replicas exchange no data). Without CUDA (the CPU tests) the same
+    calls run over gloo."""
     import torch
     import torch.distributed as dist
 
     if ws > 1:
-        torch.cuda.set_device(local)
         from datetime import timedelta
-        dist.init_process_group("nccl", timeout=timedelta(seconds=120),
-                                device_id=torch.device("cuda", local))
+        if torch.cuda.is_available():
+            torch.cuda.set_device(local)
+            dist.init_process_group("nccl", timeout=timedelta(seconds=120),
+                                    device_id=torch.device("cuda", local))
+        else:
+            dist.init_process_group("gloo", timeout=timedelta(seconds=120))
     return dist if ws > 1 else None
 
 
@@ -256,7 +262,8 @@ def allreduce_max(dist, value: float) -> float:
         return value
     import torch
 
-    t = torch.tensor([value], dtype=torch.float64, device="cuda")
+    device = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([value], dtype=torch.float64, device=device)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
 
