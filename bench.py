@@ -6,11 +6,14 @@ One step = one gravity-only P3M leapfrog step of the workload
 half kick + drift, cell-key sort and lists, CIC deposit, real FFT with the
 Green's multiply, inverse, interpolation + short range + half kick.
 
-Default workload (N=1): 400,000 bodies in two projected Plummer spheres
-inside walls, physical grid 512x256 (Hockney FFT mesh 1024x512), uint32
-fixed-point deposit, FP32 forces. The whole state and mesh (~40 MB) fit in the
-126 MB L2, so L2 is flushed (a 256 MiB write) before every timed step, outside
-the step's events.
+Default workload (N=1): the precision form at scale, 8,000,000 bodies from a
+4096x2048 lattice displaced by a Gaussian random field (P(k) ~ k^-2,
+displacement RMS 3 cells, seed 7) on a 4096x2048 torus, int64 fixed-point
+deposit, FP32 FFT and forces. Beside it (`plain_form`): 400,000 bodies in two
+projected Plummer spheres inside walls, physical grid 512x256 (Hockney FFT
+mesh 1024x512), the reference's uint32 deposit. L2 is flushed (a 256 MiB
+write) before every timed step, outside the step's events (the 400k state
+fits in the 126 MB L2; the 8M state does not).
 
 Printed (rank 0, one JSON line):
   value     bodies*steps/s from CUDA events around each step, state resident
@@ -22,7 +25,12 @@ Printed (rank 0, one JSON line):
             once, before timing, as the reference uploads them when it seeds
             bodies.
   roofline  the dominant stage's algorithmic bytes / its event-timed average
-            duration, against the measured HBM copy bandwidth.
+            duration, against the measured HBM copy bandwidth; every stage's
+            fraction is in `stages`, the deposit's and the kick's also in
+            `roofline_hbm_stages`.
+  force_rms_err_vs_fp64_by_form  RMS force error against the FP64 direct sum
+            on one seeded 4096-body subsample for the int64 form, the uint32
+            form and the CPU oracle's FP32 path.
   cpu_baseline  the CPU oracle (the C++ restatement of the reference's
             shaders) on this host's cores, on a bounded sample.
 
@@ -61,23 +69,77 @@ FORCE_SAMPLE = 4096
 
 
 # ----------------------------------------------------------------- workloads
-def make_workload(name: str):
+def make_workload(name: str, bodies: int | None = None, grid: str | None = None,
+                  sims: int | None = None):
+    """A named workload at its stated size, or with `bodies` / `grid` (WxH)
+    overridden: the smaller cases the committed Nsight Compute captures run."""
     from gravity_b200 import scenarios
 
+    g = tuple(int(v) for v in grid.split("x")) if grid else None
     if name == "plummer_walls":
-        return scenarios.plummer_walls()
+        return scenarios.plummer_walls(**({"n": bodies} if bodies else {}))
     if name == "uniform_torus":
-        return scenarios.uniform_torus()
-    if name == "lattice_scale":
-        return scenarios.lattice_scale()
-    if name == "batch":
-        return scenarios.batch()
-    if name == "adjoint":
-        return scenarios.adjoint_cluster()
-    if name == "lattice_scale_u32":
+        return scenarios.uniform_torus(**({"n": bodies} if bodies else {}))
+    if name in ("lattice_scale", "lattice_scale_u32"):
         from gravity_b200 import _abi
-        return scenarios.lattice_scale(deposit_mode=_abi.P3M_DEPOSIT_U32)
+        kw = {}
+        if bodies:
+            kw["n"] = bodies
+        if g:
+            kw["grid"] = g
+        if name == "lattice_scale_u32":
+            kw["deposit_mode"] = _abi.P3M_DEPOSIT_U32
+        return scenarios.lattice_scale(**kw)
+    if name == "batch":
+        return scenarios.batch(**({"sims": sims} if sims else {}))
+    if name == "adjoint":
+        kw = {}
+        if bodies:
+            kw["n_cluster"] = bodies - 1000
+        if g:
+            kw["grid"] = g
+        return scenarios.adjoint_cluster(**kw)
     raise SystemExit(f"unknown workload {name}")
+
+
+def run_only(args) -> None:
+    """The workload's initial pass and --steps steps, nothing timed or
+    printed but a final 'ok': the target of the committed Nsight Compute
+    captures (adjoint: a checkpointed rollout of --steps steps and its
+    backward pass; batch: --steps batch steps)."""
+    import torch
+
+    torch.cuda.set_device(0)
+    if args.workload == "batch":
+        from gravity_b200.batch import GravityBatch
+
+        scs = make_workload("batch", sims=args.sims)
+        with GravityBatch([sc.config for sc in scs]) as b:
+            for i, sc in enumerate(scs):
+                b.upload(i, sc.bodies, sc.materials)
+            b.initialize_acceleration()
+            b.step(args.steps)
+            b.synchronize()
+        print("ok", sum(sc.n for sc in scs))
+        return
+    from gravity_b200.pipeline import GravityPipeline
+
+    sc = make_workload(args.workload, args.bodies, args.grid)
+    with GravityPipeline(sc.config) as p:
+        p.upload(sc.bodies, sc.materials)
+        if args.workload == "adjoint":
+            from gravity_b200.adjoint import Rollout
+
+            r = Rollout(p, sc.n, args.steps, checkpoint_interval=max(1, args.steps // 2))
+            r.forward()
+            seed = np.zeros((sc.n, 4), np.float32)
+            seed[-1000:, 0] = 1.0
+            r.backward(seed)
+        else:
+            p.initialize_acceleration(sc.n)
+            p.step(sc.n, args.steps)
+        p.synchronize()
+    print("ok", sc.n)
 
 
 def mesh_sizes(sc):
@@ -302,7 +364,7 @@ def run_reference(args, ws, rank):
         }
         print(json.dumps(line), flush=True)
         return
-    sc = make_workload(args.workload)
+    sc = make_workload(args.workload, args.bodies, args.grid)
     threads = os.cpu_count() or 1
     budget = max(5.0, min(90.0, float(args.steps) * 2.0))
     rate, steps, el, used = cpu_oracle_rate(sc, budget, threads=threads,
@@ -366,13 +428,13 @@ def cpu_oracle_batch_rate(scs, budget_s: float, threads: int | None = None):
     return work / el, sims, el, used
 
 
-def workload_config(sc, args):
+def workload_config(sc, args, name=None):
     g = sc.config.gravity
     P, M = mesh_sizes(sc)
     mw = g.grid_width * (2 if sc.config.bounded else 1)
     mh = g.grid_height * (2 if sc.config.bounded else 1)
     return {
-        "workload": args.workload, "n_bodies": sc.n,
+        "workload": name or args.workload, "n_bodies": sc.n,
         "grid": f"{g.grid_width}x{g.grid_height}", "fft_mesh": f"{mw}x{mh}",
         "boundary": "walls" if sc.config.bounded else "torus",
         "deposit": "int64" if sc.config.deposit_mode == 1 else "uint32",
@@ -384,38 +446,32 @@ def workload_config(sc, args):
     }
 
 
-def run_b200(args, ws, rank, local):
+def measure_steps(pipe, sc, args, stream, flush, dist, local, steps, warmup, sample_clocks):
+    """Device-timed steps (graphs replayed, state resident in HBM, L2 flushed
+    before each step), then the same steps with stage events, then the e2e
+    pass through the public API with page-locked host buffers."""
     import torch
 
-    from gravity_b200 import _abi
-    from gravity_b200.pipeline import GravityPipeline, PinnedArray, kernel_launches
+    from gravity_b200.pipeline import PinnedArray, kernel_launches
 
-    dist = init_dist(ws, local)
-    torch.cuda.set_device(local)
-    sc = make_workload(args.workload)
+    ws = dist.get_world_size() if dist else 1
     n = sc.n
-    pipe = GravityPipeline(sc.config)
-    stream = torch.cuda.ExternalStream(pipe.stream_handle())
-    flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device="cuda")
-
-    force_err = force_error_vs_fp64(pipe, sc) if rank == 0 else None
-
-    # ---- value: state resident in HBM, device-timed
     pipe.upload(sc.bodies, sc.materials)
     pipe.initialize_acceleration(n)
-    for _ in range(args.warmup):
+    for _ in range(warmup):
         pipe.step(n)
     pipe.synchronize()
     if dist:
         dist.barrier()
-    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
-    stops = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
-    clocks = ClockSampler(local)
-    clocks.start()
-    time.sleep(0.3)
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
+    stops = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
+    clocks = ClockSampler(local) if sample_clocks else None
+    if clocks:
+        clocks.start()
+        time.sleep(0.3)
     launches0 = kernel_launches()
     with torch.cuda.stream(stream):
-        for i in range(args.steps):
+        for i in range(steps):
             flush.zero_()
             starts[i].record(stream)
             pipe.step(n)
@@ -423,26 +479,25 @@ def run_b200(args, ws, rank, local):
     torch.cuda.synchronize()
     pipe.synchronize()
     launches = kernel_launches() - launches0
-    clk = clocks.stop()
+    clk = clocks.stop() if clocks else None
     total_ms = sum(a.elapsed_time(b) for a, b in zip(starts, stops))
     total_ms = allreduce_max(dist, total_ms)
     if dist:
         dist.barrier()
-    value = ws * n * args.steps / (total_ms / 1000.0)
-    ms_per_step = total_ms / args.steps
+    value = ws * n * steps / (total_ms / 1000.0)
 
     # ---- per-stage device time: the same steps with stage events recorded
     # (kernels launched one by one; the value pass above replays graphs).
     pipe.profile_enable(True)
     with torch.cuda.stream(stream):
-        for i in range(args.steps):
+        for i in range(steps):
             flush.zero_()
             pipe.step(n)
     stages = pipe.profile_read()
     pipe.profile_enable(False)
 
     # ---- e2e: through the public API with page-locked host buffers
-    e2e_steps = args.steps if args.e2e_steps is None else min(args.steps, args.e2e_steps)
+    e2e_steps = steps if args.e2e_steps is None else min(steps, args.e2e_steps)
     hb = PinnedArray((n, 4))
     hm = PinnedArray((n, 4))
     out = PinnedArray((n, 4))
@@ -450,7 +505,7 @@ def run_b200(args, ws, rank, local):
     hm.array[:] = sc.materials
     pipe.upload_n(n, hb.array, hm.array)
     pipe.initialize_acceleration(n)
-    for _ in range(min(args.warmup, 3)):
+    for _ in range(min(warmup, 3)):
         pipe.upload_n(n, hb.array)
         pipe.step(n)
         pipe.download_into(n, out.array)
@@ -470,6 +525,85 @@ def run_b200(args, ws, rank, local):
     e2e_value = ws * n * e2e_steps / e2e_s
     for a in (hb, hm, out):
         a.free()
+    # No bounded device wait may have given up during any of it.
+    timeouts = pipe.wait_timeouts()
+    if timeouts:
+        raise SystemExit(f"{timeouts} look-back wait(s) of the sort gave up: results invalid")
+    return {"value": value, "ms_per_step": total_ms / steps, "stages": stages,
+            "launches": launches, "clocks": clk,
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 16 * n,
+                    "d2h_bytes_per_step": 16 * n, "steps": e2e_steps}}
+
+
+def stage_table(sc, stages):
+    """Per-stage average launch time and achieved algorithmic GB/s."""
+    from gravity_b200.config import sort_axis_bits
+
+    P, M = mesh_sizes(sc)
+    cell_passes = radix_passes_for(P)
+    morton_bits = sort_axis_bits(sc.config.viewport_width) + sort_axis_bits(sc.config.viewport_height)
+    morton_passes = radix_passes_for_bits(morton_bits)
+    peak, _ = measured_peaks()
+    rows = {}
+    for name, (ms, cnt) in stages.items():
+        if cnt == 0:
+            continue
+        passes = morton_passes if name == "spatial_sort" else cell_passes
+        avg_ms = ms / cnt
+        b = stage_bytes(sc, name, passes)
+        gbs = b / (avg_ms / 1000.0) / 1e9 if avg_ms > 0 else None
+        rows[name] = {"ms_per_launch": avg_ms, "launches": cnt, "algorithmic_bytes": b,
+                      "gbs": gbs, "frac_of_measured_hbm": gbs / peak if gbs else None}
+    return rows
+
+
+def force_errors_by_form(sc, pipe_err):
+    """RMS force error against the FP64 direct sum on the same seeded
+    4096-body subsample (initial state) for this line's deposit form, the
+    other deposit form on the GPU, and the oracle's FP32 path (the
+    reference's uint32 deposit)."""
+    import oracle
+    from gravity_b200 import _abi
+    from gravity_b200.pipeline import GravityPipeline
+
+    n = sc.n
+    rng = np.random.default_rng(4096)
+    targets = np.sort(rng.choice(n, size=min(FORCE_SAMPLE, n), replace=False)).astype(np.int32)
+    other_mode = _abi.P3M_DEPOSIT_U32 if sc.config.deposit_mode == _abi.P3M_DEPOSIT_I64 else _abi.P3M_DEPOSIT_I64
+    names = {_abi.P3M_DEPOSIT_U32: "uint32", _abi.P3M_DEPOSIT_I64: "int64"}
+    out = {names[sc.config.deposit_mode]: pipe_err}
+    with GravityPipeline(sc.config.with_(deposit_mode=other_mode)) as other:
+        other.upload(sc.bodies, sc.materials)
+        other.initialize_acceleration(n)
+        a = other.acceleration(n)[targets].astype(np.float64)
+        ref = other.direct_accel_f64(n, targets)
+    out[names[other_mode]] = float(np.sqrt(np.sum((a - ref) ** 2) / np.sum(ref ** 2)))
+    ocfg = sc.config.with_(deposit_mode=_abi.P3M_DEPOSIT_U32)
+    with oracle.OracleSim(ocfg) as sim:
+        sim.upload(sc.bodies, sc.materials)
+        sim.initialize_acceleration(n)
+        a = sim.download(n)[2][targets].astype(np.float64)
+    out["oracle_fp32_uint32"] = float(np.sqrt(np.sum((a - ref) ** 2) / np.sum(ref ** 2)))
+    return out
+
+
+def run_b200(args, ws, rank, local):
+    import torch
+
+    from gravity_b200.pipeline import GravityPipeline
+
+    dist = init_dist(ws, local)
+    torch.cuda.set_device(local)
+    sc = make_workload(args.workload, args.bodies, args.grid)
+    n = sc.n
+    pipe = GravityPipeline(sc.config)
+    stream = torch.cuda.ExternalStream(pipe.stream_handle())
+    flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device="cuda")
+
+    force_err = force_error_vs_fp64(pipe, sc) if rank == 0 else None
+    m = measure_steps(pipe, sc, args, stream, flush, dist, local, args.steps, args.warmup, True)
+    value, ms_per_step, stages, launches, clk = (m["value"], m["ms_per_step"], m["stages"],
+                                                 m["launches"], m["clocks"])
 
     # ---- aim previews on the field of the last step (S/trajectory.comp):
     # one preview, then a fan of 256, 1024 steps each (host wall clock,
@@ -489,29 +623,35 @@ def run_b200(args, ws, rank, local):
         many = time.perf_counter() - t0
         previews = {"steps": 1024, "single_ms": 1000.0 * one, "fan": 256,
                     "fan_ms": 1000.0 * many, "preview_steps_per_s": 256 * 1024 / many}
+    pipe.close()
+
+    # ---- the plain configuration beside it: 400,000 Plummer bodies inside
+    # walls with the reference's uint32 deposit (a shorter run).
+    plain = None
+    if args.workload == "lattice_scale" and not args.no_plain:
+        psc = make_workload("plummer_walls")
+        ppipe = GravityPipeline(psc.config)
+        pstream = torch.cuda.ExternalStream(ppipe.stream_handle())
+        perr = force_error_vs_fp64(ppipe, psc) if rank == 0 else None
+        psteps = min(args.steps, 200)
+        pm = measure_steps(ppipe, psc, args, pstream, flush, dist, local, psteps,
+                           args.warmup, False)
+        ppipe.close()
+        if rank == 0:
+            prow = stage_table(psc, pm["stages"])
+            plain = {"workload": "plummer_walls", "config": workload_config(psc, args, "plummer_walls"),
+                     "value": pm["value"], "ms_per_step": pm["ms_per_step"], "steps": psteps,
+                     "e2e": pm["e2e"], "force_rms_err_vs_fp64": perr, "stages": prow,
+                     "gpu_launches": pm["launches"]}
 
     if rank == 0:
         peak, peak_kind = measured_peaks()
-        P, M = mesh_sizes(sc)
-        g = sc.config.gravity
-        cell_passes = radix_passes_for(P)
-        from gravity_b200.config import sort_axis_bits
-        morton_bits = sort_axis_bits(sc.config.viewport_width) + sort_axis_bits(sc.config.viewport_height)
-        morton_passes = radix_passes_for_bits(morton_bits)
-        stage_rows = {}
-        for name, (ms, cnt) in stages.items():
-            if cnt == 0:
-                continue
-            passes = morton_passes if name == "spatial_sort" else cell_passes
-            avg_ms = ms / cnt
-            b = stage_bytes(sc, name, passes)
-            stage_rows[name] = {"ms_per_launch": avg_ms, "launches": cnt,
-                                "algorithmic_bytes": b,
-                                "gbs": b / (avg_ms / 1000.0) / 1e9 if avg_ms > 0 else None}
+        stage_rows = stage_table(sc, stages)
         dominant = max(stage_rows, key=lambda k: stage_rows[k]["ms_per_launch"] * stage_rows[k]["launches"])
         dom = stage_rows[dominant]
         achieved = dom["gbs"]
         traffic = read_traffic(dominant, args.workload)
+        errors = force_errors_by_form(sc, force_err) if not args.no_form_errors else None
         cpu = None
         if not args.no_cpu_baseline:
             rate, steps, el, used = cpu_oracle_rate(sc, args.cpu_seconds, threads=os.cpu_count())
@@ -528,19 +668,21 @@ def run_b200(args, ws, rank, local):
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": workload_config(sc, args),
             "force_rms_err_vs_fp64": force_err,
+            "force_rms_err_vs_fp64_by_form": errors,
             "roofline": {"bound": "hbm", "kernel": dominant, "achieved": achieved, "peak": peak,
                          "unit": "GB/s", "frac": achieved / peak if achieved else None,
                          "traffic": traffic, "peak_source": peak_kind},
+            "roofline_hbm_stages": {k: stage_rows[k]["frac_of_measured_hbm"]
+                                    for k in ("deposit", "kick") if k in stage_rows},
             "stages": stage_rows,
             "cpu_baseline": cpu,
-            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 16 * n,
-                    "d2h_bytes_per_step": 16 * n, "steps": e2e_steps},
+            "e2e": m["e2e"],
             "gpu_launches": launches,
             "clocks": clk,
             "previews": previews,
+            "plain_form": plain,
         }
         print(json.dumps(line), flush=True)
-    pipe.close()
     if dist:
         dist.barrier()
         dist.destroy_process_group()
@@ -924,7 +1066,7 @@ def main():
     ap.add_argument("--steps", type=int, default=2000)
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
-    ap.add_argument("--workload", default="plummer_walls",
+    ap.add_argument("--workload", default="lattice_scale",
                     choices=["plummer_walls", "uniform_torus", "lattice_scale", "lattice_scale_u32",
                              "batch", "adjoint"])
     ap.add_argument("--fp64-check", action="store_true",
@@ -932,10 +1074,22 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=None)
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--bodies", type=int, default=None, help="override the workload's body count")
+    ap.add_argument("--grid", default=None, help="override the workload's grid, WxH")
+    ap.add_argument("--sims", type=int, default=None, help="batch: number of simulations")
+    ap.add_argument("--run-only", action="store_true",
+                    help="run the initial pass and --steps steps untimed (a profiler's target)")
+    ap.add_argument("--no-plain", action="store_true",
+                    help="lattice_scale: skip the 400k plummer_walls run beside it")
+    ap.add_argument("--no-form-errors", action="store_true",
+                    help="skip the force errors of the other deposit form and the oracle")
     args = ap.parse_args()
     if args.warmup < 3:
         raise SystemExit("--warmup must be >= 3")
     ws, rank, local = dist_env()
+    if args.run_only:
+        run_only(args)
+        return
     if args.impl == "reference":
         run_reference(args, ws, rank)
         return

@@ -122,6 +122,9 @@ SIGNATURES = {
     "p3m_host_free": (ctypes.c_int, [_vp]),
     "p3m_nonfinite_count": (ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_int64)]),
     "p3m_wait_timeouts": (ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_int64)]),
+    "p3m_set_lookback_fault": (ctypes.c_int, [_vp, _i32, _i32]),
+    "p3m_validate_fft": (ctypes.c_int, [_vp, _vp]),
+    "p3m_density_spectrum": (ctypes.c_int, [_vp, _vp, ctypes.c_size_t]),
     "p3m_direct_accel_f64": (ctypes.c_int, [_vp, _i32, _vp, _i32, _vp]),
     "p3m_diagnostics_f64": (ctypes.c_int, [_vp, _i32, _vp]),
     "p3m_batch_create": (ctypes.c_int, [ctypes.POINTER(P3MConfig), _i32, ctypes.POINTER(_vp)]),

@@ -216,6 +216,8 @@ void free_all(p3m_ctx* ctx) {
     ctx->free_events.clear();
     if (ctx->traj_scratch) cudaFree(ctx->traj_scratch);
     ctx->traj_scratch = nullptr;
+    if (ctx->status_host) cudaFreeHost(ctx->status_host);
+    ctx->status_host = nullptr;
     void* ptrs[] = {ctx->diag, ctx->bodies, ctx->bodies_alt, ctx->accel, ctx->accel_alt, ctx->materials,
                     ctx->materials_alt, ctx->destinations, ctx->status, ctx->keys, ctx->vals,
                     ctx->sort.keys_alt, ctx->sort.vals_alt, ctx->sort.hist, ctx->sort.block_sums,
@@ -259,6 +261,37 @@ int check_n(p3m_ctx* ctx, int n) {
     return P3M_OK;
 }
 
+// Queues a copy of the device status words into status_host; read it with
+// device_failures() once the stream is synchronised.
+cudaError_t queue_status_read(p3m_ctx* ctx) {
+    return cudaMemcpyAsync(ctx->status_host, ctx->status, 2 * sizeof(unsigned int),
+                           cudaMemcpyDeviceToHost, ctx->stream);
+}
+
+// Failures the device detected since the last report, from status_host
+// (queue_status_read and a stream synchronisation first): a bounded look-back
+// wait that gave up (P3M_ERR_TIMEOUT; every result computed since is
+// untrustworthy), then, when `nonfinite` is set, bodies that became non-finite
+// (P3M_ERR_NON_FINITE). Each is reported once.
+int device_failures(p3m_ctx* ctx, bool nonfinite) {
+    const unsigned int waits = ctx->status_host[1];
+    const unsigned int bad = ctx->status_host[0];
+    if (waits != ctx->reported_timeouts) {
+        const unsigned int grown = waits - ctx->reported_timeouts;
+        ctx->reported_timeouts = waits;
+        return fail(ctx, P3M_ERR_TIMEOUT,
+                    std::to_string(grown) + " bounded look-back wait(s) of a sort gave up; "
+                    "the cell lists and everything computed from them since are invalid");
+    }
+    if (nonfinite && bad != ctx->reported_nonfinite) {
+        const unsigned int grown = bad - ctx->reported_nonfinite;
+        ctx->reported_nonfinite = bad;
+        return fail(ctx, P3M_ERR_NON_FINITE,
+                    std::to_string(grown) + " non-finite body state(s) seen by the drift");
+    }
+    return P3M_OK;
+}
+
 // Cell lists from keys already written in descending ID order.
 // totals_ready: radix_sort_prepare ran and the keys' producer (the drift)
 // added their digit totals.
@@ -267,8 +300,9 @@ int lists_from_keys(p3m_ctx* ctx, int n, bool totals_ready = false) {
     const long long P = (long long)phys_cells(ctx);
     uint32_t* sk = ctx->keys;
     uint32_t* sv = ctx->vals;
+    const uint32_t* failed = nullptr;
     P3M_CUDA(ctx, p3m::radix_sort_pairs(ctx->keys, ctx->vals, ctx->sort, n, bits_for(P),
-                                        ctx->stream, &sk, &sv, totals_ready));
+                                        ctx->stream, &sk, &sv, totals_ready, &failed));
     ctx->sorted_keys = sk;
     ctx->sorted_ids = sv;
     // Counts and masses are one block (cell_mass follows cell_count): one clear.
@@ -276,7 +310,7 @@ int lists_from_keys(p3m_ctx* ctx, int n, bool totals_ready = false) {
     P3M_CUDA(ctx, p3m::launch_cell_build(sk, sv, n, ctx->bodies, ctx->materials, ctx->cell_start,
                                          ctx->cell_count, ctx->cell_mass, ctx->entries,
                                          p3m::deposit_uses_cell_starts(n) ? (int)P : 0,
-                                         ctx->stream));
+                                         ctx->stream, failed));
     return P3M_OK;
 }
 
@@ -382,11 +416,12 @@ int sort_bodies(p3m_ctx* ctx, int n) {
                                           ctx->keys, ctx->vals, ctx->stream, totals));
     uint32_t* sk = ctx->keys;
     uint32_t* sv = ctx->vals;
+    const uint32_t* failed = nullptr;
     P3M_CUDA(ctx, p3m::radix_sort_pairs(ctx->keys, ctx->vals, ctx->sort, n, key_bits, ctx->stream,
-                                        &sk, &sv, totals.totals != nullptr));
+                                        &sk, &sv, totals.totals != nullptr, &failed));
     P3M_CUDA(ctx, p3m::launch_permute(sv, n, ctx->bodies, ctx->accel, ctx->materials,
                                       ctx->bodies_alt, ctx->accel_alt, ctx->materials_alt,
-                                      ctx->destinations, ctx->stream));
+                                      ctx->destinations, ctx->stream, failed));
     // Slots beyond n (capacity reserved for bodies a caller adds later) keep
     // their contents: carry them into the buffers that become current.
     const size_t tail = (size_t)ctx->cfg.capacity - (size_t)n;
@@ -661,6 +696,19 @@ int p3m_create(const p3m_config* config, p3m_ctx** out) {
     ALLOC(ctx->destinations, cap);
     ALLOC(ctx->status, 4);  // [0] non-finite bodies, [1] look-back waits that gave up
     ctx->sort.wait_timeouts = ctx->status + 1;
+    {
+        cudaError_t he = cudaHostAlloc((void**)&ctx->status_host, 4 * sizeof(unsigned int),
+                                       cudaHostAllocDefault);
+        if (he != cudaSuccess) {
+            ctx->status_host = nullptr;
+            fail_cuda(ctx, "cudaHostAlloc(status_host)", he);
+            g_create_error = ctx->last_error;
+            free_all(ctx);
+            cudaStreamDestroy(ctx->stream);
+            delete ctx;
+            return he == cudaErrorMemoryAllocation ? P3M_ERR_OUT_OF_MEMORY : P3M_ERR_CUDA;
+        }
+    }
     ALLOC(ctx->keys, cap);
     ALLOC(ctx->vals, cap);
     ALLOC(ctx->sort.keys_alt, cap);
@@ -775,8 +823,10 @@ int p3m_download_state(p3m_ctx* ctx, float* bodies4, float* materials4, float* a
         P3M_CUDA(ctx, cudaMemcpyAsync(materials4, ctx->materials, (size_t)n * 16, cudaMemcpyDefault, ctx->stream));
     if (acceleration2)
         P3M_CUDA(ctx, cudaMemcpyAsync(acceleration2, ctx->accel, (size_t)n * 8, cudaMemcpyDefault, ctx->stream));
+    P3M_CUDA(ctx, queue_status_read(ctx));
     P3M_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
-    return P3M_OK;
+    // The arrays are written; a sort whose wait gave up made them invalid.
+    return device_failures(ctx, false);
 }
 
 int p3m_debug_get(p3m_ctx* ctx, int32_t which, void* host, size_t bytes) {
@@ -892,7 +942,20 @@ int p3m_apply_kick(p3m_ctx* ctx, int32_t n, int32_t initial) {
 
 int p3m_synchronize(p3m_ctx* ctx) {
     if (!ctx) return P3M_ERR_INVALID_ARGUMENT;
+    P3M_CUDA(ctx, queue_status_read(ctx));
     P3M_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    return device_failures(ctx, true);
+}
+
+int p3m_set_lookback_fault(p3m_ctx* ctx, int32_t poll_limit, int32_t withheld_tile) {
+    if (!ctx) return P3M_ERR_INVALID_ARGUMENT;
+    if (poll_limit < 1) return fail(ctx, P3M_ERR_INVALID_ARGUMENT, "poll_limit must be >= 1");
+    if (withheld_tile < -1) return fail(ctx, P3M_ERR_INVALID_ARGUMENT, "withheld_tile must be >= -1");
+    // Captured steps bake the sort's launch arguments in: capture anew.
+    P3M_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    drop_graphs(ctx);
+    ctx->sort.poll_limit = poll_limit;
+    ctx->sort.withhold_tile = withheld_tile;
     return P3M_OK;
 }
 
@@ -954,20 +1017,95 @@ int p3m_host_free(void* host) {
 
 int p3m_nonfinite_count(p3m_ctx* ctx, int64_t* count) {
     if (!ctx || !count) return P3M_ERR_INVALID_ARGUMENT;
-    unsigned int v = 0;
-    P3M_CUDA(ctx, cudaMemcpyAsync(&v, ctx->status, sizeof(v), cudaMemcpyDeviceToHost, ctx->stream));
+    P3M_CUDA(ctx, queue_status_read(ctx));
     P3M_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
-    *count = (int64_t)v;
+    *count = (int64_t)ctx->status_host[0];
     return P3M_OK;
 }
 
 int p3m_wait_timeouts(p3m_ctx* ctx, int64_t* count) {
     if (!ctx || !count) return P3M_ERR_INVALID_ARGUMENT;
-    unsigned int v = 0;
-    P3M_CUDA(ctx, cudaMemcpyAsync(&v, ctx->status + 1, sizeof(v), cudaMemcpyDeviceToHost,
-                                  ctx->stream));
+    P3M_CUDA(ctx, queue_status_read(ctx));
     P3M_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
-    *count = (int64_t)v;
+    *count = (int64_t)ctx->status_host[1];
+    return P3M_OK;
+}
+
+// The FP32 half spectrum of the last force build, column-transformed into a
+// work copy (the force path never stores it: its column pass multiplies by
+// the Green's table and inverts in shared memory).
+namespace {
+int float_spectrum(p3m_ctx* ctx, std::vector<float2>* out) {
+    if (ctx->built_n < 0) return fail(ctx, P3M_ERR_STATE, "no force build yet");
+    const size_t cells = half_cells(ctx);
+    float2* work = nullptr;
+    P3M_CUDA(ctx, cudaMallocAsync((void**)&work, cells * sizeof(float2), ctx->stream));
+    cudaError_t e = cudaMemcpyAsync(work, ctx->half, cells * sizeof(float2),
+                                    cudaMemcpyDeviceToDevice, ctx->stream);
+    if (e == cudaSuccess) e = p3m::launch_fft_forward_columns(work, ctx->grid, ctx->twiddles, ctx->stream);
+    out->resize(cells);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(out->data(), work, cells * sizeof(float2), cudaMemcpyDeviceToHost,
+                            ctx->stream);
+    cudaFreeAsync(work, ctx->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    if (e != cudaSuccess) return fail_cuda(ctx, "density spectrum", e);
+    return P3M_OK;
+}
+}  // namespace
+
+int p3m_density_spectrum(p3m_ctx* ctx, float* spectrum2, size_t bytes) {
+    if (!ctx || !spectrum2) return P3M_ERR_INVALID_ARGUMENT;
+    if (bytes < half_cells(ctx) * sizeof(float2))
+        return fail(ctx, P3M_ERR_INVALID_ARGUMENT, "spectrum needs (MW/2+1)*MH float2 values");
+    std::vector<float2> spec;
+    const int st = float_spectrum(ctx, &spec);
+    if (st != P3M_OK) return st;
+    std::memcpy(spectrum2, spec.data(), spec.size() * sizeof(float2));
+    return P3M_OK;
+}
+
+int p3m_validate_fft(p3m_ctx* ctx, double* out3) {
+    if (!ctx || !out3) return P3M_ERR_INVALID_ARGUMENT;
+    // GravityPipeline.kt:379: check(!bounded).
+    if (ctx->bounded) return fail(ctx, P3M_ERR_STATE, "FFT validation covers the periodic mesh only");
+    std::vector<float2> spec;
+    int st = float_spectrum(ctx, &spec);
+    if (st != P3M_OK) return st;
+    const int MW = ctx->grid.MW, MH = ctx->grid.MH, SW = MW / 2 + 1;
+    // GravityPipeline.kt:1546-1547 / :390: the density over massScale (the
+    // int64 form: over 2^32), in FP64.
+    const double inv_scale = ctx->cfg.deposit_mode == P3M_DEPOSIT_I64
+                                 ? 1.0 / 4294967296.0
+                                 : 1.0 / (double)ctx->mass_scale;
+    double2* z = nullptr;
+    P3M_CUDA(ctx, cudaMallocAsync((void**)&z, mesh_cells(ctx) * sizeof(double2), ctx->stream));
+    std::vector<double2> ref(mesh_cells(ctx));
+    cudaError_t e = p3m::launch_density_spectrum_f64(ctx->density, ctx->cfg.deposit_mode,
+                                                     inv_scale, ctx->grid, z, ctx->stream);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(ref.data(), z, ref.size() * sizeof(double2), cudaMemcpyDeviceToHost,
+                            ctx->stream);
+    cudaFreeAsync(z, ctx->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    if (e != cudaSuccess) return fail_cuda(ctx, "p3m_validate_fft", e);
+    // GravityPipeline.kt:404-418 over all 2*MW*MH components; columns
+    // 1..MW/2-1 of the half spectrum stand for themselves and their mirror.
+    double max_abs = 0.0, max_ref = 0.0, sq = 0.0;
+    for (int ky = 0; ky < MH; ++ky) {
+        for (int kx = 0; kx < SW; ++kx) {
+            const double2 r = ref[(size_t)ky * MW + kx];
+            const float2 v = spec[(size_t)ky * SW + kx];
+            const double ex = std::fabs(r.x - (double)v.x), ey = std::fabs(r.y - (double)v.y);
+            const double w = (kx == 0 || 2 * kx == MW) ? 1.0 : 2.0;
+            max_abs = std::max(max_abs, std::max(ex, ey));
+            max_ref = std::max(max_ref, std::max(std::fabs(r.x), std::fabs(r.y)));
+            sq += w * (ex * ex + ey * ey);
+        }
+    }
+    out3[0] = max_abs;
+    out3[1] = max_abs / std::max(max_ref, 1e-30);
+    out3[2] = std::sqrt(sq / (2.0 * (double)MW * (double)MH));
     return P3M_OK;
 }
 

@@ -615,6 +615,18 @@ __global__ void green_final_kernel(const double2* z, int MW, int MH, double wind
     green[id] = make_float2((float)(v.y * scale), (float)(-v.x * scale));
 }
 
+// The density mesh as FP64 complex values (count / massScale, 0): the input
+// of validateFft's double-precision transform (GravityPipeline.kt:386-393).
+// The integer counts convert exactly; one FP64 product follows.
+__global__ void density_f64_kernel(const void* __restrict__ density, int i64, double inv_scale,
+                                   long long M, double2* __restrict__ z) {
+    const long long id = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (id >= M) return;
+    const double v = i64 ? (double)static_cast<const long long*>(density)[id]
+                         : (double)static_cast<const uint32_t*>(density)[id];
+    z[id] = make_double2(v * inv_scale, 0.0);
+}
+
 inline int ilog2_host(int v) {
     int b = 0;
     while ((1 << (b + 1)) <= v) ++b;
@@ -823,6 +835,17 @@ cudaError_t launch_fft_inverse_rows(const float4* cols, GridShape g, const float
     launch_chained(fft_rows_inverse_kernel, blocks, threads, smem, stream, cols, g.MW, g.MH, rows_per_cta,
                                                            twiddles, force);
     count_launches(1);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_density_spectrum_f64(const void* density, int deposit_mode, double inv_scale,
+                                        GridShape g, double2* z, cudaStream_t stream) {
+    const long long M = (long long)g.MW * g.MH;
+    density_f64_kernel<<<(int)((M + 255) / 256), 256, 0, stream>>>(
+        density, deposit_mode == P3M_DEPOSIT_I64 ? 1 : 0, inv_scale, M, z);
+    fft64_line_kernel<<<g.MH, 256, (size_t)g.MW * sizeof(double2), stream>>>(z, g.MW, g.MH, 0);
+    fft64_line_kernel<<<g.MW, 256, (size_t)g.MH * sizeof(double2), stream>>>(z, g.MW, g.MH, 1);
+    count_launches(3);
     return cudaGetLastError();
 }
 

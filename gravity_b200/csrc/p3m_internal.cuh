@@ -86,6 +86,12 @@ struct SortScratch {
     uint32_t* lookback = nullptr;
     unsigned int* wait_timeouts = nullptr;
     int capacity = 0;
+    // Polls of one look-back word before a wait gives up, and the tile whose
+    // counts are never published (-1: none). Only the timeout test changes
+    // them (p3m_set_lookback_fault): a withheld tile makes its successor's
+    // wait run out, as a tile that never arrives would.
+    int poll_limit = 200000;
+    int withhold_tile = -1;
 };
 
 size_t sort_hist_entries(int capacity);
@@ -137,9 +143,14 @@ __device__ __forceinline__ void add_digit_totals(const SortTotals& st, bool vali
 // synchronisation.
 // totals_ready: radix_sort_prepare ran for this sort and the keys' producer
 // added the digit totals.
+// failed (may be null): set to the device word that this sort sets to 1 when
+// one of its bounded look-back waits gave up (its output is then not a
+// permutation of its input), or to null when the sort has no waits. The
+// consumers of the result check it (launch_cell_build, launch_permute).
 cudaError_t radix_sort_pairs(uint32_t* keys, uint32_t* vals, const SortScratch& s, int n,
                              int key_bits, cudaStream_t stream, uint32_t** out_keys,
-                             uint32_t** out_vals, bool totals_ready = false);
+                             uint32_t** out_vals, bool totals_ready = false,
+                             const uint32_t** failed = nullptr);
 
 // Exclusive scan of n uint32 in place (n <= 4096 * 4096).
 cudaError_t exclusive_scan_u32(uint32_t* data, int n, uint32_t* block_sums,
@@ -169,17 +180,23 @@ cudaError_t launch_morton_keys(const float4* bodies, int n, int wbits, int hbits
                                uint32_t* keys, uint32_t* vals, cudaStream_t stream,
                                SortTotals totals = SortTotals());
 // Permutation of the Morton reorder (spatial_sort_scatter / _materials.comp).
+// When *sort_failed is set (the sort's look-back gave up) the bodies are
+// copied in place order instead, so no index taken from the sort is used.
 cudaError_t launch_permute(const uint32_t* order, int n, const float4* bodies, const float2* accel,
                            const float4* materials, float4* bodies_out, float2* accel_out,
-                           float4* materials_out, uint32_t* destinations, cudaStream_t stream);
+                           float4* materials_out, uint32_t* destinations, cudaStream_t stream,
+                           const uint32_t* sort_failed = nullptr);
 // Cell lists from sorted keys: start, count, mass; gathers entries. With
 // fill_cells = P > 0, cell_start (P + 1 entries) becomes a full CSR: an empty
 // cell starts where the next occupied one does and cell_start[P] = n;
-// otherwise only occupied cells are written.
+// otherwise only occupied cells are written. When *sort_failed is set (the
+// sort's look-back gave up) nothing is written: the cleared counts leave
+// every cell empty, and no key or ID from the sort is used as an index.
 cudaError_t launch_cell_build(const uint32_t* keys, const uint32_t* ids, int n,
                               const float4* bodies, const float4* materials, int* cell_start,
                               int* cell_count, uint32_t* cell_mass, float4* entries,
-                              int fill_cells, cudaStream_t stream);
+                              int fill_cells, cudaStream_t stream,
+                              const uint32_t* sort_failed = nullptr);
 
 // CIC deposit (build_grid.comp:53-69) over cell-ordered entries (keys: their
 // sorted cells; cell_start: the full CSR). Writes every mesh cell.
@@ -201,6 +218,10 @@ cudaError_t launch_fft_columns(const float2* half, const float2* green, float in
                                cudaStream_t stream);
 cudaError_t launch_fft_inverse_rows(const float4* cols, GridShape g, const float2* twiddles,
                                     float2* force, cudaStream_t stream);
+// FP64 forward 2D FFT (radix-2, exact sincospi twiddles) of the density mesh
+// scaled by inv_scale, into z (MW x MH double2): validateFft's reference.
+cudaError_t launch_density_spectrum_f64(const void* density, int deposit_mode, double inv_scale,
+                                        GridShape g, double2* z, cudaStream_t stream);
 // Forward spectrum only (diagnostic): half-spectrum columns transformed.
 cudaError_t launch_fft_forward_columns(float2* half, GridShape g, const float2* twiddles,
                                        cudaStream_t stream);
@@ -485,6 +506,10 @@ struct p3m_ctx {
     float4* materials_alt = nullptr;
     uint32_t* destinations = nullptr;
     unsigned int* status = nullptr;  // [0] non-finite bodies seen by the drift
+    // Page-locked copy of status[0..1], read at the synchronising entry
+    // points, and the counts already reported to the caller.
+    unsigned int* status_host = nullptr;
+    unsigned int reported_nonfinite = 0, reported_timeouts = 0;
 
     // cell lists
     uint32_t* keys = nullptr;

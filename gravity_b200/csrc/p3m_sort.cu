@@ -1,4 +1,4 @@
-// p3m_sort.cu — cell keys, 64-bit-key radix sort, cell lists, Morton reorder.
+// p3m_sort.cu — cell keys, their stable radix sort, cell lists, Morton reorder.
 //
 // Replaces the home-cell linked lists of build_grid.comp:71-75 and the
 // spatial reorder of spatial_sort_{count,scan,scatter,materials}.comp
@@ -162,8 +162,10 @@ constexpr uint32_t kLookbackAggregate = 1u << 30;
 constexpr uint32_t kLookbackInclusive = 2u << 30;
 constexpr uint32_t kLookbackValue = (1u << 30) - 1u;
 constexpr int kLookbackWindow = 16;    // predecessors read per round trip
-constexpr int kLookbackSpins = 200000; // polls of one word before giving up
 constexpr int kLookbackHeader = kSortMaxPasses * kLookbackMaxRadix + 32;  // totals + counters
+// Header word set to 1 when a wait of this sort gave up (cleared with the
+// header at the start of every look-back sort).
+constexpr int kLookbackFailedWord = kSortMaxPasses * kLookbackMaxRadix + 16;
 
 __device__ __forceinline__ uint32_t load_relaxed(const uint32_t* p) {
     uint32_t v;
@@ -179,11 +181,13 @@ __device__ __forceinline__ void store_relaxed(uint32_t* p, uint32_t v) {
 // tiles before this one (in the order they took their indices) publish their
 // counts; the sum back to the first inclusive prefix is this tile's offset.
 // Every tile waited on took its index earlier, so it is running and will
-// publish; each wait is still bounded (kLookbackSpins polls), after which it
-// is counted in `timeouts` and taken as 0 so that the kernel always ends.
-// `status` rows are kLookbackMaxRadix words per tile.
+// publish; each wait is still bounded (`poll_limit` polls, 200,000 unless a
+// test lowers it), after which it is counted in `timeouts` and taken as 0 so
+// that the kernel always ends. `status` rows are kLookbackMaxRadix words per
+// tile.
 __device__ __forceinline__ uint32_t lookback_exclusive(const uint32_t* status, int tile, int d,
-                                                       unsigned int* timeouts) {
+                                                       unsigned int* timeouts, int poll_limit,
+                                                       uint32_t* failed) {
     uint32_t excl = 0;
     int j = tile - 1;
     while (j >= 0) {
@@ -198,8 +202,9 @@ __device__ __forceinline__ uint32_t lookback_exclusive(const uint32_t* status, i
             uint32_t v = w[i];
             int spins = 0;
             while ((v & ~kLookbackValue) == 0) {
-                if (++spins > kLookbackSpins) {
+                if (++spins > poll_limit) {
                     atomicAdd(timeouts, 1u);
+                    store_relaxed(failed, 1u);
                     v = kLookbackInclusive;
                     break;
                 }
@@ -230,7 +235,8 @@ __device__ __forceinline__ void radix_scatter_body(
     int tile, const uint32_t* __restrict__ keys_in, const uint32_t* __restrict__ vals_in,
     uint32_t* __restrict__ keys_out, uint32_t* __restrict__ vals_out, int n, int shift, int bits,
     int tiles, const uint32_t* __restrict__ hist_scanned, uint32_t* counter = nullptr,
-    uint32_t* status = nullptr, unsigned int* timeouts = nullptr) {
+    uint32_t* status = nullptr, unsigned int* timeouts = nullptr, int poll_limit = 0,
+    int withhold_tile = -1, uint32_t* failed = nullptr) {
     constexpr int kWarps = THREADS / 32;
     constexpr int kTile = THREADS * ITEMS;
     static_assert(kTile == kSortTile, "tiles hold kSortTile keys");
@@ -294,7 +300,7 @@ __device__ __forceinline__ void radix_scatter_body(
                 warp_hist[w * radix + d] = count[q];
                 count[q] += t;
             }
-            if (LOOKBACK)  // publish this tile's count at once, so successors can go on
+            if (LOOKBACK && tile != withhold_tile)  // publish at once, so successors go on
                 store_relaxed(&status[(size_t)tile * kLookbackMaxRadix + d],
                               (tile == 0 ? kLookbackInclusive : kLookbackAggregate) | count[q]);
             else
@@ -318,8 +324,9 @@ __device__ __forceinline__ void radix_scatter_body(
         for (int q = 0; q < kPer; ++q) {
             const int d = threadIdx.x * kPer + q;
             if (d < radix) {
-                const uint32_t before = lookback_exclusive(status, tile, d, timeouts);
-                if (tile > 0)
+                const uint32_t before =
+                    lookback_exclusive(status, tile, d, timeouts, poll_limit, failed);
+                if (tile > 0 && tile != withhold_tile)
                     store_relaxed(&status[(size_t)tile * kLookbackMaxRadix + d],
                                   kLookbackInclusive | (before + count[q]));
                 out_base[d] = digit_start + before;
@@ -390,11 +397,11 @@ __global__ void __launch_bounds__(kLookbackThreads) lookback_scatter_kernel(
     const uint32_t* __restrict__ keys_in, const uint32_t* __restrict__ vals_in,
     uint32_t* __restrict__ keys_out, uint32_t* __restrict__ vals_out, int n, int shift, int bits,
     int tiles, const uint32_t* __restrict__ totals, uint32_t* counter, uint32_t* status,
-    unsigned int* timeouts) {
+    unsigned int* timeouts, int poll_limit, int withhold_tile, uint32_t* failed) {
     grid_dependency_wait();
     radix_scatter_body<true, MAXR, kLookbackThreads, kLookbackItems>(
         0, keys_in, vals_in, keys_out, vals_out, n, shift, bits, tiles, totals, counter, status,
-        timeouts);
+        timeouts, poll_limit, withhold_tile, failed);
 }
 
 // Digit totals of every pass in one read of the keys: per-CTA shared counts
@@ -542,10 +549,11 @@ __device__ __forceinline__ void permute_body(int block, const uint32_t* __restri
                                              const float2* __restrict__ accel,
                                              const float4* __restrict__ materials,
                                              float4* bodies_out, float2* accel_out,
-                                             float4* materials_out, uint32_t* destinations) {
+                                             float4* materials_out, uint32_t* destinations,
+                                             bool identity = false) {
     const int t = block * blockDim.x + threadIdx.x;
     if (t >= n) return;
-    const uint32_t src = order[t];
+    const uint32_t src = identity ? (uint32_t)t : order[t];
     bodies_out[t] = bodies[src];
     accel_out[t] = accel[src];
     materials_out[t] = materials[src];
@@ -555,10 +563,12 @@ __device__ __forceinline__ void permute_body(int block, const uint32_t* __restri
 __global__ void permute_kernel(const uint32_t* __restrict__ order, int n,
                                const float4* __restrict__ bodies, const float2* __restrict__ accel,
                                const float4* __restrict__ materials, float4* bodies_out,
-                               float2* accel_out, float4* materials_out, uint32_t* destinations) {
+                               float2* accel_out, float4* materials_out, uint32_t* destinations,
+                               const uint32_t* __restrict__ sort_failed) {
     grid_dependency_wait();
+    const bool identity = sort_failed != nullptr && *sort_failed != 0u;
     permute_body(blockIdx.x, order, n, bodies, accel, materials, bodies_out, accel_out,
-                 materials_out, destinations);
+                 materials_out, destinations, identity);
 }
 
 // Cell lists from the sorted keys. Run starts write cell_start; counts and
@@ -639,8 +649,11 @@ __global__ void cell_build_kernel(const uint32_t* __restrict__ keys, const uint3
                                   int n, const float4* __restrict__ bodies,
                                   const float4* __restrict__ materials, int* cell_start,
                                   int* cell_count, uint32_t* cell_mass, float4* entries,
-                                  int fill_cells) {
+                                  int fill_cells, const uint32_t* __restrict__ sort_failed) {
     grid_dependency_wait();
+    // A sort whose look-back gave up leaves keys and IDs that are not a
+    // permutation: build nothing (every cell stays empty).
+    if (sort_failed != nullptr && *sort_failed != 0u) return;
     cell_build_body(blockIdx.x, keys, ids, n, bodies, materials, cell_start, cell_count, cell_mass,
                     entries, fill_cells);
 }
@@ -784,9 +797,10 @@ cudaError_t radix_sort_prepare(const SortScratch& s, int n, int key_bits, cudaSt
 
 cudaError_t radix_sort_pairs(uint32_t* keys, uint32_t* vals, const SortScratch& s, int n,
                              int key_bits, cudaStream_t stream, uint32_t** out_keys,
-                             uint32_t** out_vals, bool totals_ready) {
+                             uint32_t** out_vals, bool totals_ready, const uint32_t** failed) {
     *out_keys = keys;
     *out_vals = vals;
+    if (failed) *failed = nullptr;
     if (n <= 1 || key_bits <= 0) return cudaSuccess;
     if (n > s.capacity) return cudaErrorInvalidValue;
     const int passes = (key_bits + 7) / 8;
@@ -798,6 +812,8 @@ cudaError_t radix_sort_pairs(uint32_t* keys, uint32_t* vals, const SortScratch& 
     uint32_t* vout = s.vals_alt;
     int lb_passes, lb_bits;
     if (lookback_plan(s, n, key_bits, &lb_passes, &lb_bits)) {
+        uint32_t* failed_word = s.lookback + kLookbackFailedWord;
+        if (failed) *failed = failed_word;
         // One kernel per pass: the digit totals of all passes first (here, or
         // by the keys' producer after radix_sort_prepare), then each pass's
         // tiles find their offsets by look-back.
@@ -819,11 +835,11 @@ cudaError_t radix_sort_pairs(uint32_t* keys, uint32_t* vals, const SortScratch& 
             if (pbits > 8)
                 launch_chained(lookback_scatter_kernel<512>, tiles, kLookbackThreads, 0, stream,
                     kin, vin, kout, vout, n, shift, pbits, tiles, totals, counter, status,
-                    s.wait_timeouts);
+                    s.wait_timeouts, s.poll_limit, s.withhold_tile, failed_word);
             else
                 launch_chained(lookback_scatter_kernel<256>, tiles, kLookbackThreads, 0, stream,
                     kin, vin, kout, vout, n, shift, pbits, tiles, totals, counter, status,
-                    s.wait_timeouts);
+                    s.wait_timeouts, s.poll_limit, s.withhold_tile, failed_word);
             count_launches(1);
             uint32_t* tk = kin; kin = kout; kout = tk;
             uint32_t* tv = vin; vin = vout; vout = tv;
@@ -868,11 +884,12 @@ cudaError_t launch_morton_keys(const float4* bodies, int n, int wbits, int hbits
 
 cudaError_t launch_permute(const uint32_t* order, int n, const float4* bodies, const float2* accel,
                            const float4* materials, float4* bodies_out, float2* accel_out,
-                           float4* materials_out, uint32_t* destinations, cudaStream_t stream) {
+                           float4* materials_out, uint32_t* destinations, cudaStream_t stream,
+                           const uint32_t* sort_failed) {
     if (n <= 0) return cudaSuccess;
     launch_chained(permute_kernel, blocks_for(n, 256), 256, 0, stream, order, n, bodies, accel, materials,
                                                            bodies_out, accel_out, materials_out,
-                                                           destinations);
+                                                           destinations, sort_failed);
     count_launches(1);
     return cudaGetLastError();
 }
@@ -899,7 +916,7 @@ P3M_BATCHED(batched_zero, ZeroArgs, zero_batched_kernel, kBatchThreads)
 cudaError_t launch_cell_build(const uint32_t* keys, const uint32_t* ids, int n, const float4* bodies,
                               const float4* materials, int* cell_start, int* cell_count,
                               uint32_t* cell_mass, float4* entries, int fill_cells,
-                              cudaStream_t stream) {
+                              cudaStream_t stream, const uint32_t* sort_failed) {
     if (n <= 0) {
         if (fill_cells > 0)
             return cudaMemsetAsync(cell_start, 0, ((size_t)fill_cells + 1) * sizeof(int), stream);
@@ -907,7 +924,7 @@ cudaError_t launch_cell_build(const uint32_t* keys, const uint32_t* ids, int n, 
     }
     launch_chained(cell_build_kernel, blocks_for(n, 256), 256, 0, stream, keys, ids, n, bodies, materials,
                                                               cell_start, cell_count, cell_mass,
-                                                              entries, fill_cells);
+                                                              entries, fill_cells, sort_failed);
     count_launches(1);
     return cudaGetLastError();
 }

@@ -209,8 +209,9 @@ __global__ void __launch_bounds__(32 * kWarpsPerBlock) trajectory_kernel(
         float2 half = make_float2(vel.x + acc.x * (0.5f * dt), vel.y + acc.y * (0.5f * dt));
         float2 delta = make_float2(half.x * dt, half.y * dt);
         if (P.k.bounded != 0) {
-            // Walls act like body contacts: the normal motion stops, and
-            // rebounds by the restitution coefficient.
+            // A wall is treated as a contact: the velocity component into
+            // the wall is reflected and scaled by the restitution
+            // coefficient (0 stops it).
             const float nx = pos.x + delta.x, ny = pos.y + delta.y;
             const float cx = fminf(fmaxf(nx, 0.0f), kMaximumUnit);
             const float cy = fminf(fmaxf(ny, 0.0f), kMaximumUnit);

@@ -280,6 +280,27 @@ class GravityPipeline:
         self._check(self._lib.p3m_wait_timeouts(self._ctx, ctypes.byref(c)))
         return c.value
 
+    def set_lookback_fault(self, poll_limit: int = 200_000, withheld_tile: int = -1) -> None:
+        """Test hook of the timeout path: a poll limit for the sort's look-back
+        waits and a tile whose counts are never published (-1: none)."""
+        self._check(self._lib.p3m_set_lookback_fault(self._ctx, int(poll_limit), int(withheld_tile)))
+
+    def validate_fft(self) -> dict:
+        """validateFft (GravityPipeline.kt:378-419): the FP32 density spectrum
+        of the last force build against an FP64 transform of the same mesh."""
+        out = np.zeros(3, np.float64)
+        self._check(self._lib.p3m_validate_fft(self._ctx, _ptr(out)))
+        return {"maximum_absolute_error": float(out[0]), "maximum_relative_error": float(out[1]),
+                "root_mean_square_error": float(out[2])}
+
+    def density_spectrum(self) -> np.ndarray:
+        """FP32 spectrum of density / massScale of the last force build:
+        (MH, MW/2+1) complex64, numpy.fft.rfft2's layout."""
+        mw, mh = self.mesh_shape
+        out = np.empty((mh, mw // 2 + 1), np.complex64)
+        self._check(self._lib.p3m_density_spectrum(self._ctx, _ptr(out), out.nbytes))
+        return out
+
     def direct_accel_f64(self, n: int, targets) -> np.ndarray:
         """FP64 direct-sum accelerations (unit/s^2) of the target bodies."""
         t = np.ascontiguousarray(targets, np.int32)

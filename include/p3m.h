@@ -138,7 +138,9 @@ int p3m_upload_state(p3m_ctx* ctx, const float* bodies4, const float* materials4
  * contents across steps and reorders. */
 int p3m_upload_range(p3m_ctx* ctx, int32_t first, int32_t count, const float* bodies4,
                      const float* materials4, const float* acceleration2);
-/* Readback (the reference maps the SSBOs: GravityPipeline.kt:378-443). */
+/* Readback (the reference maps the SSBOs: GravityPipeline.kt:378-443).
+ * Returns P3M_ERR_TIMEOUT, after writing the arrays, when a bounded
+ * look-back wait gave up since the last report (see p3m_synchronize). */
 int p3m_download_state(p3m_ctx* ctx, float* bodies4, float* materials4,
                        float* acceleration2, int32_t n);
 /* Copy the first `bytes` of a buffer to host memory (at most its size). */
@@ -173,8 +175,10 @@ int p3m_sort_bodies(p3m_ctx* ctx, int32_t n);                   /* sortBodies, :
 int p3m_drift(p3m_ctx* ctx, int32_t n, float kick_dt, float drift_dt); /* collision_build.comp:40-51 */
 int p3m_build_force(p3m_ctx* ctx, int32_t n);                   /* buildForce, :907-973 */
 int p3m_apply_kick(p3m_ctx* ctx, int32_t n, int32_t initial);   /* applyKick, :1213-1261 */
-/* Cell keys, 64-bit-key radix sort and cell lists only (the first part of
- * build_grid.comp, as CSR lists). */
+/* Cell keys, their sort and the cell lists only (the first part of
+ * build_grid.comp, as CSR lists). The keys are 32-bit home cells written in
+ * descending body ID; a stable LSD radix sort over the cell bits then gives
+ * the reference's (cell, ~id) order. */
 int p3m_build_cell_lists(p3m_ctx* ctx, int32_t n);
 
 /* Steps run as CUDA graphs captured once per (body count, reorder step,
@@ -182,7 +186,15 @@ int p3m_build_cell_lists(p3m_ctx* ctx, int32_t n);
  * by one. Profiling (p3m_profile_enable) always launches one by one. */
 int p3m_set_graphs(p3m_ctx* ctx, int32_t enabled);
 
-/* Wait for the context's stream; returns the first pending device error. */
+/* Wait for the context's stream. Returns the first pending CUDA error, else
+ * the first failure the device detected since the last report, each reported
+ * once: P3M_ERR_TIMEOUT when a bounded look-back wait of a sort gave up (the
+ * cell lists, and everything computed from them since, are invalid), then
+ * P3M_ERR_NON_FINITE when the drift met bodies with non-finite state (the
+ * reference counts these in measureCluster, GravityPipeline.kt:817-819).
+ * The stepping calls are asynchronous like CUDA launches: a failure inside
+ * them surfaces at the next p3m_synchronize (or, for a timeout, the next
+ * p3m_download_state). */
 int p3m_synchronize(p3m_ctx* ctx);
 
 /* ---- profiling and diagnostics ----------------------------------------- */
@@ -227,10 +239,38 @@ int p3m_nonfinite_count(p3m_ctx* ctx, int64_t* count);
  * cell and Morton sorts find each tile's output offsets by looking back at
  * the tiles before it; every such wait has a poll limit, so a kernel always
  * ends. A nonzero count means a wait ran out and the results since then
- * cannot be trusted. Expected to stay 0. No counterpart in the reference
+ * cannot be trusted; p3m_synchronize and p3m_download_state report the
+ * growth as P3M_ERR_TIMEOUT. Expected to stay 0. No counterpart in the reference
  * (its sorts are the atomic pushes of build_grid.comp and
  * spatial_sort_scatter.comp). */
 int p3m_wait_timeouts(p3m_ctx* ctx, int64_t* count);
+
+/* Test hook of the timeout path; no counterpart in the reference. Sets how
+ * many times a look-back wait polls before it gives up (1..; 200,000 by
+ * default) and a tile index whose counts the sort never publishes (-1: none,
+ * the default). With a tile withheld, the waits of the tiles after it run
+ * out: they end, are counted (p3m_wait_timeouts) and p3m_synchronize returns
+ * P3M_ERR_TIMEOUT. Nothing faults; the results of such a sort are wrong.
+ * Restore (200000, -1) to return to normal operation. */
+int p3m_set_lookback_fault(p3m_ctx* ctx, int32_t poll_limit, int32_t withheld_tile);
+
+/* validateFft (GravityPipeline.kt:378-419): the density spectrum of the last
+ * force build, as the FP32 path computes it, against an FP64 transform of
+ * the same density mesh (value / massScale, or / 2^32 for the int64 form),
+ * both on the device. out3 = {maximum absolute error, maximum absolute error
+ * / maximum |reference component|, RMS error} over every real and imaginary
+ * component of the full MW x MH spectrum (the half spectrum extended by its
+ * Hermitian symmetry). Periodic mesh only: P3M_ERR_STATE inside walls, as
+ * the reference's check(!bounded), and before any force build. Blocking;
+ * allocates its FP64 work buffers for the call. */
+int p3m_validate_fft(p3m_ctx* ctx, double* out3);
+
+/* The FP32 density spectrum of the last force build (forward 2D real FFT of
+ * the density / massScale): (MW/2 + 1) * MH complex float2 values, row ky
+ * then column kx, i.e. numpy.fft.rfft2's layout of the (MH, MW) mesh.
+ * `bytes` is the capacity of `spectrum2` (host memory). Walls: the 2x mesh.
+ * P3M_ERR_STATE before any force build. Blocking. */
+int p3m_density_spectrum(p3m_ctx* ctx, float* spectrum2, size_t bytes);
 
 /* FP64 direct-sum acceleration (unit/s^2) of `n_targets` bodies (IDs in
  * `targets`, host array) from all n bodies: the law the P3M split
@@ -350,7 +390,8 @@ int p3m_trajectories(p3m_ctx* ctx, int32_t n, const p3m_trajectory_config* confi
  * forbidden or would stall (inside a frame callback, a captured region), or a
  * host whose device memory is handed out by another runtime (a JVM, an
  * engine). Builds the same lists as p3m_build_cell_lists — keys of the home
- * cells, the 64-bit-key radix sort, the CSR lists — from caller-owned device
+ * cells, the stable sort of 32-bit cell keys written in descending ID, the
+ * CSR lists — from caller-owned device
  * arrays into caller-owned device arrays, on `stream` (a cudaStream_t, NULL
  * for the default stream), without calling cudaMalloc, cudaFree or any
  * allocating routine.
@@ -366,7 +407,10 @@ int p3m_trajectories(p3m_ctx* ctx, int32_t n, const p3m_trajectory_config* confi
  * is one array compiled into the library (about 16.3 MB held on every GPU that
  * loads it, until exit). The first call on each device looks up that array's
  * address (cudaGetSymbolAddress) with the device current; make that first call
- * before any stream capture. All calls share the array and it keeps the last
+ * before any stream capture. The address is kept for the life of the process:
+ * after a cudaDeviceReset (or anything else that destroys the device's
+ * primary context) it is stale, so do not call this entry point again in that
+ * process. All calls share the array and it keeps the last
  * call's contents: calls whose work overlaps on the GPU race, so order them on
  * one stream. */
 #define P3M_CELL_LISTS_STATIC_MAX_BODIES 1048576
