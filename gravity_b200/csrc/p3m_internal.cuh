@@ -252,7 +252,7 @@ cudaError_t launch_short_range(const float4* bodies, const float4* entries, cons
 // The two source slots of every cell for the two-slot short range (exact
 // limit 2): the monopole at the cell centre (count > 2), the first one or
 // two list entries, or empty slots (mass 0) at the centre. Two planes of W*H
-// cells: float4 (x0, y0, G m0 / M_tot, x1), then float2 (y1, G m1 / M_tot).
+// cells: float4 (x0, x1, y0, y1), then float2 (G m0 / M_tot, G m1 / M_tot).
 cudaError_t launch_cell_slots(const int* cell_start, const int* cell_count,
                               const uint32_t* cell_mass, const float4* entries, int W, int H,
                               float gravity, float total_mass, float4* slots,

@@ -66,7 +66,8 @@ __global__ void __launch_bounds__(256) interp_kick_kernel(
 // gives its entries; missing slots are massless at the centre, so they add
 // nothing. The short range then reads 24 bytes per cell instead of the
 // count -> start -> entries chain. A slot holds x, y and G m / M_tot, the
-// product the pair term forms first.
+// product the pair term forms first; the two slots of a cell are stored
+// interleaved, (x0, x1, y0, y1) and (G m0 / M, G m1 / M).
 __device__ __forceinline__ void cell_slots_body(
     int block, const int* __restrict__ cell_start, const int* __restrict__ cell_count,
     const uint32_t* __restrict__ cell_mass, const float4* __restrict__ entries, int W, int H,
@@ -86,9 +87,11 @@ __device__ __forceinline__ void cell_slots_body(
         if (count == 2) s1 = entries[start + 1];
     }
     const float g_over_m = gravity / total_mass;
-    // Two planes: (x0, y0, gm0, x1) for every cell, then (y1, gm1).
-    slots[index] = make_float4(s0.x, s0.y, g_over_m * s0.z, s1.x);
-    reinterpret_cast<float2*>(slots + (size_t)W * H)[index] = make_float2(s1.y, g_over_m * s1.z);
+    // Two planes: (x0, x1, y0, y1) for every cell, then (gm0, gm1), so that
+    // each pair the packed FP32x2 pair term takes is loaded as one pair.
+    slots[index] = make_float4(s0.x, s1.x, s0.y, s1.y);
+    reinterpret_cast<float2*>(slots + (size_t)W * H)[index] =
+        make_float2(g_over_m * s0.z, g_over_m * s1.z);
 }
 
 __global__ void __launch_bounds__(256) cell_slots_kernel(

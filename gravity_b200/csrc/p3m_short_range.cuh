@@ -237,7 +237,8 @@ __device__ __forceinline__ void stencil_sum(
             const bool home = (a == RX) && (b == RY);
             if (EXACT == 2 && !home) {
                 // The cell's two slots, prepared once per step (cell_slots):
-                // (x0, y0, G m0 / M_tot, x1) and (y1, G m1 / M_tot).
+                // (x0, x1, y0, y1) and (G m0 / M_tot, G m1 / M_tot), so each
+                // packed operand is one loaded register pair.
                 float4 s0;
                 float2 s1;
                 if (STAGED) {
@@ -250,9 +251,8 @@ __device__ __forceinline__ void stencil_sum(
                 }
                 const float2 ox = make_float2(off_x[a], off_x[a]);
                 const float2 oy = make_float2(off_y, off_y);
-                pair_add2_gm(k, __fadd2_rn(make_float2(s0.x, s0.w), ox),
-                             __fadd2_rn(make_float2(s0.y, s1.x), oy), make_float2(s0.z, s1.y),
-                             ax2, ay2);
+                pair_add2_gm(k, __fadd2_rn(make_float2(s0.x, s0.y), ox),
+                             __fadd2_rn(make_float2(s0.z, s0.w), oy), s1, ax2, ay2);
                 continue;
             }
             const int count = __ldg(&cell_count[index]);
