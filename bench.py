@@ -138,6 +138,13 @@ def run_only(args) -> None:
         else:
             p.initialize_acceleration(sc.n)
             p.step(sc.n, args.steps)
+            if args.previews:
+                # A fan of aim previews on the field of the last step.
+                w_px, h_px = sc.config.viewport_width, sc.config.viewport_height
+                ang = np.linspace(0.0, 2.0 * np.pi, args.previews, endpoint=False)
+                o = np.tile(np.array([0.3 * w_px, 0.5 * h_px], np.float32), (args.previews, 1))
+                v = (300.0 * np.stack([np.cos(ang), np.sin(ang)], axis=1)).astype(np.float32)
+                p.trajectories(sc.n, o, v, steps=1024)
         p.synchronize()
     print("ok", sc.n)
 
@@ -1079,6 +1086,8 @@ def main():
     ap.add_argument("--sims", type=int, default=None, help="batch: number of simulations")
     ap.add_argument("--run-only", action="store_true",
                     help="run the initial pass and --steps steps untimed (a profiler's target)")
+    ap.add_argument("--previews", type=int, default=0,
+                    help="--run-only: then a fan of this many 1024-step aim previews")
     ap.add_argument("--no-plain", action="store_true",
                     help="lattice_scale: skip the 400k plummer_walls run beside it")
     ap.add_argument("--no-form-errors", action="store_true",

@@ -126,6 +126,16 @@ __device__ int tile_runs(const int* __restrict__ cell_start, const TileGeom& g, 
 // and carries into it (a native 32-bit shared atomic instead of a 64-bit one).
 template <typename T>
 struct TileAcc;
+// The split form (sparse tiles, add_split / get_split) adds without reading
+// back: a 32-bit value as it is, a 64-bit value q as a high part into hi and
+// the rest (at most 2^19) into lo, value = hi * 2^19 + lo, two shared
+// atomics whose results are not waited for. Exact while a cell gets at most
+// 8191 additions of values below 2^38 (each word's sum stays below 2^32): a
+// sparse tile holds fewer than 8192 bodies, and a tile that meets a larger
+// value (a body of mass 64 or more) is redone with the carry form.
+constexpr int kSplitShift = 19;
+constexpr unsigned long long kSplitMax = 1ull << 38;
+
 template <>
 struct TileAcc<uint32_t> {
     uint32_t lo[kTileX * kTileY];
@@ -134,6 +144,9 @@ struct TileAcc<uint32_t> {
         if (v) atomicAdd(&lo[i], v);
     }
     __device__ __forceinline__ uint32_t get(int i) const { return lo[i]; }
+    __device__ __forceinline__ void add_split(int i, uint32_t v) { atomicAdd(&lo[i], v); }
+    __device__ __forceinline__ uint32_t get_split(int i) const { return lo[i]; }
+    __device__ __forceinline__ static bool too_large(uint32_t) { return false; }
 };
 template <>
 struct TileAcc<unsigned long long> {
@@ -152,7 +165,56 @@ struct TileAcc<unsigned long long> {
     __device__ __forceinline__ unsigned long long get(int i) const {
         return ((unsigned long long)hi[i] << 32) | lo[i];
     }
+    __device__ __forceinline__ void add_split(int i, unsigned long long v) {
+        atomicAdd(&lo[i], (uint32_t)v & ((1u << kSplitShift) - 1u));
+        atomicAdd(&hi[i], (uint32_t)(v >> kSplitShift));
+    }
+    __device__ __forceinline__ unsigned long long get_split(int i) const {
+        return ((unsigned long long)hi[i] << kSplitShift) + lo[i];
+    }
+    __device__ __forceinline__ static bool too_large(unsigned long long v) {
+        return v >= kSplitMax;
+    }
 };
+
+// Clears the accumulator planes of `cells` cells (a multiple of 16) with
+// 16-byte stores.
+template <typename T>
+__device__ __forceinline__ void zero_tile(TileAcc<T>& acc, int cells) {
+    uint4* w = reinterpret_cast<uint4*>(&acc);
+    const uint4 z = make_uint4(0u, 0u, 0u, 0u);
+    for (int i = threadIdx.x; i < cells / 4; i += blockDim.x) {
+        w[i] = z;
+        if (sizeof(T) == 8) w[kTileX * kTileY / 4 + i] = z;
+    }
+}
+
+// Writes the finished tile, two cells (int64) or four (uint32) per 16-byte
+// store; rows of a tile start at even cells of a row of the mesh.
+template <typename T>
+__device__ __forceinline__ void store_tile(const TileAcc<T>& acc, bool split, const TileGeom& g,
+                                           int c0, int r0, int cells, T* __restrict__ density) {
+    const uint32_t* lo = reinterpret_cast<const uint32_t*>(&acc);
+    if (sizeof(T) == 8) {
+        const uint32_t* hi = lo + kTileX * kTileY;
+        const int shift = split ? kSplitShift : 32;
+        for (int i = 2 * threadIdx.x; i < cells; i += 2 * blockDim.x) {
+            const uint2 l = *reinterpret_cast<const uint2*>(lo + i);
+            const uint2 h = *reinterpret_cast<const uint2*>(hi + i);
+            const int y = i >> g.tx_log2, x = i & (g.TX - 1);
+            ulonglong2 v;
+            v.x = ((unsigned long long)h.x << shift) + l.x;
+            v.y = ((unsigned long long)h.y << shift) + l.y;
+            *reinterpret_cast<ulonglong2*>(density + (size_t)(r0 + y) * g.MW + c0 + x) = v;
+        }
+    } else {
+        for (int i = 4 * threadIdx.x; i < cells; i += 4 * blockDim.x) {
+            const uint4 l = *reinterpret_cast<const uint4*>(lo + i);
+            const int y = i >> g.tx_log2, x = i & (g.TX - 1);
+            *reinterpret_cast<uint4*>(density + (size_t)(r0 + y) * g.MW + c0 + x) = l;
+        }
+    }
+}
 
 // One body's CIC corners, quantized, with their tile coordinates.
 template <typename T>
@@ -179,6 +241,12 @@ __device__ __forceinline__ Corners<T> corners(float4 e, const TileGeom& g, float
     return c;
 }
 
+template <typename T, bool SPLIT>
+__device__ __forceinline__ void acc_put(TileAcc<T>& acc, int i, T v) {
+    if (SPLIT) acc.add_split(i, v);
+    else acc.add(i, v);
+}
+
 template <typename T>
 __device__ __forceinline__ void add_node(TileAcc<T>& acc, const TileGeom& g, int c0, int r0,
                                          int nx, int ny, T v) {
@@ -187,30 +255,116 @@ __device__ __forceinline__ void add_node(TileAcc<T>& acc, const TileGeom& g, int
     if ((unsigned)tx < (unsigned)g.TX && (unsigned)ty < (unsigned)g.TY) acc.add(ty * g.TX + tx, v);
 }
 
-template <typename T>
+template <typename T, bool SPLIT = false>
 __device__ __forceinline__ void add_corners(const Corners<T>& c, const TileGeom& g, int c0, int r0,
                                             TileAcc<T>& acc) {
     const int x0 = wrap_index(c.bx, g.MW) - c0, x1 = wrap_index(c.bx + 1, g.MW) - c0;
     const int y0 = wrap_index(c.by, g.MH) - r0, y1 = wrap_index(c.by + 1, g.MH) - r0;
     const bool in_x0 = (unsigned)x0 < (unsigned)g.TX, in_x1 = (unsigned)x1 < (unsigned)g.TX;
     if ((unsigned)y0 < (unsigned)g.TY) {
-        if (in_x0) acc.add(y0 * g.TX + x0, c.q00);
-        if (in_x1) acc.add(y0 * g.TX + x1, c.q10);
+        if (in_x0) acc_put<T, SPLIT>(acc, y0 * g.TX + x0, c.q00);
+        if (in_x1) acc_put<T, SPLIT>(acc, y0 * g.TX + x1, c.q10);
     }
     if ((unsigned)y1 < (unsigned)g.TY) {
-        if (in_x0) acc.add(y1 * g.TX + x0, c.q01);
-        if (in_x1) acc.add(y1 * g.TX + x1, c.q11);
+        if (in_x0) acc_put<T, SPLIT>(acc, y1 * g.TX + x0, c.q01);
+        if (in_x1) acc_put<T, SPLIT>(acc, y1 * g.TX + x1, c.q11);
+    }
+}
+
+// add_corners for a body whose CIC base lies in [0, MW-2] x [0, MH-2]: no
+// mesh index wraps, so the tile coordinates are plain differences (the same
+// cells wrap_index would give).
+template <typename T, bool SPLIT>
+__device__ __forceinline__ void add_corners_inner(const Corners<T>& c, const TileGeom& g, int c0,
+                                                  int r0, TileAcc<T>& acc) {
+    const int x0 = c.bx - c0, y0 = c.by - r0;
+    const int i00 = y0 * g.TX + x0;
+    const bool in_x0 = (unsigned)x0 < (unsigned)g.TX, in_x1 = (unsigned)(x0 + 1) < (unsigned)g.TX;
+    const bool in_y0 = (unsigned)y0 < (unsigned)g.TY, in_y1 = (unsigned)(y0 + 1) < (unsigned)g.TY;
+    if (in_y0 && in_x0) acc_put<T, SPLIT>(acc, i00, c.q00);
+    if (in_y0 && in_x1) acc_put<T, SPLIT>(acc, i00 + 1, c.q10);
+    if (in_y1 && in_x0) acc_put<T, SPLIT>(acc, i00 + g.TX, c.q01);
+    if (in_y1 && in_x1) acc_put<T, SPLIT>(acc, i00 + g.TX + 1, c.q11);
+}
+
+// The split quantization of one corner weight w (int64 form, 2^-32 mass
+// quanta): q = rint(w * 2^32) = floor(t) * 2^19 + rint(frac(t) * 2^19) with
+// t = w * 2^13 (exact: a power-of-two scale), the first part an integer
+// multiple of 2^19 so that rounding ties keep their parity. Both parts come
+// out of float additions of 2^23, whose result's low bits are the integer:
+// floor by a round-down addition, the fraction's rounding by the ordinary
+// round-to-nearest-even one. Valid for t < 2^19 (q < 2^38); `large` records
+// a larger weight. lo may be 2^19 itself.
+__device__ __forceinline__ void split_quantize(float w, uint32_t& hi, uint32_t& lo, bool& large) {
+    constexpr float kMagic = 8388608.0f;  // 2^23
+    const float t = __fmul_rn(w, 8192.0f);
+    const float a = __fadd_rd(t, kMagic);
+    hi = __float_as_uint(a) - 0x4b000000u;
+    const float rem = __fsub_rn(t, __fsub_rn(a, kMagic));
+    lo = __float_as_uint(__fmaf_rn(rem, 524288.0f, kMagic)) - 0x4b000000u;
+    large |= t >= 524288.0f;
+}
+
+// One body of a sparse tile whose CIC base lies inside the mesh with room
+// for its +1 corner (0 <= gx < MW - 1, 0 <= gy < MH - 1, checked by the
+// caller): floor by a round-down addition of 1.5 * 2^23 (|g| < 2^22), no
+// wrap, the corner weights rounded like corners() (each product on its own,
+// packed in pairs), then the four corners that land in the tile.
+template <typename T>
+__device__ __forceinline__ void fast_corners(float gx, float gy, float m, const TileGeom& g, int c0,
+                                             int r0, float scale, TileAcc<T>& acc, bool& large) {
+    constexpr float kFloorMagic = 12582912.0f;  // 1.5 * 2^23
+    const float fxa = __fadd_rd(gx, kFloorMagic), fya = __fadd_rd(gy, kFloorMagic);
+    const int bx = (int)(__float_as_uint(fxa) - 0x4b400000u);
+    const int by = (int)(__float_as_uint(fya) - 0x4b400000u);
+    const float fx = __fsub_rn(gx, __fsub_rn(fxa, kFloorMagic));
+    const float fy = __fsub_rn(gy, __fsub_rn(fya, kFloorMagic));
+    const float ofx = __fsub_rn(1.0f, fx), ofy = __fsub_rn(1.0f, fy);
+    // (ofx*ofy, fx*ofy) and (ofx*fy, fx*fy), then each times m.
+    const float2 r0w = __fmul2_rn(__fmul2_rn(make_float2(ofx, fx), make_float2(ofy, ofy)),
+                                  make_float2(m, m));
+    const float2 r1w = __fmul2_rn(__fmul2_rn(make_float2(ofx, fx), make_float2(fy, fy)),
+                                  make_float2(m, m));
+    const int x0 = bx - c0, y0 = by - r0;
+    const int i00 = y0 * g.TX + x0;
+    const bool in_x0 = (unsigned)x0 < (unsigned)g.TX, in_x1 = (unsigned)(x0 + 1) < (unsigned)g.TX;
+    const bool in_y0 = (unsigned)y0 < (unsigned)g.TY, in_y1 = (unsigned)(y0 + 1) < (unsigned)g.TY;
+    if (sizeof(T) == 8) {
+        uint32_t h[4], l[4];
+        split_quantize(r0w.x, h[0], l[0], large);
+        split_quantize(r0w.y, h[1], l[1], large);
+        split_quantize(r1w.x, h[2], l[2], large);
+        split_quantize(r1w.y, h[3], l[3], large);
+        uint32_t* lo = reinterpret_cast<uint32_t*>(&acc);
+        uint32_t* hi = lo + kTileX * kTileY;
+        if (in_y0 && in_x0) { atomicAdd(&lo[i00], l[0]); atomicAdd(&hi[i00], h[0]); }
+        if (in_y0 && in_x1) { atomicAdd(&lo[i00 + 1], l[1]); atomicAdd(&hi[i00 + 1], h[1]); }
+        if (in_y1 && in_x0) { atomicAdd(&lo[i00 + g.TX], l[2]); atomicAdd(&hi[i00 + g.TX], h[2]); }
+        if (in_y1 && in_x1) {
+            atomicAdd(&lo[i00 + g.TX + 1], l[3]);
+            atomicAdd(&hi[i00 + g.TX + 1], h[3]);
+        }
+    } else {
+        uint32_t* lo = reinterpret_cast<uint32_t*>(&acc);
+        if (in_y0 && in_x0) atomicAdd(&lo[i00], __float2uint_rn(__fmul_rn(r0w.x, scale)));
+        if (in_y0 && in_x1) atomicAdd(&lo[i00 + 1], __float2uint_rn(__fmul_rn(r0w.y, scale)));
+        if (in_y1 && in_x0) atomicAdd(&lo[i00 + g.TX], __float2uint_rn(__fmul_rn(r1w.x, scale)));
+        if (in_y1 && in_x1)
+            atomicAdd(&lo[i00 + g.TX + 1], __float2uint_rn(__fmul_rn(r1w.y, scale)));
     }
 }
 
 // Sparse tiles: warp w takes the w-th share of the runs' positions, its
 // lanes consecutive positions (coalesced within a run), four loads in flight
 // per lane; each lane walks the runs forward from one search, so finding an
-// entry costs O(1). Each body's corners are added one by one.
-template <typename T>
-__device__ void tile_direct(const float4* __restrict__ entries, int total, const int* run_begin,
+// entry costs O(1). Each body's corners are added one by one, without index
+// wrapping where none can occur. SPLIT: the split accumulator form; returns
+// (in every thread) whether a value was too large for it.
+template <typename T, bool SPLIT>
+__device__ bool tile_direct(const float4* __restrict__ entries, int total, const int* run_begin,
                             const int* run_prefix, const TileGeom& g, int c0, int r0, float scale,
                             TileAcc<T>& acc) {
+    bool large = false;
     constexpr int U = 4;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, warps = blockDim.x >> 5;
     const int share = (total + warps - 1) / warps;
@@ -237,9 +391,27 @@ __device__ void tile_direct(const float4* __restrict__ entries, int total, const
             }
         }
 #pragma unroll
-        for (int u = 0; u < U; ++u)
-            if (p0 + 32 * u < ke) add_corners<T>(corners<T>(e[u], g, scale), g, c0, r0, acc);
+        for (int u = 0; u < U; ++u) {
+            if (p0 + 32 * u >= ke) continue;
+            if (SPLIT) {
+                const float gx = __fsub_rn(__fmul_rn(e[u].x, (float)g.W), 0.5f);
+                const float gy = __fsub_rn(__fmul_rn(e[u].y, (float)g.H), 0.5f);
+                if (gx >= 0.0f && gx < (float)(g.MW - 1) && gy >= 0.0f && gy < (float)(g.MH - 1)) {
+                    fast_corners<T>(gx, gy, e[u].z, g, c0, r0, scale, acc, large);
+                    continue;
+                }
+            }
+            const Corners<T> c = corners<T>(e[u], g, scale);
+            if (SPLIT)
+                large |= TileAcc<T>::too_large(c.q00) | TileAcc<T>::too_large(c.q10) |
+                         TileAcc<T>::too_large(c.q01) | TileAcc<T>::too_large(c.q11);
+            if ((unsigned)c.bx <= (unsigned)(g.MW - 2) && (unsigned)c.by <= (unsigned)(g.MH - 2))
+                add_corners_inner<T, SPLIT>(c, g, c0, r0, acc);
+            else
+                add_corners<T, SPLIT>(c, g, c0, r0, acc);
+        }
     }
+    return __syncthreads_or(large ? 1 : 0) != 0;
 }
 
 // Sums of consecutive bodies of one home cell (hx, hy) over the 3x3 mesh
@@ -350,14 +522,15 @@ __global__ void __launch_bounds__(kThreads) deposit_tiles_kernel(
     float scale, T* __restrict__ density, int4* __restrict__ work, int* __restrict__ work_count,
     int work_capacity) {
     grid_dependency_wait();
-    __shared__ TileAcc<T> acc;
+    __shared__ __align__(16) TileAcc<T> acc;
     __shared__ int run_begin[kMaxRuns], run_end[kMaxRuns], run_prefix[kMaxRuns];
     __shared__ int s_total;
     const int tile = blockIdx.x;
     const int c0 = (tile % g.tiles_x) * g.TX, r0 = (tile / g.tiles_x) * g.TY;
     const int cells = g.TX * g.TY;
-    for (int i = threadIdx.x; i < cells; i += blockDim.x) acc.zero(i);
+    zero_tile<T>(acc, cells);
     const int total = tile_runs(cell_start, g, tile, run_begin, run_end, run_prefix, &s_total);
+    bool split = false;  // uniform over the CTA
     if (total > kTileCap) {
         // Heavy tile: zeros now; its runs, in pieces of kPiece entries, to
         // the second kernel.
@@ -367,17 +540,20 @@ __global__ void __launch_bounds__(kThreads) deposit_tiles_kernel(
             for (int j = 0; j < pieces && base + j < work_capacity; ++j)
                 work[base + j] = make_int4(tile, j * kPiece, min(total, (j + 1) * kPiece), 0);
         }
+    } else if (total >= kDenseBodiesPerCell * cells) {
+        tile_dense<T>(entries, 0, total, run_begin, run_end, run_prefix, g, c0, r0, scale, acc);
     } else {
-        if (total > kDenseBodiesPerCell * cells)
-            tile_dense<T>(entries, 0, total, run_begin, run_end, run_prefix, g, c0, r0, scale, acc);
-        else
-            tile_direct<T>(entries, total, run_begin, run_prefix, g, c0, r0, scale, acc);
+        split = true;
+        if (tile_direct<T, true>(entries, total, run_begin, run_prefix, g, c0, r0, scale, acc)) {
+            // A body of mass 64 or more: the same tile again, carrying.
+            split = false;
+            zero_tile<T>(acc, cells);
+            __syncthreads();
+            tile_direct<T, false>(entries, total, run_begin, run_prefix, g, c0, r0, scale, acc);
+        }
     }
     __syncthreads();
-    for (int i = threadIdx.x; i < cells; i += blockDim.x) {
-        const int y = i >> g.tx_log2, x = i & (g.TX - 1);
-        density[(size_t)(r0 + y) * g.MW + c0 + x] = acc.get(i);
-    }
+    store_tile<T>(acc, split, g, c0, r0, cells, density);
 }
 
 // Pieces of heavy tiles: each warp takes a 1/warps share of the piece
