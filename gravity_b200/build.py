@@ -5,9 +5,12 @@ Each .cu file under gravity_b200/csrc is compiled by nvcc for
 one shared library that exports the C-ABI of include/p3m.h. The library links
 the CUDA runtime statically (nvcc's default), so it needs only the driver.
 
-Files that derive integers or positions from floating point (keys, deposit
-weights, drift) are compiled with ``--fmad=false`` so that no multiply-add is
-contracted: their results must round exactly like the CPU oracle's.
+The stage sources under csrc/step/ are compiled as one translation unit
+(p3m_step.cu), which also holds the batched form's persistent kernel. The code
+there that derives integers or positions from floating point (keys, deposit
+weights, drift) uses explicit round-to-nearest intrinsics, so no multiply-add
+is contracted and it rounds exactly like the CPU oracle; the aim previews
+(p3m_trajectory.cu) are compiled with ``--fmad=false`` for the same reason.
 
 Usage: ``python -m gravity_b200.build [--force] [--verbose]``.
 """
@@ -34,7 +37,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-O2",
           "--expt-relaxed-constexpr"]
 # Sources whose arithmetic must not contract a*b+c into one rounding.
-NO_FMA = {"p3m_sort.cu", "p3m_deposit.cu", "p3m_drift.cu", "p3m_trajectory.cu"}
+NO_FMA = {"p3m_trajectory.cu"}
 
 
 def nvcc() -> str:
@@ -49,7 +52,11 @@ def sources() -> list[Path]:
 
 
 def headers() -> list[Path]:
-    return sorted(CSRC.glob("*.cuh")) + sorted(INCLUDE.glob("*.h"))
+    """Everything a translation unit may include: the internal headers, the
+    stage sources under csrc/step/ (compiled through p3m_step.cu) and the
+    public header."""
+    return (sorted(CSRC.glob("*.cuh")) + sorted((CSRC / "step").glob("*.cu")) +
+            sorted((CSRC / "step").glob("*.cuh")) + sorted(INCLUDE.glob("*.h")))
 
 
 def _stale(target: Path, deps: list[Path]) -> bool:
@@ -76,7 +83,7 @@ def build(force: bool = False, verbose: bool = False, ptxas_verbose: bool = Fals
         objs.append(obj)
         if not force and not _stale(obj, [src] + hdrs):
             continue
-        cmd = [cc, *ARCH, *COMMON, "-I", str(INCLUDE), "-c", str(src), "-o", str(obj)]
+        cmd = [cc, *ARCH, *COMMON, "-I", str(INCLUDE), "-I", str(CSRC), "-c", str(src), "-o", str(obj)]
         if src.name in NO_FMA:
             cmd.append("--fmad=false")
         if ptxas_verbose:

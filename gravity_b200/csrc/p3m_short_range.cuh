@@ -33,7 +33,15 @@
 //
 // Each p3m_short_range_rN.cu instantiates one Rx so the instantiations
 // compile in parallel.
-#pragma once
+// Included once as it is, and once more by p3m_step.cu inside namespace
+// p3m::coherent (P3M_COHERENT_BODIES) for the batched form's persistent
+// kernel, which must not read through the non-coherent load path.
+#if defined(P3M_COHERENT_BODIES) ? !defined(P3M_SHORT_RANGE_COHERENT_) : !defined(P3M_SHORT_RANGE_PLAIN_)
+#ifdef P3M_COHERENT_BODIES
+#define P3M_SHORT_RANGE_COHERENT_
+#else
+#define P3M_SHORT_RANGE_PLAIN_
+#endif
 
 #include "p3m_internal.cuh"
 
@@ -295,9 +303,17 @@ __device__ __forceinline__ void stencil_sum(
     acc_y = ay2;
 }
 
+// Shared memory of the two-slot form (EXACT = 2): the staged slot-table box
+// and the CTA's box reduction.
+struct SlotStage {
+    float4 a[kStageCells];
+    float2 b[kStageCells];
+    int red[4 * 32];
+};
+
 template <int RX, int RY, int EXACT>
 __device__ __forceinline__ void short_range_body(
-    int block, const float4* __restrict__ bodies, const float4* __restrict__ entries,
+    SlotStage* sm, int block, const float4* __restrict__ bodies, const float4* __restrict__ entries,
     const int* __restrict__ cell_start, const int* __restrict__ cell_count,
     const uint32_t* __restrict__ cell_mass, const float4* __restrict__ slots,
     float2* __restrict__ a_short, const KickParams& p) {
@@ -317,12 +333,9 @@ __device__ __forceinline__ void short_range_body(
     float4* st_a = nullptr;
     float2* st_b = nullptr;
     if (EXACT == 2) {
-        __shared__ float4 stage_a[kStageCells];
-        __shared__ float2 stage_b[kStageCells];
-        __shared__ int red[4 * 32];
-        st_a = stage_a;
-        st_b = stage_b;
-        box = stage_slots<RX, RY>(valid, hx, hy, slots, slots_b, p, stage_a, stage_b, red);
+        st_a = sm->a;
+        st_b = sm->b;
+        box = stage_slots<RX, RY>(valid, hx, hy, slots, slots_b, p, sm->a, sm->b, sm->red);
         if (!valid) return;
         if (box.staged) sbase = (hy - RY - box.y0) * box.w + (hx - RX - box.x0);
     }
@@ -346,8 +359,13 @@ __global__ void __launch_bounds__(256) short_range_kernel(
     const uint32_t* __restrict__ cell_mass, const float4* __restrict__ slots,
     float2* __restrict__ a_short, KickParams p) {
     grid_dependency_wait();
-    short_range_body<RX, RY, EXACT>(blockIdx.x, bodies, entries, cell_start, cell_count, cell_mass,
-                                    slots, a_short, p);
+    SlotStage* sm = nullptr;  // the two-slot form's stage; the list form has none
+    if constexpr (EXACT == 2) {
+        __shared__ SlotStage stage;
+        sm = &stage;
+    }
+    short_range_body<RX, RY, EXACT>(sm, blockIdx.x, bodies, entries, cell_start, cell_count,
+                                    cell_mass, slots, a_short, p);
 }
 
 template <int RX, int RY, int EXACT>
@@ -355,12 +373,18 @@ __global__ void __launch_bounds__(256) short_range_batched_kernel(
     const ShortRangeArgs* __restrict__ args, const int* __restrict__ first, int sims) {
     const int2 sb = batch_block(first, sims);
     const ShortRangeArgs a = args[sb.x];
-    short_range_body<RX, RY, EXACT>(sb.y, a.bodies, a.entries, a.cell_start, a.cell_count,
+    SlotStage* sm = nullptr;
+    if constexpr (EXACT == 2) {
+        __shared__ SlotStage stage;
+        sm = &stage;
+    }
+    short_range_body<RX, RY, EXACT>(sm, sb.y, a.bodies, a.entries, a.cell_start, a.cell_count,
                                     a.cell_mass, a.slots, a.a_short, a.p);
 }
 
 }  // namespace sr
 
+#ifndef P3M_COHERENT_BODIES
 // Launches short_range_kernel<RX, p.ry, 2 or 0>; defined (explicitly
 // instantiated) in p3m_short_range_rN.cu.
 template <int RX>
@@ -435,4 +459,8 @@ P3M_DECLARE_SHORT_RANGE_RX(6)
         return cudaGetLastError();                                                              \
     }
 
+#endif  // !P3M_COHERENT_BODIES
+
 }  // namespace p3m
+
+#endif  // inclusion guard

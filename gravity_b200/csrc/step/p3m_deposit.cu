@@ -686,6 +686,10 @@ TileGeom tile_geom(const GridShape& g) {
 
 }  // namespace
 
+// Host-side launchers: not part of the coherent copy of the bodies that the
+// batched form's persistent kernel uses (p3m_step.cu).
+#ifndef P3M_COHERENT_BODIES
+
 cudaError_t configure_deposit() {
     const void* fns[] = {(const void*)deposit_chunks_kernel<unsigned long long>,
                          (const void*)deposit_chunks_kernel<uint32_t>,
@@ -773,4 +777,5 @@ cudaError_t launch_deposit(const float4* entries, const uint32_t* keys, const in
     return cudaGetLastError();
 }
 
+#endif  // !P3M_COHERENT_BODIES
 }  // namespace p3m

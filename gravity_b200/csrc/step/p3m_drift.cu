@@ -1,8 +1,9 @@
 // p3m_drift.cu — the leapfrog drift of the gravity step.
 //
-// Built with --fmad=false: every multiply and add rounds on its own, as in
-// the oracle, so positions and the cell keys derived from them are
-// bit-identical to it for the same accelerations.
+// Every multiply and add rounds on its own (explicit round-to-nearest
+// intrinsics, never contracted into one multiply-add), as in the oracle, so
+// positions and the cell keys derived from them are bit-identical to it for
+// the same accelerations.
 //
 // drift: collision_build.comp:40-51 (gravity-only, so only the half kick,
 //   drift and wall clamp / torus wrap of each collision substep), all S
@@ -13,7 +14,18 @@
 namespace p3m {
 namespace {
 
-__device__ __forceinline__ float fractf(float v) { return v - floorf(v); }
+// floorf(v) without the conversion unit (the drift's 32 floors per body
+// otherwise saturate it): for |v| < 2^23 the round-down sum v + 2^23 (with
+// v's sign) has a unit in the last place of 1, so subtracting 2^23 again
+// leaves floor(v) exactly; copysign restores floorf's signed zero. Larger
+// |v|, infinities and NaN are their own floor.
+__device__ __forceinline__ float floor_exact(float v) {
+    const float m = copysignf(8388608.0f, v);
+    const float f = copysignf(__fsub_rn(__fadd_rd(v, m), m), v);
+    return fabsf(v) < 8388608.0f ? f : v;
+}
+
+__device__ __forceinline__ float fractf(float v) { return __fsub_rn(v, floor_exact(v)); }
 
 // Drifts body `id` (when id < n) and writes its cell key; returns the key.
 __device__ __forceinline__ uint32_t drift_one(int id, float4* __restrict__ bodies,
@@ -30,10 +42,10 @@ __device__ __forceinline__ uint32_t drift_one(int id, float4* __restrict__ bodie
         // Substeps after the first carry kickDt = 0 (GravityPipeline.kt:465-473),
         // whose kick adds a * 0.
         const float hk = s == 0 ? half_kick : 0.0f;
-        b.z = b.z + a.x * hk;
-        b.w = b.w + a.y * hk;
-        b.x = b.x + b.z * drift_dt;
-        b.y = b.y + b.w * drift_dt;
+        b.z = __fadd_rn(b.z, __fmul_rn(a.x, hk));
+        b.w = __fadd_rn(b.w, __fmul_rn(a.y, hk));
+        b.x = __fadd_rn(b.x, __fmul_rn(b.z, drift_dt));
+        b.y = __fadd_rn(b.y, __fmul_rn(b.w, drift_dt));
         if (bounded) {
             b.x = fminf(fmaxf(b.x, 0.0f), kMaximumUnit);
             b.y = fminf(fmaxf(b.y, 0.0f), kMaximumUnit);
@@ -93,6 +105,10 @@ __global__ void drift_batched_kernel(const DriftArgs* __restrict__ args, const i
 
 }  // namespace
 
+// Host-side launchers: not part of the coherent copy of the bodies that the
+// batched form's persistent kernel uses (p3m_step.cu).
+#ifndef P3M_COHERENT_BODIES
+
 cudaError_t batched_drift(const DriftArgs* a, BatchGrid g, cudaStream_t s) {
     if (g.blocks <= 0) return cudaSuccess;
     drift_batched_kernel<<<g.blocks, kBatchThreads, 0, s>>>(a, g.first, g.sims);
@@ -110,4 +126,5 @@ cudaError_t launch_drift(float4* bodies, const float2* accel, int n, float half_
     return cudaGetLastError();
 }
 
+#endif  // !P3M_COHERENT_BODIES
 }  // namespace p3m

@@ -660,6 +660,10 @@ void column_shape(int MW, int MH, int lines_factor, int* G, int* threads, int fi
 
 }  // namespace
 
+// Host-side launchers: not part of the coherent copy of the bodies that the
+// batched form's persistent kernel uses (p3m_step.cu).
+#ifndef P3M_COHERENT_BODIES
+
 // Dynamic shared memory opt-in (above 48 KB) of every FFT kernel, once per
 // device at context creation (never inside a stream capture).
 cudaError_t configure_fft() {
@@ -864,4 +868,5 @@ cudaError_t build_green(GridShape g, GreenParams p, double2* work, float2* green
     return cudaGetLastError();
 }
 
+#endif  // !P3M_COHERENT_BODIES
 }  // namespace p3m

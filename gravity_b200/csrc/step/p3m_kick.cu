@@ -120,6 +120,10 @@ __global__ void __launch_bounds__(256) interp_kick_batched_kernel(
 
 }  // namespace
 
+// Host-side launchers: not part of the coherent copy of the bodies that the
+// batched form's persistent kernel uses (p3m_step.cu).
+#ifndef P3M_COHERENT_BODIES
+
 cudaError_t batched_interp_kick(const KickArgs* a, BatchGrid g, cudaStream_t s) {
     if (g.blocks <= 0) return cudaSuccess;
     interp_kick_batched_kernel<<<g.blocks, kBatchThreads, 0, s>>>(a, g.first, g.sims);
@@ -190,4 +194,5 @@ cudaError_t launch_interp_kick(float4* bodies, float2* accel, const float2* forc
     return cudaGetLastError();
 }
 
+#endif  // !P3M_COHERENT_BODIES
 }  // namespace p3m

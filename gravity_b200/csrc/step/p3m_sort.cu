@@ -230,24 +230,37 @@ __device__ __forceinline__ uint32_t lookback_exclusive(const uint32_t* status, i
 // (2^bits); a thread handles MAXR / 256 digits where that is above 1. The
 // per-warp digit counts and the tile staged in digit order share one shared
 // region: each key's slot is taken from the counts before the tile is staged.
+// Shared memory of one scatter tile (radix_scatter_body): the per-warp digit
+// counts, then the tile staged in digit order, in one region; each digit's
+// start in the tile and in the output.
+template <int MAXR, int THREADS = kSortThreads>
+struct ScatterShared {
+    static constexpr int kWarpHist = (THREADS / 32) * MAXR;
+    static constexpr int kWords = kWarpHist > 2 * kSortTile ? kWarpHist : 2 * kSortTile;
+    uint32_t shared[kWords];
+    uint32_t tile_start[MAXR];
+    uint32_t out_base[MAXR];
+    uint32_t warp_tot[33];
+    int s_tile;
+};
+
 template <bool LOOKBACK, int MAXR, int THREADS = kSortThreads, int ITEMS = kSortItems>
 __device__ __forceinline__ void radix_scatter_body(
-    int tile, const uint32_t* __restrict__ keys_in, const uint32_t* __restrict__ vals_in,
-    uint32_t* __restrict__ keys_out, uint32_t* __restrict__ vals_out, int n, int shift, int bits,
-    int tiles, const uint32_t* __restrict__ hist_scanned, uint32_t* counter = nullptr,
+    ScatterShared<MAXR, THREADS>& sm, int tile, const uint32_t* __restrict__ keys_in,
+    const uint32_t* __restrict__ vals_in, uint32_t* __restrict__ keys_out,
+    uint32_t* __restrict__ vals_out, int n, int shift, int bits, int tiles,
+    const uint32_t* __restrict__ hist_scanned, uint32_t* counter = nullptr,
     uint32_t* status = nullptr, unsigned int* timeouts = nullptr, int poll_limit = 0,
     int withhold_tile = -1, uint32_t* failed = nullptr) {
     constexpr int kWarps = THREADS / 32;
     constexpr int kTile = THREADS * ITEMS;
     static_assert(kTile == kSortTile, "tiles hold kSortTile keys");
     constexpr int kPer = MAXR > THREADS ? MAXR / THREADS : 1;
-    constexpr int kWarpHist = kWarps * MAXR;
-    constexpr int kShared = kWarpHist > 2 * kSortTile ? kWarpHist : 2 * kSortTile;
-    __shared__ uint32_t shared[kShared];  // warp counts, then the staged tile
-    __shared__ uint32_t tile_start[MAXR];
-    __shared__ uint32_t out_base[MAXR];
-    __shared__ uint32_t warp_tot[33];
-    __shared__ int s_tile;
+    uint32_t* shared = sm.shared;  // warp counts, then the staged tile
+    uint32_t* tile_start = sm.tile_start;
+    uint32_t* out_base = sm.out_base;
+    uint32_t* warp_tot = sm.warp_tot;
+    int& s_tile = sm.s_tile;
     uint32_t* warp_hist = shared;  // [warp * radix + d]
     uint32_t* s_keys = shared;
     uint32_t* s_vals = shared + kSortTile;
@@ -380,8 +393,9 @@ __global__ void __launch_bounds__(kSortThreads) radix_scatter_kernel(
     const uint32_t* __restrict__ keys_in, const uint32_t* __restrict__ vals_in,
     uint32_t* __restrict__ keys_out, uint32_t* __restrict__ vals_out, int n, int shift, int bits,
     int tiles, const uint32_t* __restrict__ hist_scanned) {
-    radix_scatter_body<false, kSortMaxRadix>(blockIdx.x, keys_in, vals_in, keys_out, vals_out, n,
-                                             shift, bits, tiles, hist_scanned);
+    __shared__ ScatterShared<kSortMaxRadix> sm;
+    radix_scatter_body<false, kSortMaxRadix>(sm, blockIdx.x, keys_in, vals_in, keys_out, vals_out,
+                                             n, shift, bits, tiles, hist_scanned);
 }
 
 // One pass of the one-kernel-per-pass sort: `totals` = this pass's digit
@@ -399,9 +413,10 @@ __global__ void __launch_bounds__(kLookbackThreads) lookback_scatter_kernel(
     int tiles, const uint32_t* __restrict__ totals, uint32_t* counter, uint32_t* status,
     unsigned int* timeouts, int poll_limit, int withhold_tile, uint32_t* failed) {
     grid_dependency_wait();
+    __shared__ ScatterShared<MAXR, kLookbackThreads> sm;
     radix_scatter_body<true, MAXR, kLookbackThreads, kLookbackItems>(
-        0, keys_in, vals_in, keys_out, vals_out, n, shift, bits, tiles, totals, counter, status,
-        timeouts, poll_limit, withhold_tile, failed);
+        sm, 0, keys_in, vals_in, keys_out, vals_out, n, shift, bits, tiles, totals, counter,
+        status, timeouts, poll_limit, withhold_tile, failed);
 }
 
 // Digit totals of every pass in one read of the keys: per-CTA shared counts
@@ -670,8 +685,9 @@ __global__ void __launch_bounds__(kSortThreads) radix_scatter_batched_kernel(
     const RadixArgs* __restrict__ args, const int* __restrict__ first, int sims) {
     const int2 sb = batch_block(first, sims);
     const RadixArgs a = args[sb.x];
-    radix_scatter_body<false, kSortMaxRadix>(sb.y, a.keys_in, a.vals_in, a.keys_out, a.vals_out, a.n, a.shift, a.bits,
-                       a.tiles, a.hist);
+    __shared__ ScatterShared<kSortMaxRadix> sm;
+    radix_scatter_body<false, kSortMaxRadix>(sm, sb.y, a.keys_in, a.vals_in, a.keys_out,
+                                             a.vals_out, a.n, a.shift, a.bits, a.tiles, a.hist);
 }
 
 __global__ void __launch_bounds__(kScanThreads) scan_batched_kernel(
@@ -720,6 +736,10 @@ __global__ void zero_batched_kernel(const ZeroArgs* __restrict__ args,
 inline int blocks_for(long long n, int threads) { return (int)((n + threads - 1) / threads); }
 
 }  // namespace
+
+// Host-side launchers: not part of the coherent copy of the bodies that the
+// batched form's persistent kernel uses (p3m_step.cu).
+#ifndef P3M_COHERENT_BODIES
 
 size_t sort_hist_entries(int capacity) {
     const size_t tiles = ((size_t)capacity + kSortTile - 1) / kSortTile;
@@ -929,4 +949,5 @@ cudaError_t launch_cell_build(const uint32_t* keys, const uint32_t* ids, int n, 
     return cudaGetLastError();
 }
 
+#endif  // !P3M_COHERENT_BODIES
 }  // namespace p3m
