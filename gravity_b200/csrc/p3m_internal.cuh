@@ -443,6 +443,33 @@ cudaError_t batched_interp_kick(const KickArgs* a, BatchGrid g, cudaStream_t s);
 cudaError_t batched_cell_slots(const SlotsArgs* a, BatchGrid g, cudaStream_t s);
 cudaError_t configure_batched();
 
+// ---- the batched step as one persistent launch (step/p3m_batch_persistent.cu)
+// A stage: `blocks` virtual blocks of the batched body `kind` over `sims`
+// simulations; `args` and `first` are byte offsets of its argument array and
+// block prefix (sims + 1 ints) in the plan's device blob. A phase: stages
+// first_stage .. first_stage + stages - 1, independent of one another; a grid
+// barrier separates phases.
+enum PStageKind {
+    kPStageMorton, kPStageRadixHist, kPStageScan, kPStageRadixScatter, kPStagePermute,
+    kPStageCopy, kPStageDrift, kPStageZero, kPStageCellBuild, kPStageSlots,
+    kPStageShortRangeSlots, kPStageShortRangeLists, kPStageDepositU32, kPStageDepositI64,
+    kPStageFftRowsU32, kPStageFftRowsI64, kPStageFftColumns, kPStageFftInverse, kPStageKick
+};
+struct PStage { int kind, sims, blocks, args, first; };
+struct PPhase { int first_stage, stages; };
+struct CopyArgs { const uint32_t* src; uint32_t* dst; long long words; };  // 4-byte words
+// The persistent kernel's stencil: the short range stages it runs are (3, 3).
+constexpr int kPersistentRx = 3, kPersistentRy = 3;
+constexpr int kPersistentMaxStamps = 64;  // per-phase timer stamps of one launch
+size_t persistent_base_smem();
+int persistent_scan_limit();
+int persistent_ctas_per_sm(size_t smem);
+cudaError_t launch_batch_persistent(const unsigned char* blob, const PStage* stages,
+                                    const PPhase* phases, int n_phases, const float2* tw,
+                                    unsigned int* sync, int poll_limit, int withhold_cta,
+                                    int withhold_phase, int ctas, size_t smem,
+                                    unsigned long long* phase_ns, cudaStream_t stream);
+
 // Sets the message p3m_last_error(NULL) returns on this thread (entry points
 // without a context).
 void set_detached_error(const std::string& what);

@@ -771,8 +771,10 @@ cudaError_t launch_fft_adjoint(const float* cotangent, const float2* green, floa
 // launches and the simulation's line count.
 void fft_batch_shape(const GridShape& g, int* rows_per_cta, int* cols_per_cta, int* inv_per_cta,
                      size_t* rows_smem, size_t* cols_smem, size_t* inv_smem) {
-    auto fill = [](int lines_total, int L, int cap) {
-        int per = (256 * 8 + L - 1) / L;
+    // Lines per CTA: the autotuner's choice (g.fft_lines), else as many as
+    // make one radix-8 pass fill 256 threads; at most `cap` and the lines.
+    auto fill = [&g](int lines_total, int L, int cap) {
+        int per = g.fft_lines > 0 ? g.fft_lines : (256 * 8 + L - 1) / L;
         if (per > cap) per = cap;
         if (per > lines_total) per = lines_total;
         return per < 1 ? 1 : per;
