@@ -2,9 +2,12 @@
 
 The batched form of the C-ABI (include/p3m.h, p3m_batch_*): simulations of
 uneven body counts and grid sizes — the application's trajectory previews and
-ensembles — each keep a full context; one batch step is one CUDA graph launch
-that runs every simulation's step on its own stream. ``autotune`` picks launch
-shapes per grid by timing them.
+ensembles — each keep a full context. One batch step is, by default, ONE
+persistent cooperative kernel launch (captured in a CUDA graph) that runs
+every stage over all simulations phase by phase; ``set_persistent(False)``
+gives one launch per stage, ``set_fused(False)`` one step per simulation on
+its own stream. All forms give the same bits. ``autotune`` picks launch
+shapes by timing whole batch steps.
 """
 
 from __future__ import annotations
@@ -74,6 +77,33 @@ class GravityBatch:
         """One launch per stage for all simulations (default) or one step
         per simulation inside one graph; the results are the same bits."""
         self._check(self._lib.p3m_batch_set_fused(self._b, 1 if enabled else 0))
+
+    def set_persistent(self, enabled: bool, ctas_per_sm: int = 0) -> None:
+        """One persistent launch per batch step (default) or one launch per
+        stage; ``ctas_per_sm`` 0 keeps as many CTAs per SM as stay resident."""
+        self._check(self._lib.p3m_batch_set_persistent(self._b, 1 if enabled else 0, ctas_per_sm))
+
+    def set_barrier_fault(self, poll_limit: int = 1 << 20, withheld_cta: int = -1,
+                          phase: int = -1) -> None:
+        """Test hook of the persistent step's grid barrier: the poll limit of
+        each wait, and a CTA that never arrives after ``phase``. The defaults
+        clear it."""
+        self._check(self._lib.p3m_batch_set_barrier_fault(self._b, poll_limit, withheld_cta, phase))
+
+    def plan_info(self) -> dict:
+        """The last fused step's plan: persistent or not, kernel launches per
+        step, phases and CTAs of the persistent launch."""
+        out = np.zeros(4, np.int32)
+        self._check(self._lib.p3m_batch_plan_info(self._b, _ptr(out)))
+        return {"persistent": bool(out[0]), "launches": int(out[1]), "phases": int(out[2]),
+                "ctas": int(out[3])}
+
+    def phase_times(self) -> list[float]:
+        """Device milliseconds of each phase of the last persistent step."""
+        out = np.zeros(64, np.float64)
+        n = ctypes.c_int32(0)
+        self._check(self._lib.p3m_batch_phase_times(self._b, _ptr(out), 64, ctypes.byref(n)))
+        return [float(v) for v in out[:n.value]]
 
     def synchronize(self) -> None:
         self._check(self._lib.p3m_batch_synchronize(self._b))

@@ -1188,13 +1188,26 @@ struct p3m_batch {
         std::vector<std::pair<uint32_t*, uint32_t*>> sorted;
     };
     std::vector<Graph> graphs;
-    // Fused form: one launch per stage for every simulation (see batch_plan).
+    // Fused form: the stages of a step over all simulations at once, either
+    // as one persistent launch (the default) or one launch per stage.
     bool fused = true;
+    bool persistent = true;
+    int persistent_ctas_per_sm = 0;  // 0: as many as stay resident
+    // The persistent launch's grid barrier: polls before a wait gives up, and
+    // the test hook (a CTA that never arrives at one phase's barrier).
+    int barrier_polls = 1 << 20;
+    int withhold_cta = -1, withhold_phase = -1;
+    unsigned int* sync = nullptr;  // device: arrivals, waits given up
+    unsigned int reported_timeouts = 0;
+    unsigned long long* phase_ns = nullptr;  // device: the last launch's phase stamps
+    int32_t last_info[4] = {0, 0, 0, 0};     // of the last step's plan: see p3m_batch_plan_info
     struct Plan {
         std::vector<uint64_t> key;
         void* blob = nullptr;  // per-simulation arguments and block prefixes
         cudaGraphExec_t exec = nullptr;
         long long kernels = 0;
+        bool persistent = false;
+        int phases = 0, ctas = 0;
         std::vector<char> swap;  // simulations whose buffers the reorder swapped
         std::vector<std::pair<uint32_t*, uint32_t*>> sorted;
     };
@@ -1348,23 +1361,53 @@ struct BlobBuilder {
     }
 };
 
+// Each stage is recorded twice: as a launch of its batched kernel (the
+// per-stage form) and as an entry of the persistent kernel's stage table
+// with its phase (stages of one phase are independent of one another). Raw
+// launches (copies, stream forks) belong to the per-stage form only; the
+// persistent form has its own entries for them.
 struct FusedBuilder {
     BlobBuilder blob;
     std::vector<std::function<cudaError_t(unsigned char*, cudaStream_t)>> launches;
+    struct PEntry { p3m::PStage st; int phase; };
+    std::vector<PEntry> pstages;
+    bool persistent_ok = true;  // every stage has a persistent form
+    size_t pool = 0;            // the largest dynamic shared memory of a stage
 
-    template <typename Args, typename Fn>
-    void stage(const std::vector<Args>& args, const std::vector<int>& blocks, Fn fn) {
-        if (args.empty()) return;
+    template <typename Args>
+    bool offsets(const std::vector<Args>& args, const std::vector<int>& blocks, size_t* a_off,
+                 size_t* f_off, int* total) {
+        if (args.empty()) return false;
         std::vector<int> first(args.size() + 1, 0);
         for (size_t i = 0; i < args.size(); ++i) first[i + 1] = first[i] + blocks[i];
-        if (first.back() == 0) return;
-        const size_t a_off = blob.add(args.data(), args.size() * sizeof(Args));
-        const size_t f_off = blob.add(first.data(), first.size() * sizeof(int));
-        const int sims = (int)args.size(), total = first.back();
+        if (first.back() == 0) return false;
+        *a_off = blob.add(args.data(), args.size() * sizeof(Args));
+        *f_off = blob.add(first.data(), first.size() * sizeof(int));
+        *total = first.back();
+        return true;
+    }
+    template <typename Args, typename Fn>
+    void stage(const std::vector<Args>& args, const std::vector<int>& blocks, Fn fn, int kind,
+               int phase, size_t smem) {
+        size_t a_off, f_off;
+        int total;
+        if (!offsets(args, blocks, &a_off, &f_off, &total)) return;
+        const int sims = (int)args.size();
         launches.push_back([=](unsigned char* dev, cudaStream_t st) {
             p3m::BatchGrid g{reinterpret_cast<const int*>(dev + f_off), sims, total};
             return fn(reinterpret_cast<const Args*>(dev + a_off), g, st);
         });
+        if (kind < 0) persistent_ok = false;
+        pstages.push_back({{kind, sims, total, (int)a_off, (int)f_off}, phase});
+        pool = std::max(pool, smem);
+    }
+    template <typename Args>
+    void persistent_stage(const std::vector<Args>& args, const std::vector<int>& blocks, int kind,
+                          int phase) {
+        size_t a_off, f_off;
+        int total;
+        if (!offsets(args, blocks, &a_off, &f_off, &total)) return;
+        pstages.push_back({{kind, (int)args.size(), total, (int)a_off, (int)f_off}, phase});
     }
     void raw(std::function<cudaError_t(unsigned char*, cudaStream_t)> fn) { launches.push_back(fn); }
 };
@@ -1387,7 +1430,7 @@ struct SimRoles {
 // keys/vals ping-ponging between (keys, vals) and the sort scratch.
 void fused_radix(FusedBuilder& fb, const p3m_batch* b, const std::vector<int>& who,
                  const std::vector<int>& key_bits, std::vector<uint32_t*>& kin,
-                 std::vector<uint32_t*>& vin) {
+                 std::vector<uint32_t*>& vin, int& phase) {
     int max_passes = 0;
     std::vector<int> passes(who.size()), bits(who.size());
     for (size_t j = 0; j < who.size(); ++j) {
@@ -1420,15 +1463,17 @@ void fused_radix(FusedBuilder& fb, const p3m_batch* b, const std::vector<int>& w
             std::swap(kin[j], kout[j]);
             std::swap(vin[j], vout[j]);
         }
-        fb.stage(ra, tiles, p3m::batched_radix_hist);
-        fb.stage(sa, ones, p3m::batched_scan);
-        fb.stage(ra, tiles, p3m::batched_radix_scatter);
+        fb.stage(ra, tiles, p3m::batched_radix_hist, p3m::kPStageRadixHist, ++phase, 0);
+        fb.stage(sa, ones, p3m::batched_scan, p3m::kPStageScan, ++phase, 0);
+        fb.stage(ra, tiles, p3m::batched_radix_scatter, p3m::kPStageRadixScatter, ++phase,
+                 p3m::persistent_base_smem());
     }
 }
 
 int build_fused(p3m_batch* b, const std::vector<char>& sort, p3m_batch::Plan& plan) {
     const size_t S = b->sims.size();
     FusedBuilder fb;
+    int phase = 0;  // the persistent form's phase of the stages being added
     std::vector<SimRoles> role(S);
     plan.swap.assign(S, 0);
     for (size_t i = 0; i < S; ++i) {
@@ -1448,14 +1493,17 @@ int build_fused(p3m_batch* b, const std::vector<char>& sort, p3m_batch::Plan& pl
             ma.push_back({c->bodies, c->keys, c->vals, b->n[i], c->sort_wbits, c->sort_hbits});
             blocks.push_back((b->n[i] + 255) / 256);
         }
-        fb.stage(ma, blocks, p3m::batched_morton_keys);
+        fb.stage(ma, blocks, p3m::batched_morton_keys, p3m::kPStageMorton, phase, 0);
         std::vector<uint32_t*> kin(who.size()), vin(who.size());
         for (size_t j = 0; j < who.size(); ++j) {
             kin[j] = b->sims[who[j]]->keys;
             vin[j] = b->sims[who[j]]->vals;
         }
-        fused_radix(fb, b, who, bits, kin, vin);
+        fused_radix(fb, b, who, bits, kin, vin, phase);
+        ++phase;
         std::vector<p3m::PermuteArgs> pa;
+        std::vector<p3m::CopyArgs> copies;  // the persistent form's tail copies
+        std::vector<int> copy_blocks;
         for (size_t j = 0; j < who.size(); ++j) {
             p3m_ctx* c = b->sims[who[j]];
             const int n = b->n[who[j]];
@@ -1472,13 +1520,23 @@ int build_fused(p3m_batch* b, const std::vector<char>& sort, p3m_batch::Plan& pl
                     if (e == cudaSuccess) e = cudaMemcpyAsync(md, ms, tail * sizeof(float4), cudaMemcpyDeviceToDevice, st);
                     return e;
                 });
+                auto add_copy = [&](const void* src, void* dst, size_t bytes) {
+                    const long long words = (long long)(bytes / 4);
+                    copies.push_back({static_cast<const uint32_t*>(src), static_cast<uint32_t*>(dst), words});
+                    copy_blocks.push_back((int)((words + p3m::kBatchThreads - 1) / p3m::kBatchThreads));
+                };
+                add_copy(bs, bd, tail * sizeof(float4));
+                add_copy(as, ad, tail * sizeof(float2));
+                add_copy(ms, md, tail * sizeof(float4));
             }
             role[who[j]].bodies = c->bodies_alt;
             role[who[j]].accel = c->accel_alt;
             role[who[j]].materials = c->materials_alt;
             plan.swap[who[j]] = 1;
         }
-        fb.stage(pa, blocks, p3m::batched_permute);
+        fb.stage(pa, blocks, p3m::batched_permute, p3m::kPStagePermute, phase, 0);
+        fb.persistent_stage(copies, copy_blocks, p3m::kPStageCopy, phase);
+        if (!who.empty()) ++phase;
     }
     // 2. Drift, with the home-cell keys.
     {
@@ -1493,12 +1551,32 @@ int build_fused(p3m_batch* b, const std::vector<char>& sort, p3m_batch::Plan& pl
                           c->grid.bounded, c->grid.W, c->grid.H});
             blocks.push_back((b->n[i] + 255) / 256);
         }
-        fb.stage(da, blocks, p3m::batched_drift);
+        fb.stage(da, blocks, p3m::batched_drift, p3m::kPStageDrift, phase, 0);
     }
-    // 3. Cell lists (simulations with mutual gravity).
+    // 3. Cell lists (simulations with mutual gravity). The cell counts and
+    // masses and the density mesh are cleared beside the drift: nothing in
+    // the step reads them before the cell build and the deposit.
     std::vector<int> mut;
     for (size_t i = 0; i < S; ++i)
         if (b->sims[i]->mutual && b->n[i] > 0) mut.push_back((int)i);
+    {
+        std::vector<p3m::ZeroArgs> za;
+        std::vector<int> zb;
+        for (int i : mut) {
+            p3m_ctx* c = b->sims[i];
+            const long long P = (long long)phys_cells(c);
+            const int zblocks = (int)((P + p3m::kBatchThreads * 16 - 1) / (p3m::kBatchThreads * 16));
+            za.push_back({reinterpret_cast<uint32_t*>(c->cell_count), P});
+            za.push_back({c->cell_mass, P});
+            zb.push_back(zblocks);
+            zb.push_back(zblocks);
+            const bool i64 = c->cfg.deposit_mode == P3M_DEPOSIT_I64;
+            const long long words = (long long)mesh_cells(c) * (i64 ? 2 : 1);
+            za.push_back({static_cast<uint32_t*>(c->density), words});
+            zb.push_back((int)((words + p3m::kBatchThreads * 16 - 1) / (p3m::kBatchThreads * 16)));
+        }
+        fb.stage(za, zb, p3m::batched_zero, p3m::kPStageZero, phase, 0);
+    }
     {
         std::vector<int> bits;
         std::vector<uint32_t*> kin, vin;
@@ -1507,28 +1585,20 @@ int build_fused(p3m_batch* b, const std::vector<char>& sort, p3m_batch::Plan& pl
             kin.push_back(b->sims[i]->keys);
             vin.push_back(b->sims[i]->vals);
         }
-        fused_radix(fb, b, mut, bits, kin, vin);
-        std::vector<p3m::ZeroArgs> za;
-        std::vector<int> zb;
+        fused_radix(fb, b, mut, bits, kin, vin, phase);
         std::vector<p3m::CellBuildArgs> ca;
         std::vector<int> cb;
         for (size_t j = 0; j < mut.size(); ++j) {
             p3m_ctx* c = b->sims[mut[j]];
-            const long long P = (long long)phys_cells(c);
-            const int zblocks = (int)((P + p3m::kBatchThreads * 16 - 1) / (p3m::kBatchThreads * 16));
-            za.push_back({reinterpret_cast<uint32_t*>(c->cell_count), P});
-            za.push_back({c->cell_mass, P});
-            zb.push_back(zblocks);
-            zb.push_back(zblocks);
             role[mut[j]].sk = kin[j];
             role[mut[j]].sv = vin[j];
             ca.push_back({kin[j], vin[j], role[mut[j]].bodies, role[mut[j]].materials,
                           c->cell_start, c->cell_count, c->cell_mass, c->entries, b->n[mut[j]]});
             cb.push_back((b->n[mut[j]] + 255) / 256);
         }
-        fb.stage(za, zb, p3m::batched_zero);
-        fb.stage(ca, cb, p3m::batched_cell_build);
+        fb.stage(ca, cb, p3m::batched_cell_build, p3m::kPStageCellBuild, ++phase, 0);
     }
+    const int phase_lists = phase;  // the phase of the cell build
     // 4. Short range (by stencil shape) on the side stream: it reads only the
     // cell lists, so it runs beside the deposit and FFT.
     {
@@ -1556,7 +1626,7 @@ int build_fused(p3m_batch* b, const std::vector<char>& sort, p3m_batch::Plan& pl
             if (!sl.empty())
                 fb.stage(sl, slb, [side](const p3m::SlotsArgs* a, p3m::BatchGrid g, cudaStream_t) {
                     return p3m::batched_cell_slots(a, g, side);
-                });
+                }, p3m::kPStageSlots, phase_lists + 1, 0);
         }
         std::map<int, std::vector<int>> groups;  // rx * 64 + ry * 2 + two-slot form
         for (int i : mut) {
@@ -1573,25 +1643,20 @@ int build_fused(p3m_batch* b, const std::vector<char>& sort, p3m_batch::Plan& pl
                 sb.push_back((b->n[i] + p3m::kBatchThreads - 1) / p3m::kBatchThreads);
             }
             const int rx = kv.first / 64, ry = (kv.first % 64) / 2, ex = kv.first % 2;
+            // The persistent kernel carries the (3, 3) stencil only.
+            const int kind = rx == p3m::kPersistentRx && ry == p3m::kPersistentRy
+                                 ? (ex ? p3m::kPStageShortRangeSlots : p3m::kPStageShortRangeLists)
+                                 : -1;
             fb.stage(sa, sb, [rx, ry, ex, side](const p3m::ShortRangeArgs* a, p3m::BatchGrid g, cudaStream_t) {
                 return p3m::batched_short_range(a, g, rx, ry, ex, side);
-            });
+            }, kind, phase_lists + 2, ex ? p3m::persistent_base_smem() : 0);
         }
         cudaEvent_t join_ev = b->side_join;
         fb.raw([=](unsigned char*, cudaStream_t) { return cudaEventRecord(join_ev, side); });
     }
-    // 5. Mesh force: clear, deposit, FFT with the Green's multiply, inverse.
+    // 5. Mesh force (the mesh was cleared beside the drift): deposit, FFT with
+    // the Green's multiply, inverse.
     {
-        std::vector<p3m::ZeroArgs> za;
-        std::vector<int> zb;
-        for (int i : mut) {
-            p3m_ctx* c = b->sims[i];
-            const bool i64 = c->cfg.deposit_mode == P3M_DEPOSIT_I64;
-            const long long words = (long long)mesh_cells(c) * (i64 ? 2 : 1);
-            za.push_back({static_cast<uint32_t*>(c->density), words});
-            zb.push_back((int)((words + p3m::kBatchThreads * 16 - 1) / (p3m::kBatchThreads * 16)));
-        }
-        fb.stage(za, zb, p3m::batched_zero);
         for (int mode : {P3M_DEPOSIT_U32, P3M_DEPOSIT_I64}) {
             std::vector<p3m::DepositArgs> dep;
             std::vector<int> db;
@@ -1614,13 +1679,15 @@ int build_fused(p3m_batch* b, const std::vector<char>& sort, p3m_batch::Plan& pl
                 fblocks.push_back((g.MH / 2 + rp - 1) / rp);
                 smem = std::max(smem, rs);
             }
+            const bool i64 = mode == P3M_DEPOSIT_I64;
             fb.stage(dep, db, [mode](const p3m::DepositArgs* a, p3m::BatchGrid g, cudaStream_t st) {
                 return p3m::batched_deposit(a, g, mode, st);
-            });
+            }, i64 ? p3m::kPStageDepositI64 : p3m::kPStageDepositU32, phase_lists + 1,
+                     p3m::persistent_base_smem());
             const float2* tw0 = mut.empty() ? nullptr : b->sims[mut[0]]->twiddles;
             fb.stage(fr, fblocks, [mode, smem, tw0](const p3m::FftRowsArgs* a, p3m::BatchGrid g, cudaStream_t st) {
                 return p3m::batched_fft_rows(a, g, mode, smem, tw0, st);
-            });
+            }, i64 ? p3m::kPStageFftRowsI64 : p3m::kPStageFftRowsU32, phase_lists + 2, smem);
         }
         std::vector<p3m::FftColumnsArgs> fc;
         std::vector<p3m::FftInverseArgs> fi;
@@ -1642,10 +1709,10 @@ int build_fused(p3m_batch* b, const std::vector<char>& sort, p3m_batch::Plan& pl
         const float2* tw0 = mut.empty() ? nullptr : b->sims[mut[0]]->twiddles;
         fb.stage(fc, cbk, [csm, tw0](const p3m::FftColumnsArgs* a, p3m::BatchGrid g, cudaStream_t st) {
             return p3m::batched_fft_columns(a, g, csm, tw0, st);
-        });
+        }, p3m::kPStageFftColumns, phase_lists + 3, csm);
         fb.stage(fi, ibk, [ism, tw0](const p3m::FftInverseArgs* a, p3m::BatchGrid g, cudaStream_t st) {
             return p3m::batched_fft_inverse(a, g, ism, tw0, st);
-        });
+        }, p3m::kPStageFftInverse, phase_lists + 4, ism);
     }
     // 6. Interpolation + kick, after the short range has joined.
     {
@@ -1659,10 +1726,44 @@ int build_fused(p3m_batch* b, const std::vector<char>& sort, p3m_batch::Plan& pl
             ka.push_back({role[i].bodies, role[i].accel, c->force, c->a_short, kick_params(c, b->n[i], 0)});
             kb.push_back((b->n[i] + p3m::kBatchThreads - 1) / p3m::kBatchThreads);
         }
-        fb.stage(ka, kb, p3m::batched_interp_kick);
+        fb.stage(ka, kb, p3m::batched_interp_kick, p3m::kPStageKick, phase_lists + 5, 0);
     }
     plan.sorted.resize(S);
     for (size_t i = 0; i < S; ++i) plan.sorted[i] = {role[i].sk, role[i].sv};
+
+    // The persistent form: the stage table ordered by phase (empty phases
+    // dropped), in the blob beside the arguments, and the grid that stays
+    // resident with the largest stage's shared memory.
+    size_t st_off = 0, ph_off = 0, psmem = 0;
+    int n_phases = 0, ctas = 0;
+    plan.persistent = b->persistent && fb.persistent_ok && !fb.pstages.empty();
+    if (plan.persistent) {
+        std::stable_sort(fb.pstages.begin(), fb.pstages.end(),
+                         [](const FusedBuilder::PEntry& x, const FusedBuilder::PEntry& y) {
+                             return x.phase < y.phase;
+                         });
+        std::vector<p3m::PStage> table;
+        std::vector<p3m::PPhase> phases;
+        for (size_t k = 0; k < fb.pstages.size(); ++k) {
+            if (k == 0 || fb.pstages[k].phase != fb.pstages[k - 1].phase)
+                phases.push_back({(int)k, 0});
+            phases.back().stages++;
+            table.push_back(fb.pstages[k].st);
+        }
+        n_phases = (int)phases.size();
+        st_off = fb.blob.add(table.data(), table.size() * sizeof(p3m::PStage));
+        ph_off = fb.blob.add(phases.data(), phases.size() * sizeof(p3m::PPhase));
+        psmem = (std::max(fb.pool, p3m::persistent_base_smem()) + 15) & ~(size_t)15;
+        const int fit = p3m::persistent_ctas_per_sm(psmem);
+        int dev = 0, sms = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        const int per_sm = b->persistent_ctas_per_sm > 0 ? std::min(b->persistent_ctas_per_sm, fit) : fit;
+        ctas = sms * per_sm;
+        if (ctas <= 0) plan.persistent = false;  // cannot stay resident: per-stage launches
+    }
+    plan.phases = plan.persistent ? n_phases : 0;
+    plan.ctas = plan.persistent ? ctas : 0;
 
     // Upload the arguments, capture the launches.
     cudaError_t e = cudaMalloc(&plan.blob, std::max<size_t>(fb.blob.host.size(), 16));
@@ -1675,9 +1776,18 @@ int build_fused(p3m_batch* b, const std::vector<char>& sort, p3m_batch::Plan& pl
     e = cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal);
     if (e != cudaSuccess) return batch_fail(b, P3M_ERR_CUDA, cudaGetErrorString(e));
     cudaError_t le = cudaSuccess;
-    for (auto& fn : fb.launches) {
-        le = fn(dev, b->stream);
-        if (le != cudaSuccess) break;
+    if (plan.persistent) {
+        const float2* tw0 = mut.empty() ? nullptr : b->sims[mut[0]]->twiddles;
+        le = p3m::launch_batch_persistent(
+            dev, reinterpret_cast<const p3m::PStage*>(dev + st_off),
+            reinterpret_cast<const p3m::PPhase*>(dev + ph_off), n_phases, tw0, b->sync,
+            b->barrier_polls, b->withhold_cta, b->withhold_phase, ctas, psmem, b->phase_ns,
+            b->stream);
+    } else {
+        for (auto& fn : fb.launches) {
+            le = fn(dev, b->stream);
+            if (le != cudaSuccess) break;
+        }
     }
     cudaGraph_t graph = nullptr;
     e = cudaStreamEndCapture(b->stream, &graph);
@@ -1717,6 +1827,10 @@ int batch_fused_step(p3m_batch* b, const std::vector<char>& sort, const std::vec
     cudaError_t e = cudaGraphLaunch(plan->exec, b->stream);
     if (e != cudaSuccess) return batch_fail(b, P3M_ERR_CUDA, cudaGetErrorString(e));
     p3m::count_launches((int)plan->kernels);
+    b->last_info[0] = plan->persistent ? 1 : 0;
+    b->last_info[1] = (int32_t)plan->kernels;
+    b->last_info[2] = plan->phases;
+    b->last_info[3] = plan->ctas;
     for (size_t i = 0; i < b->sims.size(); ++i) {
         p3m_ctx* c = b->sims[i];
         if (plan->swap[i]) swap_body_buffers(c);
@@ -1751,6 +1865,133 @@ int time_direct_steps(p3m_ctx* c, int n, int steps, float* ms) {
     return P3M_OK;
 }
 
+// The fused form's autotuner. It times whole batch steps, the launches the
+// batch really runs: coordinate descent over the FFT lines per CTA of each
+// distinct grid in turn (the other grids held), then over the persistent
+// kernel's CTAs per SM. Every simulation's bodies, materials, accelerations
+// and step counter are saved first and put back after.
+int autotune_fused(p3m_batch* b, int trial_steps, int32_t* chosen) {
+    const size_t S = b->sims.size();
+    struct Saved { float4* bodies = nullptr; float4* materials = nullptr; float2* accel = nullptr; long long steps = 0; };
+    std::vector<Saved> saved(S);
+    cudaEvent_t t0 = nullptr, t1 = nullptr;
+    auto finish = [&](int st) {
+        for (auto& v : saved) {
+            if (v.bodies) cudaFree(v.bodies);
+            if (v.materials) cudaFree(v.materials);
+            if (v.accel) cudaFree(v.accel);
+        }
+        if (t0) cudaEventDestroy(t0);
+        if (t1) cudaEventDestroy(t1);
+        return st;
+    };
+    auto cuda_fail = [&](cudaError_t e) { return finish(batch_fail(b, P3M_ERR_CUDA, cudaGetErrorString(e))); };
+    cudaError_t e = cudaEventCreate(&t0);
+    if (e == cudaSuccess) e = cudaEventCreate(&t1);
+    if (e != cudaSuccess) return cuda_fail(e);
+    for (size_t i = 0; i < S; ++i) {
+        p3m_ctx* c = b->sims[i];
+        const size_t cap = (size_t)c->cfg.capacity;
+        e = cudaMalloc((void**)&saved[i].bodies, cap * sizeof(float4));
+        if (e == cudaSuccess) e = cudaMalloc((void**)&saved[i].materials, cap * sizeof(float4));
+        if (e == cudaSuccess) e = cudaMalloc((void**)&saved[i].accel, cap * sizeof(float2));
+        if (e != cudaSuccess) return finish(batch_fail(b, P3M_ERR_OUT_OF_MEMORY, "autotune state copies"));
+        e = cudaMemcpyAsync(saved[i].bodies, c->bodies, cap * sizeof(float4), cudaMemcpyDeviceToDevice, b->stream);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(saved[i].materials, c->materials, cap * sizeof(float4), cudaMemcpyDeviceToDevice, b->stream);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(saved[i].accel, c->accel, cap * sizeof(float2), cudaMemcpyDeviceToDevice, b->stream);
+        if (e != cudaSuccess) return cuda_fail(e);
+        saved[i].steps = c->physics_steps;
+    }
+    // One trial: fresh plans, four untimed steps (every plan of the reorder
+    // and buffer cycle built), then `trial_steps` timed steps.
+    auto trial = [&](float* ms) -> int {
+        batch_drop_graphs(b);
+        for (int w = 0; w < 4; ++w) {
+            int st = batch_one_step(b);
+            if (st != P3M_OK) return st;
+        }
+        cudaError_t te = cudaEventRecord(t0, b->stream);
+        for (int k = 0; k < trial_steps && te == cudaSuccess; ++k) {
+            int st = batch_one_step(b);
+            if (st != P3M_OK) return st;
+        }
+        if (te == cudaSuccess) te = cudaEventRecord(t1, b->stream);
+        if (te == cudaSuccess) te = cudaEventSynchronize(t1);
+        if (te == cudaSuccess) te = cudaEventElapsedTime(ms, t0, t1);
+        if (te != cudaSuccess) return batch_fail(b, P3M_ERR_CUDA, cudaGetErrorString(te));
+        return P3M_OK;
+    };
+    // The distinct grids, each with its simulations.
+    std::vector<std::vector<size_t>> groups;
+    for (size_t i = 0; i < S; ++i) {
+        const p3m_ctx* c = b->sims[i];
+        bool placed = false;
+        for (auto& g : groups) {
+            const p3m_ctx* q = b->sims[g[0]];
+            if (q->grid.W == c->grid.W && q->grid.H == c->grid.H && q->bounded == c->bounded) {
+                g.push_back(i);
+                placed = true;
+                break;
+            }
+        }
+        if (!placed) groups.push_back({i});
+    }
+    auto set_lines = [&](const std::vector<size_t>& g, int lines) {
+        for (size_t i : g) {
+            b->sims[i]->tune_fft_lines = lines;
+            b->sims[i]->grid = grid_for(b->sims[i]);
+        }
+    };
+    const int fft_choices[] = {0, 1, 2, 4, 8};
+    std::vector<int> best_lines(groups.size(), 0);
+    float ms = 0.0f;
+    for (size_t gi = 0; gi < groups.size(); ++gi) {
+        float best = 3.4e38f;
+        for (int f : fft_choices) {
+            set_lines(groups[gi], f);
+            int st = trial(&ms);
+            if (st != P3M_OK) return finish(st);
+            if (ms < best) { best = ms; best_lines[gi] = f; }
+        }
+        set_lines(groups[gi], best_lines[gi]);
+    }
+    if (b->persistent) {
+        float best = 3.4e38f;
+        int best_ctas = 0;
+        for (int per_sm : {0, 1, 2, 3}) {
+            b->persistent_ctas_per_sm = per_sm;
+            int st = trial(&ms);
+            if (st != P3M_OK) return finish(st);
+            if (ms < best) { best = ms; best_ctas = per_sm; }
+        }
+        b->persistent_ctas_per_sm = best_ctas;
+    }
+    // Put every simulation's state back (the buffer roles may have swapped;
+    // the contents are what matter).
+    e = cudaStreamSynchronize(b->stream);
+    if (e != cudaSuccess) return cuda_fail(e);
+    batch_drop_graphs(b);
+    for (size_t i = 0; i < S; ++i) {
+        p3m_ctx* c = b->sims[i];
+        const size_t cap = (size_t)c->cfg.capacity;
+        e = cudaMemcpyAsync(c->bodies, saved[i].bodies, cap * sizeof(float4), cudaMemcpyDeviceToDevice, b->stream);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(c->materials, saved[i].materials, cap * sizeof(float4), cudaMemcpyDeviceToDevice, b->stream);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(c->accel, saved[i].accel, cap * sizeof(float2), cudaMemcpyDeviceToDevice, b->stream);
+        if (e != cudaSuccess) return cuda_fail(e);
+        c->physics_steps = saved[i].steps;
+    }
+    e = cudaStreamSynchronize(b->stream);
+    if (e != cudaSuccess) return cuda_fail(e);
+    for (size_t gi = 0; gi < groups.size() && chosen && gi < 64; ++gi) {
+        const p3m_ctx* c = b->sims[groups[gi][0]];
+        chosen[4 * gi + 0] = c->grid.W;
+        chosen[4 * gi + 1] = c->grid.H;
+        chosen[4 * gi + 2] = best_lines[gi];
+        chosen[4 * gi + 3] = p3m::kBatchThreads;
+    }
+    return finish(P3M_OK);
+}
+
 }  // namespace
 
 extern "C" {
@@ -1763,6 +2004,8 @@ int p3m_batch_create(const p3m_config* configs, int32_t count, p3m_batch** out) 
     if (!b) return batch_fail(nullptr, P3M_ERR_OUT_OF_MEMORY, "host allocation failed");
     auto undo = [&](int st) {
         for (p3m_ctx* c : b->sims) p3m_destroy(c);
+        if (b->sync) cudaFree(b->sync);
+        if (b->phase_ns) cudaFree(b->phase_ns);
         for (cudaEvent_t e : b->join) cudaEventDestroy(e);
         if (b->fork) cudaEventDestroy(b->fork);
         if (b->side_fork) cudaEventDestroy(b->side_fork);
@@ -1778,6 +2021,13 @@ int p3m_batch_create(const p3m_config* configs, int32_t count, p3m_batch** out) 
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->side_join, cudaEventDisableTiming);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming);
     if (e != cudaSuccess) return undo(fail_cuda(nullptr, "batch stream/event", e));
+    e = cudaMalloc((void**)&b->sync, 2 * sizeof(unsigned int));
+    if (e == cudaSuccess)
+        e = cudaMalloc((void**)&b->phase_ns, p3m::kPersistentMaxStamps * sizeof(unsigned long long));
+    if (e == cudaSuccess) e = cudaMemset(b->sync, 0, 2 * sizeof(unsigned int));
+    if (e == cudaSuccess)
+        e = cudaMemset(b->phase_ns, 0, p3m::kPersistentMaxStamps * sizeof(unsigned long long));
+    if (e != cudaSuccess) return undo(fail_cuda(nullptr, "batch barrier words", e));
     for (int32_t i = 0; i < count; ++i) {
         p3m_ctx* c = nullptr;
         int st = p3m_create(&configs[i], &c);
@@ -1801,6 +2051,8 @@ int p3m_batch_destroy(p3m_batch* b) {
     cudaStreamSynchronize(b->stream);
     batch_drop_graphs(b);
     for (p3m_ctx* c : b->sims) p3m_destroy(c);
+    cudaFree(b->sync);
+    cudaFree(b->phase_ns);
     for (cudaEvent_t e : b->join) cudaEventDestroy(e);
     cudaEventDestroy(b->fork);
     cudaEventDestroy(b->side_fork);
@@ -1873,6 +2125,7 @@ int p3m_batch_autotune(p3m_batch* b, int32_t trial_steps, int32_t* chosen) {
     cudaError_t e = cudaStreamSynchronize(b->stream);
     if (e != cudaSuccess) return batch_fail(b, P3M_ERR_CUDA, cudaGetErrorString(e));
     batch_drop_graphs(b);
+    if (b->fused && fused_supported(b)) return autotune_fused(b, trial_steps, chosen);
     // One probe per distinct grid: the simulation with the most bodies.
     std::vector<size_t> probes;
     for (size_t i = 0; i < b->sims.size(); ++i) {
@@ -1970,6 +2223,64 @@ int p3m_batch_synchronize(p3m_batch* b) {
     if (!b) return P3M_ERR_INVALID_ARGUMENT;
     cudaError_t e = cudaStreamSynchronize(b->stream);
     if (e != cudaSuccess) return batch_fail(b, P3M_ERR_CUDA, cudaGetErrorString(e));
+    unsigned int gave_up = 0;  // grid-barrier waits that ran out, over all launches
+    e = cudaMemcpy(&gave_up, b->sync + 1, sizeof(gave_up), cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) return batch_fail(b, P3M_ERR_CUDA, cudaGetErrorString(e));
+    if (gave_up != b->reported_timeouts) {
+        b->reported_timeouts = gave_up;
+        return batch_fail(b, P3M_ERR_TIMEOUT,
+                          "a grid barrier of the persistent batch step gave up waiting (" +
+                              std::to_string(gave_up) + " waits so far); the simulations' "
+                              "state is incomplete and must be uploaded again");
+    }
+    return P3M_OK;
+}
+
+int p3m_batch_set_persistent(p3m_batch* b, int32_t enabled, int32_t ctas_per_sm) {
+    if (!b) return P3M_ERR_INVALID_ARGUMENT;
+    if (ctas_per_sm < 0) return batch_fail(b, P3M_ERR_INVALID_ARGUMENT, "ctas_per_sm must be >= 0");
+    cudaError_t e = cudaStreamSynchronize(b->stream);
+    if (e != cudaSuccess) return batch_fail(b, P3M_ERR_CUDA, cudaGetErrorString(e));
+    batch_drop_graphs(b);
+    b->persistent = enabled != 0;
+    b->persistent_ctas_per_sm = ctas_per_sm;
+    return P3M_OK;
+}
+
+int p3m_batch_set_barrier_fault(p3m_batch* b, int32_t poll_limit, int32_t withheld_cta,
+                                int32_t phase) {
+    if (!b) return P3M_ERR_INVALID_ARGUMENT;
+    if (poll_limit <= 0 || withheld_cta < -1 || phase < -1)
+        return batch_fail(b, P3M_ERR_INVALID_ARGUMENT,
+                          "poll_limit must be > 0, withheld_cta and phase >= -1");
+    cudaError_t e = cudaStreamSynchronize(b->stream);
+    if (e != cudaSuccess) return batch_fail(b, P3M_ERR_CUDA, cudaGetErrorString(e));
+    batch_drop_graphs(b);  // the plans bake the barrier's arguments in
+    b->barrier_polls = poll_limit;
+    b->withhold_cta = withheld_cta;
+    b->withhold_phase = phase;
+    return P3M_OK;
+}
+
+int p3m_batch_plan_info(p3m_batch* b, int32_t* info4) {
+    if (!b || !info4) return P3M_ERR_INVALID_ARGUMENT;
+    for (int i = 0; i < 4; ++i) info4[i] = b->last_info[i];
+    return P3M_OK;
+}
+
+int p3m_batch_phase_times(p3m_batch* b, double* ms, int32_t capacity, int32_t* phases) {
+    if (!b || !phases || capacity < 0 || (capacity > 0 && !ms)) return P3M_ERR_INVALID_ARGUMENT;
+    *phases = 0;
+    if (!b->last_info[0]) return P3M_OK;
+    const int np = std::min(b->last_info[2], p3m::kPersistentMaxStamps - 1);
+    cudaError_t e = cudaStreamSynchronize(b->stream);
+    if (e != cudaSuccess) return batch_fail(b, P3M_ERR_CUDA, cudaGetErrorString(e));
+    std::vector<unsigned long long> ns(np + 1, 0);
+    e = cudaMemcpy(ns.data(), b->phase_ns, ns.size() * sizeof(unsigned long long), cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) return batch_fail(b, P3M_ERR_CUDA, cudaGetErrorString(e));
+    for (int i = 0; i < np && i < capacity; ++i)
+        ms[i] = ns[i + 1] >= ns[i] ? (double)(ns[i + 1] - ns[i]) * 1e-6 : 0.0;
+    *phases = np;
     return P3M_OK;
 }
 

@@ -313,19 +313,51 @@ int p3m_batch_upload(p3m_batch* batch, int32_t sim, const float* bodies4,
 int p3m_batch_initialize_acceleration(p3m_batch* batch);
 /* `steps` steps of every simulation, one graph launch per step. */
 int p3m_batch_step(p3m_batch* batch, int32_t steps);
-/* Autotuner: for each distinct grid, times `trial_steps` steps of its largest
- * simulation under each candidate launch shape (FFT lines per CTA: automatic,
- * 1, 2, 4, 8; short-range block: 64, 128, 256 threads), keeps the fastest for
- * every simulation on that grid and restores the probe's state. Writes up to
- * 64 rows of (grid_width, grid_height, fft_lines, short_range_threads) to
- * `chosen` when it is not NULL. Results do not depend on the shapes. */
+/* Autotuner. Fused form: times `trial_steps` whole batch steps (after four
+ * untimed ones) under each candidate and keeps the fastest, by coordinate
+ * descent: FFT lines per CTA (automatic, 1, 2, 4, 8) for each distinct grid
+ * in turn, then the persistent launch's CTAs per SM (as many as fit, 1, 2,
+ * 3); every simulation's state is saved before and restored after. Other
+ * form: for each distinct grid, times `trial_steps` steps of its largest
+ * simulation under each FFT line count and short-range block (64, 128, 256
+ * threads) and restores that simulation's state. Writes up to 64 rows of
+ * (grid_width, grid_height, fft_lines, short_range_threads) to `chosen` when
+ * it is not NULL. Results do not depend on the choices. */
 int p3m_batch_autotune(p3m_batch* batch, int32_t trial_steps, int32_t* chosen);
-/* Fused form (the default): every stage of a batch step is one launch over
- * all simulations, captured once per plan. Off: every simulation enqueues
- * its own step (one graph over the simulations' streams). Both give the same
- * bits. The fused form needs every simulation at most 131,072 bodies; a
- * batch with a larger one runs the other form. */
+/* Fused form (the default): the stages of a batch step run over all
+ * simulations at once -- as ONE persistent cooperative launch per step (the
+ * default, p3m_batch_set_persistent), or one launch per stage -- captured
+ * once per plan. Off: every simulation enqueues its own step (one graph over
+ * the simulations' streams). All forms give the same bits. The fused form
+ * needs every simulation at most 131,072 bodies; a batch with a larger one
+ * runs the other form. */
 int p3m_batch_set_fused(p3m_batch* batch, int32_t enabled);
+/* Persistent form of the fused step (default on): one cooperative launch
+ * whose CTAs stay resident and run the step's stages phase by phase, a
+ * bounded grid barrier between phases. ctas_per_sm: CTAs per SM (0: as many
+ * as stay resident; larger values are clamped to that). A batch with a
+ * short-range stencil other than 3x3 cells (interaction radius), or whose
+ * stages cannot stay resident, takes the per-stage launches instead. */
+int p3m_batch_set_persistent(p3m_batch* batch, int32_t enabled, int32_t ctas_per_sm);
+/* Test hook of the persistent form's grid barrier: each wait polls the
+ * arrival counter at most poll_limit times (default 1 << 20, a few
+ * milliseconds to a second), then gives up, counts the wait and ends its CTA;
+ * withheld_cta (>= 0) never arrives at the barrier after phase `phase` (a
+ * CTA that does not arrive). -1 / -1 clears it. P3M_ERR_INVALID_ARGUMENT for
+ * poll_limit <= 0 or values below -1. */
+int p3m_batch_set_barrier_fault(p3m_batch* batch, int32_t poll_limit, int32_t withheld_cta,
+                                int32_t phase);
+/* The plan of the last fused step: info4 = (persistent 0/1, kernel launches
+ * per step, phases, CTAs of the persistent launch). All zero before one. */
+int p3m_batch_plan_info(p3m_batch* batch, int32_t* info4);
+/* Device time of each phase of the last persistent step (global-timer
+ * stamps by CTA 0 as it leaves each phase's barrier), in milliseconds, up to
+ * `capacity` values; *phases = the number of phases (0 when the last step was
+ * not persistent). Synchronises the batch's stream. */
+int p3m_batch_phase_times(p3m_batch* batch, double* ms, int32_t capacity, int32_t* phases);
+/* Waits for the batch's stream. P3M_ERR_TIMEOUT (once per new occurrence)
+ * when a grid barrier of a persistent step gave up: the simulations' state
+ * is then incomplete and must be uploaded again. */
 int p3m_batch_synchronize(p3m_batch* batch);
 int p3m_batch_get_stream(p3m_batch* batch, void** stream);
 
