@@ -696,8 +696,11 @@ def run_b200(args, ws, rank, local):
 
 
 def run_batch(args, ws, rank, local):
-    """256 simulations of uneven sizes stepped together (one graph launch per
-    batch step), after the autotuner has picked launch shapes per grid."""
+    """256 simulations of uneven sizes stepped together (one persistent
+    kernel launch per batch step, captured in a graph), after the autotuner
+    has picked launch shapes by timing whole batch steps. The same batch with
+    one launch per stage, and the simulations as serial runs, are timed
+    beside it."""
     import torch
 
     from gravity_b200.batch import GravityBatch
@@ -745,6 +748,31 @@ def run_batch(args, ws, rank, local):
     clk = clocks.stop()
     total_ms = allreduce_max(dist, sum(a.elapsed_time(b) for a, b in zip(starts, stops)))
     value = ws * total_n * args.steps / (total_ms / 1000.0)
+    plan = batch.plan_info()
+    plan["phase_ms_last_step"] = [round(t, 5) for t in batch.phase_times()]
+
+    # ---- the same batch with one launch per stage (the persistent kernel's
+    # stages as separate batched launches), timed the same way.
+    sms = torch.cuda.get_device_properties(local).multi_processor_count
+    per_sm = plan["ctas"] // sms if plan["ctas"] else 0
+    batch.set_persistent(False, per_sm)
+    batch.step(warmup)
+    batch.synchronize()
+    with torch.cuda.stream(stream):
+        for i in range(args.steps):
+            flush.zero_()
+            starts[i].record(stream)
+            batch.step(1)
+            stops[i].record(stream)
+    torch.cuda.synchronize()
+    batch.synchronize()
+    per_stage_plan = batch.plan_info()
+    ps_ms = allreduce_max(dist, sum(a.elapsed_time(b) for a, b in zip(starts, stops)))
+    plan["per_stage_launches_value"] = ws * total_n * args.steps / (ps_ms / 1000.0)
+    plan["per_stage_launches_per_step"] = per_stage_plan["launches"]
+    batch.set_persistent(True, per_sm)
+    batch.step(warmup)
+    batch.synchronize()
 
     # ---- e2e: every step uploads every simulation's body state from
     # page-locked memory (materials once, before timing), steps the batch and
@@ -856,6 +884,7 @@ def run_batch(args, ws, rank, local):
             "config": batch_config(scs, args),
             "autotuned": [{"grid": f"{r[0]}x{r[1]}", "fft_lines_per_cta": r[2] or "auto",
                            "short_range_threads": r[3]} for r in tuned],
+            "plan": plan,
             "serial_runs_value": serial_value,
             "overlapped_contexts_value": overlapped_value,
             "roofline": {"bound": "hbm", "kernel": dominant, "achieved": achieved, "peak": peak,

@@ -1,11 +1,14 @@
 """The batched form (p3m_batch_*) against simulations stepped one by one.
 
-In both forms of a batch step — fused (one launch per stage for every
-simulation) and per-simulation (one graph over the simulations' streams) —
-each simulation must come out bit for bit as the same simulation stepped
-alone in its own context, before and after the autotuner changes launch
-shapes, and across the reorder phases (a batch cycles through several
-captured plans).
+In every form of a batch step — persistent (one cooperative launch per step
+running all stages of all simulations phase by phase, the default),
+per-stage (one launch per stage for every simulation) and per-simulation
+(one graph over the simulations' streams) — each simulation must come out
+bit for bit as the same simulation stepped alone in its own context, before
+and after the autotuner changes launch shapes, and across the reorder
+phases (a batch cycles through several captured plans). The persistent
+step's grid barrier is bounded: a CTA that never arrives makes the waits run
+out, which the next synchronising call reports as P3M_ERR_TIMEOUT.
 """
 
 from dataclasses import replace
@@ -13,7 +16,7 @@ from dataclasses import replace
 import numpy as np
 import pytest
 
-from gravity_b200 import scenarios
+from gravity_b200 import _abi, scenarios
 from gravity_b200.batch import GravityBatch
 from gravity_b200.pipeline import GravityPipeline
 
@@ -38,17 +41,27 @@ def step_alone(sc, steps, field=(0.0, 0.0)):
         return p.download(sc.n)
 
 
+MODES = ("persistent", "per_stage", "per_simulation")
+
+
+def set_mode(batch, mode):
+    if mode == "per_stage":
+        batch.set_persistent(False)
+    elif mode == "per_simulation":
+        batch.set_fused(False)
+
+
 def assert_same(got, want, what):
     for g, w, name in zip(got, want, ("bodies", "materials", "acceleration")):
         np.testing.assert_array_equal(g, w, err_msg=f"{what}: {name}")
 
 
-@pytest.mark.parametrize("fused", [True, False])
-def test_batch_matches_individual_steps(cuda_device, fused):
+@pytest.mark.parametrize("mode", MODES)
+def test_batch_matches_individual_steps(cuda_device, mode):
     scs = mixed_batch()
     field = (0.0, 3.5)
     with GravityBatch([sc.config for sc in scs]) as batch:
-        batch.set_fused(fused)
+        set_mode(batch, mode)
         for i, sc in enumerate(scs):
             batch.upload(i, sc.bodies, sc.materials)
         batch.simulation(5).set_field_acceleration(*field)
@@ -59,11 +72,11 @@ def test_batch_matches_individual_steps(cuda_device, fused):
             assert_same(batch.download(i), want, f"simulation {i}")
 
 
-@pytest.mark.parametrize("fused", [True, False])
-def test_batch_after_autotune_is_unchanged(cuda_device, fused):
+@pytest.mark.parametrize("mode", MODES)
+def test_batch_after_autotune_is_unchanged(cuda_device, mode):
     scs = mixed_batch()
     with GravityBatch([sc.config for sc in scs]) as batch:
-        batch.set_fused(fused)
+        set_mode(batch, mode)
         for i, sc in enumerate(scs):
             batch.upload(i, sc.bodies, sc.materials)
         batch.initialize_acceleration()
@@ -73,6 +86,8 @@ def test_batch_after_autotune_is_unchanged(cuda_device, fused):
         assert {(r[0], r[1]) for r in rows} == grids
         assert all(r[2] in (0, 1, 2, 4, 8) and r[3] in (64, 128, 256) for r in rows)
         batch.step(4)
+        if mode == "persistent":
+            assert batch.plan_info()["persistent"]
         for i, sc in enumerate(scs):
             assert_same(batch.download(i), step_alone(sc, 7), f"simulation {i}")
 
@@ -98,3 +113,74 @@ def test_batch_rejects_bad_arguments(cuda_device):
             batch.step(-1)
         with pytest.raises(ValueError):
             batch.upload(0, np.zeros((scs[0].config.capacity + 1, 4), np.float32))
+
+
+def test_persistent_step_is_one_launch_and_matches_per_stage_launches(cuda_device):
+    scs = scenarios.batch(sims=24, seed=8, nmin=500, nmax=40000)
+    got = {}
+    for mode in ("persistent", "per_stage"):
+        with GravityBatch([sc.config for sc in scs]) as batch:
+            set_mode(batch, mode)
+            for i, sc in enumerate(scs):
+                batch.upload(i, sc.bodies, sc.materials)
+            batch.initialize_acceleration()
+            batch.step(4)
+            info = batch.plan_info()
+            if mode == "persistent":
+                assert info["persistent"] and info["launches"] == 1, info
+                assert info["phases"] >= 8 and info["ctas"] > 0, info
+                times = batch.phase_times()
+                assert len(times) == info["phases"] and all(t >= 0.0 for t in times)
+            else:
+                assert not info["persistent"] and info["launches"] > 10, info
+                assert batch.phase_times() == []
+            got[mode] = [batch.download(i) for i in range(len(scs))]
+    for i in range(len(scs)):
+        assert_same(got["persistent"][i], got["per_stage"][i], f"simulation {i}")
+
+
+def test_batch_workload_scale_matches_individual_steps(cuda_device):
+    """The trajectory-preview batch at its benchmark size: 256 simulations of
+    1,000 to 65,536 bodies on mixed grids, four steps (both reorder phases,
+    every captured plan of the cycle)."""
+    scs = scenarios.batch()
+    assert len(scs) == 256
+    with GravityBatch([sc.config for sc in scs]) as batch:
+        for i, sc in enumerate(scs):
+            batch.upload(i, sc.bodies, sc.materials)
+        batch.initialize_acceleration()
+        batch.step(4)
+        assert batch.plan_info()["persistent"]
+        for i, sc in enumerate(scs):
+            assert_same(batch.download(i), step_alone(sc, 4), f"simulation {i}")
+
+
+def test_persistent_barrier_that_runs_out_is_reported(cuda_device):
+    scs = scenarios.batch(sims=6, seed=9, nmin=500, nmax=8000)
+    with GravityBatch([sc.config for sc in scs]) as batch:
+        with pytest.raises(ValueError):
+            batch.set_barrier_fault(poll_limit=0)
+        with pytest.raises(ValueError):
+            batch.set_barrier_fault(withheld_cta=-2)
+        for i, sc in enumerate(scs):
+            batch.upload(i, sc.bodies, sc.materials)
+        batch.initialize_acceleration()
+        batch.step(1)
+        batch.synchronize()
+        # CTA 0 never arrives at the barrier after phase 2; every other CTA's
+        # wait gives up after 2,000 polls and its CTA ends.
+        batch.set_barrier_fault(poll_limit=2000, withheld_cta=0, phase=2)
+        batch.step(1)
+        with pytest.raises(_abi.P3MError) as err:
+            batch.synchronize()
+        assert err.value.status == _abi.P3M_ERR_TIMEOUT
+        batch.synchronize()  # reported once
+        # Cleared: the same batch steps correctly from a fresh upload.
+        batch.set_barrier_fault()
+        for i, sc in enumerate(scs):
+            batch.upload(i, sc.bodies, sc.materials)
+        batch.initialize_acceleration()
+        batch.step(3)
+        batch.synchronize()
+        for i, sc in enumerate(scs):
+            assert_same(batch.download(i), step_alone(sc, 3), f"simulation {i}")
