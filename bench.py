@@ -115,6 +115,10 @@ def run_only(args) -> None:
 
         scs = make_workload("batch", sims=args.sims)
         with GravityBatch([sc.config for sc in scs]) as b:
+            if args.batch_form == "per_stage":
+                b.set_persistent(False)
+            elif args.batch_form == "per_simulation":
+                b.set_fused(False)
             for i, sc in enumerate(scs):
                 b.upload(i, sc.bodies, sc.materials)
             b.initialize_acceleration()
@@ -1113,6 +1117,10 @@ def main():
     ap.add_argument("--bodies", type=int, default=None, help="override the workload's body count")
     ap.add_argument("--grid", default=None, help="override the workload's grid, WxH")
     ap.add_argument("--sims", type=int, default=None, help="batch: number of simulations")
+    ap.add_argument("--batch-form", default="persistent",
+                    choices=["persistent", "per_stage", "per_simulation"],
+                    help="batch --run-only: one persistent launch per step, one launch per "
+                         "stage, or one step per simulation")
     ap.add_argument("--run-only", action="store_true",
                     help="run the initial pass and --steps steps untimed (a profiler's target)")
     ap.add_argument("--previews", type=int, default=0,

@@ -69,11 +69,12 @@ __device__ __forceinline__ void scan256_body(uint32_t* data, int n, uint32_t* wa
     }
 }
 
-// Every stage kind's virtual block, each out of line: the kernel's register
-// budget then binds each body on its own instead of all of them at once.
+// Every stage kind's virtual block, each out of line (one function per
+// kind, no branch on the kind inside): registers are then allocated for each
+// body on its own, under the kernel's budget, instead of for all at once.
 namespace C = coherent::p3m;
 #define P3M_STAGE(name) \
-    __device__ __noinline__ void name(int kind, int2 sb, const unsigned char* args, const float2* tw, unsigned char* pool)
+    __device__ __noinline__ void name(int2 sb, const unsigned char* args, const float2* tw, unsigned char* pool)
 
 P3M_STAGE(stage_morton) {
     const MortonArgs a = reinterpret_cast<const MortonArgs*>(args)[sb.x];
@@ -126,37 +127,38 @@ P3M_STAGE(stage_slots) {
     C::cell_slots_body(sb.y, a.cell_start, a.cell_count, a.cell_mass, a.entries, a.W, a.H,
                        a.gravity, a.total_mass, a.slots);
 }
-P3M_STAGE(stage_short_range) {
+P3M_STAGE(stage_short_range_slots) {
     const ShortRangeArgs a = reinterpret_cast<const ShortRangeArgs*>(args)[sb.x];
-    if (kind == kPStageShortRangeSlots)
-        C::sr::short_range_body<kPersistentRx, kPersistentRy, 2>(
-            reinterpret_cast<C::sr::SlotStage*>(pool), sb.y, a.bodies, a.entries, a.cell_start,
-            a.cell_count, a.cell_mass, a.slots, a.a_short, a.p);
-    else
-        C::sr::short_range_body<kPersistentRx, kPersistentRy, 0>(
-            nullptr, sb.y, a.bodies, a.entries, a.cell_start, a.cell_count, a.cell_mass, a.slots,
-            a.a_short, a.p);
+    C::sr::short_range_body<kPersistentRx, kPersistentRy, 2>(
+        reinterpret_cast<C::sr::SlotStage*>(pool), sb.y, a.bodies, a.entries, a.cell_start,
+        a.cell_count, a.cell_mass, a.slots, a.a_short, a.p);
 }
-P3M_STAGE(stage_deposit) {
+P3M_STAGE(stage_short_range_lists) {
+    const ShortRangeArgs a = reinterpret_cast<const ShortRangeArgs*>(args)[sb.x];
+    C::sr::short_range_body<kPersistentRx, kPersistentRy, 0>(
+        nullptr, sb.y, a.bodies, a.entries, a.cell_start, a.cell_count, a.cell_mass, a.slots,
+        a.a_short, a.p);
+}
+P3M_STAGE(stage_deposit_i64) {
     const DepositArgs a = reinterpret_cast<const DepositArgs*>(args)[sb.x];
-    if (kind == kPStageDepositI64)
-        C::deposit_chunks_body<unsigned long long>(sb.y, a.entries, a.keys, a.n, a.W, a.H, a.MW,
-                                                   a.MH, a.scale,
-                                                   static_cast<unsigned long long*>(a.density),
-                                                   C::kWindowBytes / 8);
-    else
-        C::deposit_chunks_body<uint32_t>(sb.y, a.entries, a.keys, a.n, a.W, a.H, a.MW, a.MH,
-                                         a.scale, static_cast<uint32_t*>(a.density),
-                                         C::kWindowBytes / 4);
+    C::deposit_chunks_body<unsigned long long>(sb.y, a.entries, a.keys, a.n, a.W, a.H, a.MW, a.MH,
+                                               a.scale, static_cast<unsigned long long*>(a.density),
+                                               C::kWindowBytes / 8);
 }
-P3M_STAGE(stage_fft_rows) {
+P3M_STAGE(stage_deposit_u32) {
+    const DepositArgs a = reinterpret_cast<const DepositArgs*>(args)[sb.x];
+    C::deposit_chunks_body<uint32_t>(sb.y, a.entries, a.keys, a.n, a.W, a.H, a.MW, a.MH, a.scale,
+                                     static_cast<uint32_t*>(a.density), C::kWindowBytes / 4);
+}
+P3M_STAGE(stage_fft_rows_i64) {
     const FftRowsArgs a = reinterpret_cast<const FftRowsArgs*>(args)[sb.x];
-    if (kind == kPStageFftRowsI64)
-        C::fft_rows_forward_body<long long>(sb.y, static_cast<const long long*>(a.density),
-                                            a.inv_scale, a.MW, a.MH, a.per_cta, tw, a.half);
-    else
-        C::fft_rows_forward_body<uint32_t>(sb.y, static_cast<const uint32_t*>(a.density),
-                                           a.inv_scale, a.MW, a.MH, a.per_cta, tw, a.half);
+    C::fft_rows_forward_body<long long>(sb.y, static_cast<const long long*>(a.density), a.inv_scale,
+                                        a.MW, a.MH, a.per_cta, tw, a.half);
+}
+P3M_STAGE(stage_fft_rows_u32) {
+    const FftRowsArgs a = reinterpret_cast<const FftRowsArgs*>(args)[sb.x];
+    C::fft_rows_forward_body<uint32_t>(sb.y, static_cast<const uint32_t*>(a.density), a.inv_scale,
+                                       a.MW, a.MH, a.per_cta, tw, a.half);
 }
 P3M_STAGE(stage_fft_columns) {
     const FftColumnsArgs a = reinterpret_cast<const FftColumnsArgs*>(args)[sb.x];
@@ -190,25 +192,25 @@ __device__ __forceinline__ bool stage_uses_shared(int kind) {
 __device__ __forceinline__ void run_stage(int kind, int2 sb, const unsigned char* args,
                                           const float2* tw, unsigned char* pool) {
     switch (kind) {
-        case kPStageMorton: stage_morton(kind, sb, args, tw, pool); break;
-        case kPStageRadixHist: stage_radix_hist(kind, sb, args, tw, pool); break;
-        case kPStageScan: stage_scan(kind, sb, args, tw, pool); break;
-        case kPStageRadixScatter: stage_radix_scatter(kind, sb, args, tw, pool); break;
-        case kPStagePermute: stage_permute(kind, sb, args, tw, pool); break;
-        case kPStageCopy: stage_copy(kind, sb, args, tw, pool); break;
-        case kPStageDrift: stage_drift(kind, sb, args, tw, pool); break;
-        case kPStageZero: stage_zero(kind, sb, args, tw, pool); break;
-        case kPStageCellBuild: stage_cell_build(kind, sb, args, tw, pool); break;
-        case kPStageSlots: stage_slots(kind, sb, args, tw, pool); break;
-        case kPStageShortRangeSlots:
-        case kPStageShortRangeLists: stage_short_range(kind, sb, args, tw, pool); break;
-        case kPStageDepositU32:
-        case kPStageDepositI64: stage_deposit(kind, sb, args, tw, pool); break;
-        case kPStageFftRowsU32:
-        case kPStageFftRowsI64: stage_fft_rows(kind, sb, args, tw, pool); break;
-        case kPStageFftColumns: stage_fft_columns(kind, sb, args, tw, pool); break;
-        case kPStageFftInverse: stage_fft_inverse(kind, sb, args, tw, pool); break;
-        case kPStageKick: stage_kick(kind, sb, args, tw, pool); break;
+        case kPStageMorton: stage_morton(sb, args, tw, pool); break;
+        case kPStageRadixHist: stage_radix_hist(sb, args, tw, pool); break;
+        case kPStageScan: stage_scan(sb, args, tw, pool); break;
+        case kPStageRadixScatter: stage_radix_scatter(sb, args, tw, pool); break;
+        case kPStagePermute: stage_permute(sb, args, tw, pool); break;
+        case kPStageCopy: stage_copy(sb, args, tw, pool); break;
+        case kPStageDrift: stage_drift(sb, args, tw, pool); break;
+        case kPStageZero: stage_zero(sb, args, tw, pool); break;
+        case kPStageCellBuild: stage_cell_build(sb, args, tw, pool); break;
+        case kPStageSlots: stage_slots(sb, args, tw, pool); break;
+        case kPStageShortRangeSlots: stage_short_range_slots(sb, args, tw, pool); break;
+        case kPStageShortRangeLists: stage_short_range_lists(sb, args, tw, pool); break;
+        case kPStageDepositU32: stage_deposit_u32(sb, args, tw, pool); break;
+        case kPStageDepositI64: stage_deposit_i64(sb, args, tw, pool); break;
+        case kPStageFftRowsU32: stage_fft_rows_u32(sb, args, tw, pool); break;
+        case kPStageFftRowsI64: stage_fft_rows_i64(sb, args, tw, pool); break;
+        case kPStageFftColumns: stage_fft_columns(sb, args, tw, pool); break;
+        case kPStageFftInverse: stage_fft_inverse(sb, args, tw, pool); break;
+        case kPStageKick: stage_kick(sb, args, tw, pool); break;
         default: break;
     }
 }
