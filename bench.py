@@ -700,11 +700,11 @@ def run_b200(args, ws, rank, local):
 
 
 def run_batch(args, ws, rank, local):
-    """256 simulations of uneven sizes stepped together (one persistent
-    kernel launch per batch step, captured in a graph), after the autotuner
-    has picked launch shapes by timing whole batch steps. The same batch with
-    one launch per stage, and the simulations as serial runs, are timed
-    beside it."""
+    """256 simulations of uneven sizes stepped together (one graph launch per
+    batch step), after the autotuner has picked the form -- one launch per
+    stage or one persistent kernel launch -- and the launch shapes by timing
+    whole batch steps. The other form, and the simulations as serial runs,
+    are timed beside it."""
     import torch
 
     from gravity_b200.batch import GravityBatch
@@ -753,13 +753,15 @@ def run_batch(args, ws, rank, local):
     total_ms = allreduce_max(dist, sum(a.elapsed_time(b) for a, b in zip(starts, stops)))
     value = ws * total_n * args.steps / (total_ms / 1000.0)
     plan = batch.plan_info()
-    plan["phase_ms_last_step"] = [round(t, 5) for t in batch.phase_times()]
-
-    # ---- the same batch with one launch per stage (the persistent kernel's
-    # stages as separate batched launches), timed the same way.
+    chosen_persistent = plan["persistent"]
+    if chosen_persistent:
+        plan["phase_ms_last_step"] = [round(t, 5) for t in batch.phase_times()]
     sms = torch.cuda.get_device_properties(local).multi_processor_count
     per_sm = plan["ctas"] // sms if plan["ctas"] else 0
-    batch.set_persistent(False, per_sm)
+
+    # ---- the same batch in the other form (persistent <-> one launch per
+    # stage), timed the same way.
+    batch.set_persistent(not chosen_persistent, per_sm)
     batch.step(warmup)
     batch.synchronize()
     with torch.cuda.stream(stream):
@@ -770,11 +772,14 @@ def run_batch(args, ws, rank, local):
             stops[i].record(stream)
     torch.cuda.synchronize()
     batch.synchronize()
-    per_stage_plan = batch.plan_info()
-    ps_ms = allreduce_max(dist, sum(a.elapsed_time(b) for a, b in zip(starts, stops)))
-    plan["per_stage_launches_value"] = ws * total_n * args.steps / (ps_ms / 1000.0)
-    plan["per_stage_launches_per_step"] = per_stage_plan["launches"]
-    batch.set_persistent(True, per_sm)
+    other = batch.plan_info()
+    other_ms = allreduce_max(dist, sum(a.elapsed_time(b) for a, b in zip(starts, stops)))
+    other["value"] = ws * total_n * args.steps / (other_ms / 1000.0)
+    other["ms_per_step"] = other_ms / args.steps
+    if other["persistent"]:
+        other["phase_ms_last_step"] = [round(t, 5) for t in batch.phase_times()]
+    plan["other_form"] = other
+    batch.set_persistent(chosen_persistent, per_sm)
     batch.step(warmup)
     batch.synchronize()
 

@@ -2,12 +2,12 @@
 
 The batched form of the C-ABI (include/p3m.h, p3m_batch_*): simulations of
 uneven body counts and grid sizes — the application's trajectory previews and
-ensembles — each keep a full context. One batch step is, by default, ONE
-persistent cooperative kernel launch (captured in a CUDA graph) that runs
-every stage over all simulations phase by phase; ``set_persistent(False)``
-gives one launch per stage, ``set_fused(False)`` one step per simulation on
-its own stream. All forms give the same bits. ``autotune`` picks launch
-shapes by timing whole batch steps.
+ensembles — each keep a full context. One batch step is, by default, one
+launch per stage over all simulations (captured in a CUDA graph);
+``set_persistent(True)`` makes it ONE persistent cooperative kernel launch
+that runs every stage phase by phase, ``set_fused(False)`` one step per
+simulation on its own stream. All forms give the same bits. ``autotune``
+picks the form and launch shapes by timing whole batch steps.
 """
 
 from __future__ import annotations
@@ -79,8 +79,9 @@ class GravityBatch:
         self._check(self._lib.p3m_batch_set_fused(self._b, 1 if enabled else 0))
 
     def set_persistent(self, enabled: bool, ctas_per_sm: int = 0) -> None:
-        """One persistent launch per batch step (default) or one launch per
-        stage; ``ctas_per_sm`` 0 keeps as many CTAs per SM as stay resident."""
+        """One persistent launch per batch step, or one launch per stage (the
+        default); ``ctas_per_sm`` 0 keeps as many CTAs per SM as stay
+        resident."""
         self._check(self._lib.p3m_batch_set_persistent(self._b, 1 if enabled else 0, ctas_per_sm))
 
     def set_barrier_fault(self, poll_limit: int = 1 << 20, withheld_cta: int = -1,

@@ -1189,9 +1189,9 @@ struct p3m_batch {
     };
     std::vector<Graph> graphs;
     // Fused form: the stages of a step over all simulations at once, either
-    // as one persistent launch (the default) or one launch per stage.
+    // as one launch per stage (the default) or as one persistent launch.
     bool fused = true;
-    bool persistent = true;
+    bool persistent = false;
     int persistent_ctas_per_sm = 0;  // 0: as many as stay resident
     // The persistent launch's grid barrier: polls before a wait gives up, and
     // the test hook (a CTA that never arrives at one phase's barrier).
@@ -1866,10 +1866,12 @@ int time_direct_steps(p3m_ctx* c, int n, int steps, float* ms) {
 }
 
 // The fused form's autotuner. It times whole batch steps, the launches the
-// batch really runs: coordinate descent over the FFT lines per CTA of each
-// distinct grid in turn (the other grids held), then over the persistent
-// kernel's CTAs per SM. Every simulation's bodies, materials, accelerations
-// and step counter are saved first and put back after.
+// batch really runs: first the form (one launch per stage, or the persistent
+// launch with as many CTAs per SM as stay resident), then coordinate descent
+// over the FFT lines per CTA of each distinct grid in turn (the other grids
+// held), then, for the persistent form, over its CTAs per SM. Every
+// simulation's bodies, materials, accelerations and step counter are saved
+// first and put back after.
 int autotune_fused(p3m_batch* b, int trial_steps, int32_t* chosen) {
     const size_t S = b->sims.size();
     struct Saved { float4* bodies = nullptr; float4* materials = nullptr; float2* accel = nullptr; long long steps = 0; };
@@ -1945,6 +1947,18 @@ int autotune_fused(p3m_batch* b, int trial_steps, int32_t* chosen) {
     const int fft_choices[] = {0, 1, 2, 4, 8};
     std::vector<int> best_lines(groups.size(), 0);
     float ms = 0.0f;
+    {
+        float best = 3.4e38f;
+        bool best_form = false;
+        for (bool form : {false, true}) {
+            b->persistent = form;
+            b->persistent_ctas_per_sm = 0;
+            int st = trial(&ms);
+            if (st != P3M_OK) return finish(st);
+            if (ms < best) { best = ms; best_form = form; }
+        }
+        b->persistent = best_form;
+    }
     for (size_t gi = 0; gi < groups.size(); ++gi) {
         float best = 3.4e38f;
         for (int f : fft_choices) {

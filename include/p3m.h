@@ -315,9 +315,11 @@ int p3m_batch_initialize_acceleration(p3m_batch* batch);
 int p3m_batch_step(p3m_batch* batch, int32_t steps);
 /* Autotuner. Fused form: times `trial_steps` whole batch steps (after four
  * untimed ones) under each candidate and keeps the fastest, by coordinate
- * descent: FFT lines per CTA (automatic, 1, 2, 4, 8) for each distinct grid
- * in turn, then the persistent launch's CTAs per SM (as many as fit, 1, 2,
- * 3); every simulation's state is saved before and restored after. Other
+ * descent: the form (one launch per stage, or one persistent launch), FFT
+ * lines per CTA (automatic, 1, 2, 4, 8) for each distinct grid in turn, then
+ * for the persistent form its CTAs per SM (as many as fit, 1, 2, 3); every
+ * simulation's state is saved before and restored after (the choice of form
+ * stays; p3m_batch_plan_info reports it). Other
  * form: for each distinct grid, times `trial_steps` steps of its largest
  * simulation under each FFT line count and short-range block (64, 128, 256
  * threads) and restores that simulation's state. Writes up to 64 rows of
@@ -325,16 +327,19 @@ int p3m_batch_step(p3m_batch* batch, int32_t steps);
  * it is not NULL. Results do not depend on the choices. */
 int p3m_batch_autotune(p3m_batch* batch, int32_t trial_steps, int32_t* chosen);
 /* Fused form (the default): the stages of a batch step run over all
- * simulations at once -- as ONE persistent cooperative launch per step (the
- * default, p3m_batch_set_persistent), or one launch per stage -- captured
- * once per plan. Off: every simulation enqueues its own step (one graph over
+ * simulations at once -- one launch per stage (the default), or ONE
+ * persistent cooperative launch per step (p3m_batch_set_persistent) --
+ * captured once per plan. Off: every simulation enqueues its own step (one graph over
  * the simulations' streams). All forms give the same bits. The fused form
  * needs every simulation at most 131,072 bodies; a batch with a larger one
  * runs the other form. */
 int p3m_batch_set_fused(p3m_batch* batch, int32_t enabled);
-/* Persistent form of the fused step (default on): one cooperative launch
- * whose CTAs stay resident and run the step's stages phase by phase, a
- * bounded grid barrier between phases. ctas_per_sm: CTAs per SM (0: as many
+/* Persistent form of the fused step (default off; the autotuner picks the
+ * faster form): one cooperative launch whose CTAs stay resident and run the
+ * step's stages phase by phase, a bounded grid barrier between phases. Its
+ * one register budget is the largest stage's (the radix scatter's), so it
+ * keeps fewer warps per SM than the per-stage launches; it wins where the
+ * launches' gaps outweigh that (many short stages). ctas_per_sm: CTAs per SM (0: as many
  * as stay resident; larger values are clamped to that). A batch with a
  * short-range stencil other than 3x3 cells (interaction radius), or whose
  * stages cannot stay resident, takes the per-stage launches instead. */

@@ -1,8 +1,8 @@
 """The batched form (p3m_batch_*) against simulations stepped one by one.
 
-In every form of a batch step — persistent (one cooperative launch per step
-running all stages of all simulations phase by phase, the default),
-per-stage (one launch per stage for every simulation) and per-simulation
+In every form of a batch step — per-stage (one launch per stage for every
+simulation, the default), persistent (one cooperative launch per step
+running all stages of all simulations phase by phase) and per-simulation
 (one graph over the simulations' streams) — each simulation must come out
 bit for bit as the same simulation stepped alone in its own context, before
 and after the autotuner changes launch shapes, and across the reorder
@@ -45,7 +45,9 @@ MODES = ("persistent", "per_stage", "per_simulation")
 
 
 def set_mode(batch, mode):
-    if mode == "per_stage":
+    if mode == "persistent":
+        batch.set_persistent(True)
+    elif mode == "per_stage":
         batch.set_persistent(False)
     elif mode == "per_simulation":
         batch.set_fused(False)
@@ -86,8 +88,8 @@ def test_batch_after_autotune_is_unchanged(cuda_device, mode):
         assert {(r[0], r[1]) for r in rows} == grids
         assert all(r[2] in (0, 1, 2, 4, 8) and r[3] in (64, 128, 256) for r in rows)
         batch.step(4)
-        if mode == "persistent":
-            assert batch.plan_info()["persistent"]
+        if mode != "per_simulation":
+            assert batch.plan_info()["launches"] >= 1  # a fused plan ran (either form)
         for i, sc in enumerate(scs):
             assert_same(batch.download(i), step_alone(sc, 7), f"simulation {i}")
 
@@ -145,19 +147,26 @@ def test_batch_workload_scale_matches_individual_steps(cuda_device):
     every captured plan of the cycle)."""
     scs = scenarios.batch()
     assert len(scs) == 256
-    with GravityBatch([sc.config for sc in scs]) as batch:
-        for i, sc in enumerate(scs):
-            batch.upload(i, sc.bodies, sc.materials)
-        batch.initialize_acceleration()
-        batch.step(4)
-        assert batch.plan_info()["persistent"]
-        for i, sc in enumerate(scs):
-            assert_same(batch.download(i), step_alone(sc, 4), f"simulation {i}")
+    got = {}
+    for mode in ("per_stage", "persistent"):
+        with GravityBatch([sc.config for sc in scs]) as batch:
+            set_mode(batch, mode)
+            for i, sc in enumerate(scs):
+                batch.upload(i, sc.bodies, sc.materials)
+            batch.initialize_acceleration()
+            batch.step(4)
+            assert batch.plan_info()["persistent"] == (mode == "persistent")
+            got[mode] = [batch.download(i) for i in range(len(scs))]
+    for i, sc in enumerate(scs):
+        want = step_alone(sc, 4)
+        for mode in got:
+            assert_same(got[mode][i], want, f"{mode}: simulation {i}")
 
 
 def test_persistent_barrier_that_runs_out_is_reported(cuda_device):
     scs = scenarios.batch(sims=6, seed=9, nmin=500, nmax=8000)
     with GravityBatch([sc.config for sc in scs]) as batch:
+        batch.set_persistent(True)
         with pytest.raises(ValueError):
             batch.set_barrier_fault(poll_limit=0)
         with pytest.raises(ValueError):
