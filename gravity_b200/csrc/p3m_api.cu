@@ -586,6 +586,8 @@ size_t buffer_bytes(const p3m_ctx* ctx, int which, void** dptr) {
     }
 }
 
+int autotune_context(p3m_ctx* c, int n, int trial_steps, int* best_fft_out, int* best_sr_out);
+
 }  // namespace
 
 namespace p3m {
@@ -899,6 +901,39 @@ int p3m_step(p3m_ctx* ctx, int32_t n, int32_t steps) {
     for (int i = 0; i < steps; ++i) {
         st = one_step(ctx, n);
         if (st != P3M_OK) return st;
+    }
+    return P3M_OK;
+}
+
+int p3m_set_launch_shape(p3m_ctx* ctx, int32_t fft_lines, int32_t short_range_threads) {
+    if (!ctx) return P3M_ERR_INVALID_ARGUMENT;
+    if (fft_lines < 0 || fft_lines > 16)
+        return fail(ctx, P3M_ERR_INVALID_ARGUMENT, "fft_lines must be in [0, 16]");
+    if (short_range_threads != 64 && short_range_threads != 128 && short_range_threads != 256)
+        return fail(ctx, P3M_ERR_INVALID_ARGUMENT, "short_range_threads must be 64, 128 or 256");
+    P3M_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    ctx->tune_fft_lines = fft_lines;
+    ctx->tune_sr_threads = short_range_threads;
+    ctx->grid = grid_for(ctx);
+    drop_graphs(ctx);
+    return P3M_OK;
+}
+
+int p3m_autotune(p3m_ctx* ctx, int32_t n, int32_t trial_steps, int32_t* chosen2) {
+    int st = check_n(ctx, n);
+    if (st != P3M_OK) return st;
+    if (trial_steps <= 0) return fail(ctx, P3M_ERR_INVALID_ARGUMENT, "trial_steps must be > 0");
+    if (n == 0) return fail(ctx, P3M_ERR_STATE, "autotune needs active bodies");
+    P3M_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    normalize_to(ctx, n);
+    st = ensure_green(ctx);
+    if (st != P3M_OK) return st;
+    int f = 0, t = 256;
+    st = autotune_context(ctx, n, trial_steps, &f, &t);
+    if (st != P3M_OK) return st;
+    if (chosen2) {
+        chosen2[0] = f;
+        chosen2[1] = t;
     }
     return P3M_OK;
 }
@@ -1865,6 +1900,64 @@ int time_direct_steps(p3m_ctx* c, int n, int steps, float* ms) {
     return P3M_OK;
 }
 
+// Launch shapes of one context by timing: `trial_steps` direct steps (after
+// one untimed step) under each FFT line count per CTA (automatic, 1, 2, 4,
+// 8), then each short-range block (64, 128, 256 threads) with the best line
+// count. The trials step the context; its bodies, materials, accelerations
+// and step counter are put back afterwards (the buffer roles may have
+// swapped: the contents are what matter). Leaves the best shapes set.
+int autotune_context(p3m_ctx* c, int n, int trial_steps, int* best_fft_out, int* best_sr_out) {
+    const size_t cap = (size_t)c->cfg.capacity;
+    float4 *sb = nullptr, *sm = nullptr;
+    float2* sa = nullptr;
+    const long long steps_before = c->physics_steps;
+    P3M_CUDA(c, cudaMallocAsync((void**)&sb, cap * sizeof(float4), c->stream));
+    P3M_CUDA(c, cudaMallocAsync((void**)&sm, cap * sizeof(float4), c->stream));
+    P3M_CUDA(c, cudaMallocAsync((void**)&sa, cap * sizeof(float2), c->stream));
+    P3M_CUDA(c, cudaMemcpyAsync(sb, c->bodies, cap * sizeof(float4), cudaMemcpyDeviceToDevice, c->stream));
+    P3M_CUDA(c, cudaMemcpyAsync(sm, c->materials, cap * sizeof(float4), cudaMemcpyDeviceToDevice, c->stream));
+    P3M_CUDA(c, cudaMemcpyAsync(sa, c->accel, cap * sizeof(float2), cudaMemcpyDeviceToDevice, c->stream));
+    auto trial = [&](float* ms) -> int {
+        c->grid = grid_for(c);
+        int st = time_direct_steps(c, n, 1, ms);  // warm-up
+        if (st == P3M_OK) st = time_direct_steps(c, n, trial_steps, ms);
+        return st;
+    };
+    const int fft_choices[] = {0, 1, 2, 4, 8};
+    const int sr_choices[] = {64, 128, 256};
+    int best_fft = 0, best_sr = 256;
+    float best = 3.4e38f, ms = 0.0f;
+    c->tune_sr_threads = 256;
+    for (int f : fft_choices) {
+        c->tune_fft_lines = f;
+        int st = trial(&ms);
+        if (st != P3M_OK) return st;
+        if (ms < best) { best = ms; best_fft = f; }
+    }
+    c->tune_fft_lines = best_fft;
+    best = 3.4e38f;
+    for (int t : sr_choices) {
+        c->tune_sr_threads = t;
+        int st = trial(&ms);
+        if (st != P3M_OK) return st;
+        if (ms < best) { best = ms; best_sr = t; }
+    }
+    c->tune_sr_threads = best_sr;
+    c->grid = grid_for(c);
+    P3M_CUDA(c, cudaMemcpyAsync(c->bodies, sb, cap * sizeof(float4), cudaMemcpyDeviceToDevice, c->stream));
+    P3M_CUDA(c, cudaMemcpyAsync(c->materials, sm, cap * sizeof(float4), cudaMemcpyDeviceToDevice, c->stream));
+    P3M_CUDA(c, cudaMemcpyAsync(c->accel, sa, cap * sizeof(float2), cudaMemcpyDeviceToDevice, c->stream));
+    cudaFreeAsync(sb, c->stream);
+    cudaFreeAsync(sm, c->stream);
+    cudaFreeAsync(sa, c->stream);
+    P3M_CUDA(c, cudaStreamSynchronize(c->stream));
+    c->physics_steps = steps_before;
+    drop_graphs(c);
+    *best_fft_out = best_fft;
+    *best_sr_out = best_sr;
+    return P3M_OK;
+}
+
 // The fused form's autotuner. It times whole batch steps, the launches the
 // batch really runs: first the form (one launch per stage, or the persistent
 // launch with as many CTAs per SM as stay resident), then coordinate descent
@@ -2155,55 +2248,12 @@ int p3m_batch_autotune(p3m_batch* b, int32_t trial_steps, int32_t* chosen) {
         }
         if (!placed) probes.push_back(i);
     }
-    const int fft_choices[] = {0, 1, 2, 4, 8};
-    const int sr_choices[] = {64, 128, 256};
     int tuned = 0;
     for (size_t p : probes) {
         p3m_ctx* c = b->sims[p];
-        const int n = b->n[p];
-        const size_t cap = (size_t)c->cfg.capacity;
-        // The trials step the probe; its state is put back afterwards.
-        float4 *sb = nullptr, *sm = nullptr;
-        float2* sa = nullptr;
-        const long long steps_before = c->physics_steps;
-        P3M_CUDA(c, cudaMallocAsync((void**)&sb, cap * sizeof(float4), c->stream));
-        P3M_CUDA(c, cudaMallocAsync((void**)&sm, cap * sizeof(float4), c->stream));
-        P3M_CUDA(c, cudaMallocAsync((void**)&sa, cap * sizeof(float2), c->stream));
-        P3M_CUDA(c, cudaMemcpyAsync(sb, c->bodies, cap * sizeof(float4), cudaMemcpyDeviceToDevice, c->stream));
-        P3M_CUDA(c, cudaMemcpyAsync(sm, c->materials, cap * sizeof(float4), cudaMemcpyDeviceToDevice, c->stream));
-        P3M_CUDA(c, cudaMemcpyAsync(sa, c->accel, cap * sizeof(float2), cudaMemcpyDeviceToDevice, c->stream));
-        auto trial = [&](float* ms) -> int {
-            c->grid = grid_for(c);
-            int st = time_direct_steps(c, n, 1, ms);  // warm-up
-            if (st == P3M_OK) st = time_direct_steps(c, n, trial_steps, ms);
-            return st;
-        };
         int best_fft = 0, best_sr = 256;
-        float best = 3.4e38f, ms = 0.0f;
-        c->tune_sr_threads = 256;
-        for (int f : fft_choices) {
-            c->tune_fft_lines = f;
-            int st = trial(&ms);
-            if (st != P3M_OK) return batch_fail_ctx(b, p, st);
-            if (ms < best) { best = ms; best_fft = f; }
-        }
-        c->tune_fft_lines = best_fft;
-        best = 3.4e38f;
-        for (int t : sr_choices) {
-            c->tune_sr_threads = t;
-            int st = trial(&ms);
-            if (st != P3M_OK) return batch_fail_ctx(b, p, st);
-            if (ms < best) { best = ms; best_sr = t; }
-        }
-        // Put the probe's state back (the buffer roles may have swapped).
-        P3M_CUDA(c, cudaMemcpyAsync(c->bodies, sb, cap * sizeof(float4), cudaMemcpyDeviceToDevice, c->stream));
-        P3M_CUDA(c, cudaMemcpyAsync(c->materials, sm, cap * sizeof(float4), cudaMemcpyDeviceToDevice, c->stream));
-        P3M_CUDA(c, cudaMemcpyAsync(c->accel, sa, cap * sizeof(float2), cudaMemcpyDeviceToDevice, c->stream));
-        cudaFreeAsync(sb, c->stream);
-        cudaFreeAsync(sm, c->stream);
-        cudaFreeAsync(sa, c->stream);
-        P3M_CUDA(c, cudaStreamSynchronize(c->stream));
-        c->physics_steps = steps_before;
+        int st = autotune_context(c, b->n[p], trial_steps, &best_fft, &best_sr);
+        if (st != P3M_OK) return batch_fail_ctx(b, p, st);
         for (size_t i = 0; i < b->sims.size(); ++i) {
             p3m_ctx* o = b->sims[i];
             if (o->grid.W == c->grid.W && o->grid.H == c->grid.H && o->bounded == c->bounded) {

@@ -14,20 +14,26 @@
 namespace p3m {
 namespace {
 
-// floorf(v) without the conversion unit (the drift's 32 floors per body
-// otherwise saturate it): for |v| < 2^23 the round-down sum v + 2^23 (with
-// v's sign) has a unit in the last place of 1, so subtracting 2^23 again
-// leaves floor(v) exactly; copysign restores floorf's signed zero. Larger
-// |v|, infinities and NaN are their own floor.
-__device__ __forceinline__ float floor_exact(float v) {
-    const float m = copysignf(8388608.0f, v);
-    const float f = copysignf(__fsub_rn(__fadd_rd(v, m), m), v);
-    return fabsf(v) < 8388608.0f ? f : v;
+// v - floor(v) for v in [-1, 2) without the conversion unit: -floor(v) is
+// 1, +0 or -1 from two compares, and v + (-floor(v)) is the same single
+// rounding as v - floor(v) (for v = -0 both give +0).
+__device__ __forceinline__ float fract_near(float v) {
+    const float neg_floor = __fsub_rn((float)(v < 0.0f), (float)(v >= 1.0f));
+    return __fadd_rn(v, neg_floor);
 }
 
-__device__ __forceinline__ float fractf(float v) { return __fsub_rn(v, floor_exact(v)); }
+__device__ __forceinline__ float fract_any(float v) { return __fsub_rn(v, floorf(v)); }
 
 // Drifts body `id` (when id < n) and writes its cell key; returns the key.
+//
+// Substep 0 kicks by a*dt/2, every later substep by a*0 (kickDt = 0,
+// GravityPipeline.kt:465-473). Adding the same a*0 (a signed zero, or NaN
+// for a non-finite a) a second time changes nothing, so from substep 1 on
+// the velocity, and with it the displacement v*dt/S, are the same: they are
+// computed once. On the torus, when the position is in [0, 1] and the
+// displacement below half a period, every later substep's sum stays in
+// [-1, 2), where fract_near is exact; one axis takes it and the other the
+// conversion unit's floor, so neither pipe limits the loop.
 __device__ __forceinline__ uint32_t drift_one(int id, float4* __restrict__ bodies,
                                               const float2* __restrict__ accel, int n,
                                               float half_kick, float drift_dt, int substeps,
@@ -38,20 +44,39 @@ __device__ __forceinline__ uint32_t drift_one(int id, float4* __restrict__ bodie
     if (id >= n) return 0u;
     float4 b = bodies[id];
     const float2 a = accel[id];
-    for (int s = 0; s < substeps; ++s) {
-        // Substeps after the first carry kickDt = 0 (GravityPipeline.kt:465-473),
-        // whose kick adds a * 0.
-        const float hk = s == 0 ? half_kick : 0.0f;
-        b.z = __fadd_rn(b.z, __fmul_rn(a.x, hk));
-        b.w = __fadd_rn(b.w, __fmul_rn(a.y, hk));
-        b.x = __fadd_rn(b.x, __fmul_rn(b.z, drift_dt));
-        b.y = __fadd_rn(b.y, __fmul_rn(b.w, drift_dt));
+    if (substeps > 0) {
+        b.z = __fadd_rn(b.z, __fmul_rn(a.x, half_kick));
+        b.w = __fadd_rn(b.w, __fmul_rn(a.y, half_kick));
+        float dx = __fmul_rn(b.z, drift_dt), dy = __fmul_rn(b.w, drift_dt);
         if (bounded) {
-            b.x = fminf(fmaxf(b.x, 0.0f), kMaximumUnit);
-            b.y = fminf(fmaxf(b.y, 0.0f), kMaximumUnit);
+            b.x = fminf(fmaxf(__fadd_rn(b.x, dx), 0.0f), kMaximumUnit);
+            b.y = fminf(fmaxf(__fadd_rn(b.y, dy), 0.0f), kMaximumUnit);
         } else {
-            b.x = fractf(b.x);
-            b.y = fractf(b.y);
+            b.x = fract_any(__fadd_rn(b.x, dx));
+            b.y = fract_any(__fadd_rn(b.y, dy));
+        }
+        if (substeps > 1) {
+            b.z = __fadd_rn(b.z, __fmul_rn(a.x, 0.0f));
+            b.w = __fadd_rn(b.w, __fmul_rn(a.y, 0.0f));
+            dx = __fmul_rn(b.z, drift_dt);
+            dy = __fmul_rn(b.w, drift_dt);
+            if (bounded) {
+                for (int s = 1; s < substeps; ++s) {
+                    b.x = fminf(fmaxf(__fadd_rn(b.x, dx), 0.0f), kMaximumUnit);
+                    b.y = fminf(fmaxf(__fadd_rn(b.y, dy), 0.0f), kMaximumUnit);
+                }
+            } else if (b.x >= 0.0f && b.x <= 1.0f && fabsf(dx) < 0.5f && b.y >= 0.0f &&
+                       b.y <= 1.0f && fabsf(dy) < 0.5f) {
+                for (int s = 1; s < substeps; ++s) {
+                    b.x = fract_any(__fadd_rn(b.x, dx));
+                    b.y = fract_near(__fadd_rn(b.y, dy));
+                }
+            } else {
+                for (int s = 1; s < substeps; ++s) {
+                    b.x = fract_any(__fadd_rn(b.x, dx));
+                    b.y = fract_any(__fadd_rn(b.y, dy));
+                }
+            }
         }
     }
     bodies[id] = b;

@@ -213,6 +213,18 @@ class GravityPipeline:
     def step(self, active_bodies: int, steps: int = 1) -> None:
         self._check(self._lib.p3m_step(self._ctx, active_bodies, steps))
 
+    def set_launch_shape(self, fft_lines: int = 0, short_range_threads: int = 256) -> None:
+        """FFT lines per CTA (0: automatic) and short-range block size; the
+        results do not depend on them."""
+        self._check(self._lib.p3m_set_launch_shape(self._ctx, fft_lines, short_range_threads))
+
+    def autotune(self, active_bodies: int, trial_steps: int = 3) -> tuple[int, int]:
+        """Times steps under each launch shape, keeps the fastest and puts the
+        state back; returns (fft_lines, short_range_threads)."""
+        out = (ctypes.c_int32 * 2)()
+        self._check(self._lib.p3m_autotune(self._ctx, active_bodies, trial_steps, out))
+        return int(out[0]), int(out[1])
+
     def build_force(self, active_bodies: int) -> None:
         self._check(self._lib.p3m_build_force(self._ctx, active_bodies))
 

@@ -169,6 +169,19 @@ int p3m_initialize_acceleration(p3m_ctx* ctx, int32_t n);
  * applyKick. Collisions, liquid and sleep are not part of this path. */
 int p3m_step(p3m_ctx* ctx, int32_t n, int32_t steps);
 
+/* Launch shapes (results do not depend on them): FFT lines per CTA of the
+ * row, column and inverse kernels (0: automatic, else 1..16, clamped to what
+ * shared memory holds) and the short-range block (64, 128 or 256 threads).
+ * Drops the captured step graphs. */
+int p3m_set_launch_shape(p3m_ctx* ctx, int32_t fft_lines, int32_t short_range_threads);
+/* Autotuner of one context: times `trial_steps` steps of its n active bodies
+ * (after one untimed step) under each FFT line count (automatic, 1, 2, 4,
+ * 8), then each short-range block with the best count, keeps the fastest
+ * and puts the bodies, materials, accelerations and step counter back.
+ * Writes (fft_lines, short_range_threads) to chosen2 when it is not NULL.
+ * The reference has no counterpart (its dispatch sizes are fixed). */
+int p3m_autotune(p3m_ctx* ctx, int32_t n, int32_t trial_steps, int32_t* chosen2);
+
 /* Separately callable stages, for parity tests and for a host that keeps its
  * own loop. */
 int p3m_sort_bodies(p3m_ctx* ctx, int32_t n);                   /* sortBodies, :1269-1319 */
