@@ -13,7 +13,11 @@ deposit, FP32 FFT and forces. Beside it (`plain_form`): 400,000 bodies in two
 projected Plummer spheres inside walls, physical grid 512x256 (Hockney FFT
 mesh 1024x512), the reference's uint32 deposit. L2 is flushed (a 256 MiB
 write) before every timed step, outside the step's events (the 400k state
-fits in the 126 MB L2; the 8M state does not).
+fits in the 126 MB L2; the 8M state does not). Without flags, W = 5 warm-up
+and K = 45 timed steps: the 50 steps of the precision-form configuration
+(the lattice clusters as it evolves, so longer runs time other states).
+Before timing, the library's autotuner (p3m_autotune) picks the launch
+shapes and puts the state back; the line reports its choice.
 
 Printed (rank 0, one JSON line):
   value     bodies*steps/s from CUDA events around each step, state resident
@@ -458,9 +462,11 @@ def workload_config(sc, args, name=None):
 
 
 def measure_steps(pipe, sc, args, stream, flush, dist, local, steps, warmup, sample_clocks):
-    """Device-timed steps (graphs replayed, state resident in HBM, L2 flushed
-    before each step), then the same steps with stage events, then the e2e
-    pass through the public API with page-locked host buffers."""
+    """The autotuner picks the launch shapes (the state is put back), then
+    device-timed steps (graphs replayed, state resident in HBM, L2 flushed
+    before each step), then the same steps again from the initial state with
+    stage events, then the e2e pass through the public API with page-locked
+    host buffers."""
     import torch
 
     from gravity_b200.pipeline import PinnedArray, kernel_launches
@@ -469,6 +475,7 @@ def measure_steps(pipe, sc, args, stream, flush, dist, local, steps, warmup, sam
     n = sc.n
     pipe.upload(sc.bodies, sc.materials)
     pipe.initialize_acceleration(n)
+    tuned = pipe.autotune(n, 3)
     for _ in range(warmup):
         pipe.step(n)
     pipe.synchronize()
@@ -497,8 +504,14 @@ def measure_steps(pipe, sc, args, stream, flush, dist, local, steps, warmup, sam
         dist.barrier()
     value = ws * n * steps / (total_ms / 1000.0)
 
-    # ---- per-stage device time: the same steps with stage events recorded
-    # (kernels launched one by one; the value pass above replays graphs).
+    # ---- per-stage device time: the same steps from the same initial state
+    # (the bodies cluster as they evolve, which changes the stages' work),
+    # with stage events recorded (kernels launched one by one; the value pass
+    # above replays graphs).
+    pipe.upload(sc.bodies, sc.materials)
+    pipe.initialize_acceleration(n)
+    for _ in range(warmup):
+        pipe.step(n)
     pipe.profile_enable(True)
     with torch.cuda.stream(stream):
         for i in range(steps):
@@ -542,6 +555,7 @@ def measure_steps(pipe, sc, args, stream, flush, dist, local, steps, warmup, sam
         raise SystemExit(f"{timeouts} look-back wait(s) of the sort gave up: results invalid")
     return {"value": value, "ms_per_step": total_ms / steps, "stages": stages,
             "launches": launches, "clocks": clk,
+            "autotuned": {"fft_lines_per_cta": tuned[0] or "auto", "short_range_threads": tuned[1]},
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 16 * n,
                     "d2h_bytes_per_step": 16 * n, "steps": e2e_steps}}
 
@@ -653,7 +667,7 @@ def run_b200(args, ws, rank, local):
             plain = {"workload": "plummer_walls", "config": workload_config(psc, args, "plummer_walls"),
                      "value": pm["value"], "ms_per_step": pm["ms_per_step"], "steps": psteps,
                      "e2e": pm["e2e"], "force_rms_err_vs_fp64": perr, "stages": prow,
-                     "gpu_launches": pm["launches"]}
+                     "autotuned": pm["autotuned"], "gpu_launches": pm["launches"]}
 
     if rank == 0:
         peak, peak_kind = measured_peaks()
@@ -680,6 +694,7 @@ def run_b200(args, ws, rank, local):
             "config": workload_config(sc, args),
             "force_rms_err_vs_fp64": force_err,
             "force_rms_err_vs_fp64_by_form": errors,
+            "autotuned": m["autotuned"],
             "roofline": {"bound": "hbm", "kernel": dominant, "achieved": achieved, "peak": peak,
                          "unit": "GB/s", "frac": achieved / peak if achieved else None,
                          "traffic": traffic, "peak_source": peak_kind},
@@ -1108,8 +1123,8 @@ def run_adjoint(args, ws, rank, local):
 def main():
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=2000)
-    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=45)
+    ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
     ap.add_argument("--workload", default="lattice_scale",
                     choices=["plummer_walls", "uniform_torus", "lattice_scale", "lattice_scale_u32",
@@ -1122,7 +1137,7 @@ def main():
     ap.add_argument("--bodies", type=int, default=None, help="override the workload's body count")
     ap.add_argument("--grid", default=None, help="override the workload's grid, WxH")
     ap.add_argument("--sims", type=int, default=None, help="batch: number of simulations")
-    ap.add_argument("--batch-form", default="persistent",
+    ap.add_argument("--batch-form", default="per_stage",
                     choices=["persistent", "per_stage", "per_simulation"],
                     help="batch --run-only: one persistent launch per step, one launch per "
                          "stage, or one step per simulation")
