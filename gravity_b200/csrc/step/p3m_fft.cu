@@ -649,11 +649,13 @@ void line_shape(int lines_total, int L, int cap, int* per_cta, int* threads, int
     *threads = t < 64 ? 64 : (t > 256 ? 256 : t);
 }
 
-// Columns per CTA of the column kernels: at most 16 and at most what 128 KB
-// of shared memory holds.
+// Columns per CTA of the column kernels: at most 16 and at most what 64 KB
+// of shared memory holds, so that three CTAs share an SM even for
+// 2048-point columns (the kernels are latency-bound: at 4096x2048 one
+// 128 KB CTA per SM took the spectral pass 0.18 ms, three of 64 KB 0.14).
 void column_shape(int MW, int MH, int lines_factor, int* G, int* threads, int fixed) {
     const int SW = MW / 2 + 1;
-    int cap = (128 * 1024) / (lines_factor * MH * (int)sizeof(float2));
+    int cap = (64 * 1024) / (lines_factor * MH * (int)sizeof(float2));
     if (cap > 16) cap = 16;
     line_shape(SW, MH, cap, G, threads, fixed);
 }
@@ -780,7 +782,7 @@ void fft_batch_shape(const GridShape& g, int* rows_per_cta, int* cols_per_cta, i
         return per < 1 ? 1 : per;
     };
     const int row_cap = g.MW >= 4096 ? 1 : 4096 / g.MW;
-    int col_cap = (128 * 1024) / (4 * g.MH * (int)sizeof(float2));
+    int col_cap = (64 * 1024) / (4 * g.MH * (int)sizeof(float2));
     if (col_cap > 16) col_cap = 16;
     *rows_per_cta = fill(g.MH / 2, g.MW, row_cap);
     // + the staged twiddles of one line
