@@ -119,7 +119,9 @@ def run_only(args) -> None:
 
         scs = make_workload("batch", sims=args.sims)
         with GravityBatch([sc.config for sc in scs]) as b:
-            if args.batch_form == "per_stage":
+            if args.batch_form == "persistent":
+                b.set_persistent(True)
+            elif args.batch_form == "per_stage":
                 b.set_persistent(False)
             elif args.batch_form == "per_simulation":
                 b.set_fused(False)
