@@ -1690,77 +1690,64 @@ int build_fused(p3m_batch* b, const std::vector<char>& sort, p3m_batch::Plan& pl
         fb.raw([=](unsigned char*, cudaStream_t) { return cudaEventRecord(join_ev, side); });
     }
     // 5. Mesh force (the mesh was cleared beside the drift): deposit, FFT with
-    // the Green's multiply, inverse. The FFT stages run one launch per mesh
-    // shape: a launch's dynamic shared memory is its largest simulation's, so
-    // one launch over all shapes would hold every CTA to the largest line
-    // buffers (and their few CTAs per SM).
+    // the Green's multiply, inverse.
     {
-        const float2* tw0 = mut.empty() ? nullptr : b->sims[mut[0]]->twiddles;
-        std::map<std::pair<int, int>, std::vector<int>> shapes;  // (MW, MH) -> simulations
-        for (int i : mut) shapes[{b->sims[i]->grid.MW, b->sims[i]->grid.MH}].push_back(i);
         for (int mode : {P3M_DEPOSIT_U32, P3M_DEPOSIT_I64}) {
-            const bool i64 = mode == P3M_DEPOSIT_I64;
             std::vector<p3m::DepositArgs> dep;
             std::vector<int> db;
+            std::vector<p3m::FftRowsArgs> fr;
+            std::vector<int> fblocks;
+            size_t smem = 0;
             for (int i : mut) {
                 p3m_ctx* c = b->sims[i];
                 if (c->cfg.deposit_mode != mode) continue;
                 const p3m::GridShape& g = c->grid;
+                const bool i64 = mode == P3M_DEPOSIT_I64;
                 dep.push_back({c->entries, role[i].sk, c->density, b->n[i], g.W, g.H, g.MW, g.MH,
                                i64 ? 4294967296.0f : (float)c->mass_scale});
                 db.push_back(p3m::chunk_deposit_blocks(b->n[i]));
+                int rp, cp, ip;
+                size_t rs, cs, is;
+                p3m::fft_batch_shape(g, &rp, &cp, &ip, &rs, &cs, &is);
+                fr.push_back({c->density, c->half, i64 ? 1.0f / 4294967296.0f : 1.0f / (float)c->mass_scale,
+                              g.MW, g.MH, rp});
+                fblocks.push_back((g.MH / 2 + rp - 1) / rp);
+                smem = std::max(smem, rs);
             }
+            const bool i64 = mode == P3M_DEPOSIT_I64;
             fb.stage(dep, db, [mode](const p3m::DepositArgs* a, p3m::BatchGrid g, cudaStream_t st) {
                 return p3m::batched_deposit(a, g, mode, st);
             }, i64 ? p3m::kPStageDepositI64 : p3m::kPStageDepositU32, phase_lists + 1,
                      p3m::persistent_base_smem());
-            for (const auto& kv : shapes) {
-                std::vector<p3m::FftRowsArgs> fr;
-                std::vector<int> fblocks;
-                size_t smem = 0;
-                for (int i : kv.second) {
-                    p3m_ctx* c = b->sims[i];
-                    if (c->cfg.deposit_mode != mode) continue;
-                    const p3m::GridShape& g = c->grid;
-                    int rp, cp, ip;
-                    size_t rs, cs, is;
-                    p3m::fft_batch_shape(g, &rp, &cp, &ip, &rs, &cs, &is);
-                    fr.push_back({c->density, c->half,
-                                  i64 ? 1.0f / 4294967296.0f : 1.0f / (float)c->mass_scale,
-                                  g.MW, g.MH, rp});
-                    fblocks.push_back((g.MH / 2 + rp - 1) / rp);
-                    smem = std::max(smem, rs);
-                }
-                fb.stage(fr, fblocks, [mode, smem, tw0](const p3m::FftRowsArgs* a, p3m::BatchGrid g, cudaStream_t st) {
-                    return p3m::batched_fft_rows(a, g, mode, smem, tw0, st);
-                }, i64 ? p3m::kPStageFftRowsI64 : p3m::kPStageFftRowsU32, phase_lists + 2, smem);
-            }
+            const float2* tw0 = mut.empty() ? nullptr : b->sims[mut[0]]->twiddles;
+            fb.stage(fr, fblocks, [mode, smem, tw0](const p3m::FftRowsArgs* a, p3m::BatchGrid g, cudaStream_t st) {
+                return p3m::batched_fft_rows(a, g, mode, smem, tw0, st);
+            }, i64 ? p3m::kPStageFftRowsI64 : p3m::kPStageFftRowsU32, phase_lists + 2, smem);
         }
-        for (const auto& kv : shapes) {
-            std::vector<p3m::FftColumnsArgs> fc;
-            std::vector<p3m::FftInverseArgs> fi;
-            std::vector<int> cbk, ibk;
-            size_t csm = 0, ism = 0;
-            for (int i : kv.second) {
-                p3m_ctx* c = b->sims[i];
-                const p3m::GridShape& g = c->grid;
-                int rp, cp, ip;
-                size_t rs, cs, is;
-                p3m::fft_batch_shape(g, &rp, &cp, &ip, &rs, &cs, &is);
-                fc.push_back({c->half, c->green, c->cols, 1.0f / c->normalization_mass, g.MW, g.MH, cp});
-                cbk.push_back((g.MW / 2 + 1 + cp - 1) / cp);
-                fi.push_back({c->cols, c->force, g.MW, g.MH, ip});
-                ibk.push_back((g.MH + ip - 1) / ip);
-                csm = std::max(csm, cs);
-                ism = std::max(ism, is);
-            }
-            fb.stage(fc, cbk, [csm, tw0](const p3m::FftColumnsArgs* a, p3m::BatchGrid g, cudaStream_t st) {
-                return p3m::batched_fft_columns(a, g, csm, tw0, st);
-            }, p3m::kPStageFftColumns, phase_lists + 3, csm);
-            fb.stage(fi, ibk, [ism, tw0](const p3m::FftInverseArgs* a, p3m::BatchGrid g, cudaStream_t st) {
-                return p3m::batched_fft_inverse(a, g, ism, tw0, st);
-            }, p3m::kPStageFftInverse, phase_lists + 4, ism);
+        std::vector<p3m::FftColumnsArgs> fc;
+        std::vector<p3m::FftInverseArgs> fi;
+        std::vector<int> cbk, ibk;
+        size_t csm = 0, ism = 0;
+        for (int i : mut) {
+            p3m_ctx* c = b->sims[i];
+            const p3m::GridShape& g = c->grid;
+            int rp, cp, ip;
+            size_t rs, cs, is;
+            p3m::fft_batch_shape(g, &rp, &cp, &ip, &rs, &cs, &is);
+            fc.push_back({c->half, c->green, c->cols, 1.0f / c->normalization_mass, g.MW, g.MH, cp});
+            cbk.push_back((g.MW / 2 + 1 + cp - 1) / cp);
+            fi.push_back({c->cols, c->force, g.MW, g.MH, ip});
+            ibk.push_back((g.MH + ip - 1) / ip);
+            csm = std::max(csm, cs);
+            ism = std::max(ism, is);
         }
+        const float2* tw0 = mut.empty() ? nullptr : b->sims[mut[0]]->twiddles;
+        fb.stage(fc, cbk, [csm, tw0](const p3m::FftColumnsArgs* a, p3m::BatchGrid g, cudaStream_t st) {
+            return p3m::batched_fft_columns(a, g, csm, tw0, st);
+        }, p3m::kPStageFftColumns, phase_lists + 3, csm);
+        fb.stage(fi, ibk, [ism, tw0](const p3m::FftInverseArgs* a, p3m::BatchGrid g, cudaStream_t st) {
+            return p3m::batched_fft_inverse(a, g, ism, tw0, st);
+        }, p3m::kPStageFftInverse, phase_lists + 4, ism);
     }
     // 6. Interpolation + kick, after the short range has joined.
     {
