@@ -605,30 +605,55 @@ __device__ __forceinline__ void fill_ranges(int* cell_start, uint32_t f0, uint32
     }
 }
 
-__device__ __forceinline__ void cell_build_body(int block, const uint32_t* __restrict__ keys,
-                                                const uint32_t* __restrict__ ids, int n,
-                                                const float4* __restrict__ bodies,
-                                                const float4* __restrict__ materials,
-                                                int* cell_start, int* cell_count,
-                                                uint32_t* cell_mass, float4* entries,
-                                                int fill_cells) {
-    const int i = block * blockDim.x + threadIdx.x;
-    const int lane = threadIdx.x & 31;
-    const bool valid = i < n;
-    const uint32_t c = valid ? keys[i] : 0xffffffffu;
-    uint32_t prev = __shfl_up_sync(kFull, c, 1);
-    if (lane == 0) prev = (valid && i > 0) ? keys[i - 1] : 0xfffffffeu;
-    uint32_t next = __shfl_down_sync(kFull, c, 1);
-    if (lane == 31) next = (i + 1 < n) ? keys[i + 1] : 0xfffffffeu;
+// One sorted entry of the cell build: its cell key and the keys either side
+// (equal keys are contiguous lanes), its body's ID, position and mass.
+struct BuildItem {
+    int i;
+    bool valid;
+    uint32_t c, prev, next, id;
+    float4 b;
+    float m;
+};
 
+// The entry's key, its neighbours' keys (shuffles, and one load at each end
+// of the warp) and its ID: entry i of a warp-contiguous run of 32.
+__device__ __forceinline__ void build_load_keys(BuildItem& it, int i, const uint32_t* __restrict__ keys,
+                                                const uint32_t* __restrict__ ids, int n) {
+    const int lane = threadIdx.x & 31;
+    it.i = i;
+    it.valid = i < n;
+    it.c = it.valid ? keys[i] : 0xffffffffu;
+    it.prev = __shfl_up_sync(kFull, it.c, 1);
+    if (lane == 0) it.prev = (it.valid && i > 0) ? keys[i - 1] : 0xfffffffeu;
+    it.next = __shfl_down_sync(kFull, it.c, 1);
+    if (lane == 31) it.next = (i + 1 < n) ? keys[i + 1] : 0xfffffffeu;
+    it.id = it.valid ? ids[i] : 0u;
+}
+
+// The body's position and mass (the ID-ordered gathers).
+__device__ __forceinline__ void build_gather(BuildItem& it, const float4* __restrict__ bodies,
+                                             const float4* __restrict__ materials) {
+    if (it.valid) {
+        it.b = bodies[it.id];
+        it.m = materials[it.id].x;
+    }
+}
+
+// The entry, the run's count and mass (segmented sum across the warp, one
+// atomic per run and warp), the run's start, and (fill_cells > 0) the starts
+// of the empty cells.
+__device__ __forceinline__ void build_finish(const BuildItem& it, int n, int* cell_start,
+                                             int* cell_count, uint32_t* cell_mass, float4* entries,
+                                             int fill_cells) {
+    const int lane = threadIdx.x & 31;
+    const int i = it.i;
+    const uint32_t c = it.c, prev = it.prev, next = it.next;
+    const bool valid = it.valid;
     uint32_t cnt = 0, mq = 0;
     if (valid) {
-        const uint32_t id = ids[i];
-        const float4 b = bodies[id];
-        const float m = materials[id].x;
-        entries[i] = make_float4(b.x, b.y, m, __uint_as_float(id));
+        entries[i] = make_float4(it.b.x, it.b.y, it.m, __uint_as_float(it.id));
         cnt = 1;
-        mq = (uint32_t)__float2uint_rn(__fmul_rn(m, kCellMassUnits));
+        mq = (uint32_t)__float2uint_rn(__fmul_rn(it.m, kCellMassUnits));
         if (i == 0 || prev != c) cell_start[c] = i;
     }
     // Segmented inclusive sum over equal keys (keys are sorted, so equal keys
@@ -660,6 +685,26 @@ __device__ __forceinline__ void cell_build_body(int block, const uint32_t* __res
     }
 }
 
+// One entry per thread: block b covers entries [256 b, 256 b + 256) (the
+// batched and persistent forms' block).
+__device__ __forceinline__ void cell_build_body(int block, const uint32_t* __restrict__ keys,
+                                                const uint32_t* __restrict__ ids, int n,
+                                                const float4* __restrict__ bodies,
+                                                const float4* __restrict__ materials,
+                                                int* cell_start, int* cell_count,
+                                                uint32_t* cell_mass, float4* entries,
+                                                int fill_cells) {
+    BuildItem it;
+    build_load_keys(it, block * blockDim.x + threadIdx.x, keys, ids, n);
+    build_gather(it, bodies, materials);
+    build_finish(it, n, cell_start, cell_count, cell_mass, entries, fill_cells);
+}
+
+// Entries per thread of the single-context cell build: each warp takes
+// kBuildItems runs of 32 consecutive entries and issues all their gathers
+// before it uses the first, so twice the gathers are in flight.
+constexpr int kBuildItems = 2;
+
 __global__ void cell_build_kernel(const uint32_t* __restrict__ keys, const uint32_t* __restrict__ ids,
                                   int n, const float4* __restrict__ bodies,
                                   const float4* __restrict__ materials, int* cell_start,
@@ -669,8 +714,16 @@ __global__ void cell_build_kernel(const uint32_t* __restrict__ keys, const uint3
     // A sort whose look-back gave up leaves keys and IDs that are not a
     // permutation: build nothing (every cell stays empty).
     if (sort_failed != nullptr && *sort_failed != 0u) return;
-    cell_build_body(blockIdx.x, keys, ids, n, bodies, materials, cell_start, cell_count, cell_mass,
-                    entries, fill_cells);
+    const int warp_base = (blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5)) * (32 * kBuildItems);
+    BuildItem it[kBuildItems];
+#pragma unroll
+    for (int j = 0; j < kBuildItems; ++j)
+        build_load_keys(it[j], warp_base + 32 * j + (threadIdx.x & 31), keys, ids, n);
+#pragma unroll
+    for (int j = 0; j < kBuildItems; ++j) build_gather(it[j], bodies, materials);
+#pragma unroll
+    for (int j = 0; j < kBuildItems; ++j)
+        build_finish(it[j], n, cell_start, cell_count, cell_mass, entries, fill_cells);
 }
 
 // ------------------------------------------------------- batched launches
@@ -942,7 +995,7 @@ cudaError_t launch_cell_build(const uint32_t* keys, const uint32_t* ids, int n, 
             return cudaMemsetAsync(cell_start, 0, ((size_t)fill_cells + 1) * sizeof(int), stream);
         return cudaSuccess;
     }
-    launch_chained(cell_build_kernel, blocks_for(n, 256), 256, 0, stream, keys, ids, n, bodies, materials,
+    launch_chained(cell_build_kernel, blocks_for(n, 256 * kBuildItems), 256, 0, stream, keys, ids, n, bodies, materials,
                                                               cell_start, cell_count, cell_mass,
                                                               entries, fill_cells, sort_failed);
     count_launches(1);
