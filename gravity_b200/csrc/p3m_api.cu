@@ -384,7 +384,8 @@ p3m::KickParams kick_params(const p3m_ctx* ctx, int n, int initial) {
 int short_range(p3m_ctx* ctx, const p3m::KickParams& p, cudaStream_t stream) {
     if (p.slot_form && p.n > 0)
         P3M_CUDA(ctx, p3m::launch_cell_slots(ctx->cell_start, ctx->cell_count, ctx->cell_mass,
-                                             ctx->entries, p, ctx->cell_slots, stream));
+                                             ctx->entries, ctx->grid.W, ctx->grid.H,
+                                             p.gravity, p.total_mass, ctx->cell_slots, stream));
     P3M_CUDA(ctx, p3m::launch_short_range(ctx->bodies, ctx->entries, ctx->cell_start,
                                           ctx->cell_count, ctx->cell_mass, ctx->cell_slots,
                                           ctx->a_short, p, stream));
@@ -1654,7 +1655,7 @@ int build_fused(p3m_batch* b, const std::vector<char>& sort, p3m_batch::Plan& pl
                 if (!slot_form(i)) continue;
                 const p3m::KickParams kp = kick_params(c, b->n[i], 0);
                 sl.push_back({c->cell_start, c->cell_count, c->cell_mass, c->entries,
-                              c->cell_slots, kp});
+                              c->cell_slots, c->grid.W, c->grid.H, kp.gravity, kp.total_mass});
                 slb.push_back((int)((phys_cells(c) + p3m::kBatchThreads - 1) / p3m::kBatchThreads));
             }
             if (!sl.empty())

@@ -243,28 +243,6 @@ struct KickParams {
     int slot_form;
     float aspect, gravity, sigma_cells, total_mass, min_frac, dt, field_x, field_y;
 };
-// The two-slot short range's scaled coordinates: x' = x aspect s, y' = y s
-// with s^2 = log2(e) / (2 sigma^2) (sigma in unit coordinates of the grid
-// height), so that the Gaussian's exponent is -r'^2; gm = (G / M_tot) s^2 is
-// the factor of a source's mass in the slot table. The cell-slots and the
-// short-range kernels both take it from here.
-struct SlotScale {
-    float sx, sy;   // aspect s, s
-    float s2;       // s^2
-    float gm;       // (G / M_tot) s^2
-};
-
-__device__ __forceinline__ SlotScale slot_scale(const KickParams& p) {
-    const float sigma = p.sigma_cells / (float)p.H;
-    SlotScale q;
-    q.s2 = 1.4426950408889634f / (2.0f * sigma * sigma);
-    const float s = sqrtf(q.s2);
-    q.sx = p.aspect * s;
-    q.sy = s;
-    q.gm = (p.gravity / p.total_mass) * q.s2;
-    return q;
-}
-
 // Short-range correction over the cell stencil (kick.comp:122-151), one
 // thread per body; writes a_short[id]. Radii 1..6.
 cudaError_t launch_short_range(const float4* bodies, const float4* entries, const int* cell_start,
@@ -273,12 +251,12 @@ cudaError_t launch_short_range(const float4* bodies, const float4* entries, cons
                                cudaStream_t stream);
 // The two source slots of every cell for the two-slot short range (exact
 // limit 2): the monopole at the cell centre (count > 2), the first one or
-// two list entries, or empty slots (mass 0) at the centre. Two planes of
-// p.W*p.H cells in the scaled coordinates of slot_scale(p): float4
-// (x0', x1', y0', y1'), then float2 (gm m0, gm m1).
+// two list entries, or empty slots (mass 0) at the centre. Two planes of W*H
+// cells: float4 (x0, x1, y0, y1), then float2 (G m0 / M_tot, G m1 / M_tot).
 cudaError_t launch_cell_slots(const int* cell_start, const int* cell_count,
-                              const uint32_t* cell_mass, const float4* entries,
-                              const KickParams& p, float4* slots, cudaStream_t stream);
+                              const uint32_t* cell_mass, const float4* entries, int W, int H,
+                              float gravity, float total_mass, float4* slots,
+                              cudaStream_t stream);
 // CIC interpolation + field + a_short, then the half kick (kick.comp:82-103,
 // :153-154), one thread per body in ID order.
 cudaError_t launch_interp_kick(float4* bodies, float2* accel, const float2* force,
@@ -429,7 +407,7 @@ struct ShortRangeArgs {
 };
 struct SlotsArgs {
     const int* cell_start; const int* cell_count; const uint32_t* cell_mass; const float4* entries;
-    float4* slots; KickParams p;
+    float4* slots; int W, H; float gravity, total_mass;
 };
 struct KickArgs {
     float4* bodies; float2* accel; const float2* force; const float2* a_short; KickParams p;

@@ -113,27 +113,6 @@ __device__ __forceinline__ void pair_add2_gm(const PairConst& k, float2 dx, floa
     ay = __ffma2_rn(phys, dy, ay);
 }
 
-// The two-slot form works in scaled coordinates, in which the Gaussian's
-// exponent is the squared distance itself: x' = x aspect s, y' = y s with
-// s^2 = log2(e) / (2 sigma^2), so r'^2 = r^2 s^2 and exp(-r^2/2s^2) =
-// exp2(-r'^2). Then G m exp(-r^2/2s^2) d / (M max(r^2, r_min^2)) =
-// (G/M) s^2 m exp2(-r'^2) d' / max(r'^2, r_min^2 s^2) with d = (d'x / (aspect s),
-// d'y / s): the slot table holds x', y' and (G/M) s^2 m, and the target
-// divides its sums by (aspect s, s) once. That takes the aspect and exponent
-// multiplies out of every pair.
-// The pair term of two sources in scaled coordinates (px, py: source minus
-// target; gm: the sources' (G/M) s^2 m), accumulated per packed half into
-// (ax, ay) (scaled sums: divided by (aspect s, s) at the end).
-__device__ __forceinline__ void pair_add2_scaled(float min_r2, float2 px, float2 py, float2 gm,
-                                                 float2& ax, float2& ay) {
-    const float2 r2 = __ffma2_rn(px, px, __fmul2_rn(py, py));
-    const float2 num = __fmul2_rn(gm, make_float2(fast_exp2(-r2.x), fast_exp2(-r2.y)));
-    const float2 inv = make_float2(fast_rcp(fmaxf(r2.x, min_r2)), fast_rcp(fmaxf(r2.y, min_r2)));
-    const float2 phys = __fmul2_rn(num, inv);
-    ax = __ffma2_rn(phys, px, ax);
-    ay = __ffma2_rn(phys, py, ay);
-}
-
 // Cells of the slot table a CTA stages in shared memory (24 bytes each): the
 // box spanned by its bodies' stencils, when it holds at most this many.
 constexpr int kStageCells = 1536;
@@ -232,14 +211,9 @@ __device__ __forceinline__ void stencil_sum(
     const float4* __restrict__ slots, const float2* __restrict__ slots_b, const float4* st_a,
     const float2* st_b, int sbase, int bw, float2& acc_x, float2& acc_y) {
     const float inv_w = 1.0f / (float)p.W, inv_h = 1.0f / (float)p.H;
-    // The two-slot form's scaled coordinates (SlotScale); its target.
-    const SlotScale q = slot_scale(p);
-    const float min_r2s = k.min_dist2 * q.s2;
-    const float tsx = t.x * q.sx, tsy = t.y * q.sy;
     // Per stencil column: wrapped column, periodic image shift, validity.
     // off_x: the image shift less the target's x, so that a source at x on
-    // that column is at dx = x + off_x (exactly x - t.x where no wrap); in
-    // the two-slot form, in scaled coordinates.
+    // that column is at dx = x + off_x (exactly x - t.x where no wrap).
     int col[2 * RX + 1];
     float shift_x[2 * RX + 1];
     float off_x[2 * RX + 1];
@@ -250,7 +224,7 @@ __device__ __forceinline__ void stencil_sum(
         const int wx = wrap_index(cx, p.W);
         col[a] = wx;
         shift_x[a] = (float)(cx - wx) * inv_w;
-        off_x[a] = EXACT == 2 ? shift_x[a] * q.sx - tsx : shift_x[a] - t.x;
+        off_x[a] = shift_x[a] - t.x;
         ok_x[a] = !p.bounded || (cx >= 0 && cx < p.W);
     }
     const float2 neg_t = make_float2(-t.x, -t.y);
@@ -263,17 +237,16 @@ __device__ __forceinline__ void stencil_sum(
         const int row = wy * p.W;
         const float shift_y = (float)(cy - wy) * inv_h;
         const float cyr = ((float)wy + 0.5f) * inv_h;  // wrapped row centre
-        const float off_y = EXACT == 2 ? shift_y * q.sy - tsy : shift_y - t.y;
+        const float off_y = shift_y - t.y;
 #pragma unroll
         for (int a = 0; a < 2 * RX + 1; ++a) {
             if (!ok_x[a]) continue;
             const int index = row + col[a];
             const bool home = (a == RX) && (b == RY);
             if (EXACT == 2 && !home) {
-                // The cell's two slots, prepared once per step (cell_slots),
-                // in scaled coordinates: (x0, x1, y0, y1) and the two masses'
-                // (G/M) s^2 m, so each packed operand is one loaded register
-                // pair.
+                // The cell's two slots, prepared once per step (cell_slots):
+                // (x0, x1, y0, y1) and (G m0 / M_tot, G m1 / M_tot), so each
+                // packed operand is one loaded register pair.
                 float4 s0;
                 float2 s1;
                 if (STAGED) {
@@ -286,8 +259,8 @@ __device__ __forceinline__ void stencil_sum(
                 }
                 const float2 ox = make_float2(off_x[a], off_x[a]);
                 const float2 oy = make_float2(off_y, off_y);
-                pair_add2_scaled(min_r2s, __fadd2_rn(make_float2(s0.x, s0.y), ox),
-                                 __fadd2_rn(make_float2(s0.z, s0.w), oy), s1, ax2, ay2);
+                pair_add2_gm(k, __fadd2_rn(make_float2(s0.x, s0.y), ox),
+                             __fadd2_rn(make_float2(s0.z, s0.w), oy), s1, ax2, ay2);
                 continue;
             }
             const int count = __ldg(&cell_count[index]);
@@ -318,24 +291,13 @@ __device__ __forceinline__ void stencil_sum(
                                                  make_float2(neg_t.x, neg_t.x));
                     const float2 dy = __fadd2_rn(__fadd2_rn(make_float2(o0.y, o1.y), sy),
                                                  make_float2(neg_t.y, neg_t.y));
-                    if (EXACT == 2)  // the home cell of the two-slot form: scaled
-                        pair_add2_scaled(min_r2s, __fmul2_rn(dx, make_float2(q.sx, q.sx)),
-                                         __fmul2_rn(dy, make_float2(q.sy, q.sy)),
-                                         __fmul2_rn(make_float2(q.gm, q.gm), make_float2(m0, m1)),
-                                         ax2, ay2);
-                    else
-                        pair_add2_gm(k, dx, dy,
-                                     __fmul2_rn(make_float2(k.g_over_m, k.g_over_m),
-                                                make_float2(m0, m1)),
-                                     ax2, ay2);
+                    pair_add2_gm(k, dx, dy,
+                                 __fmul2_rn(make_float2(k.g_over_m, k.g_over_m),
+                                            make_float2(m0, m1)),
+                                 ax2, ay2);
                 }
             }
         }
-    }
-    if (EXACT == 2) {  // back from scaled coordinates
-        const float ix = 1.0f / q.sx, iy = 1.0f / q.sy;
-        ax2 = __fmul2_rn(ax2, make_float2(ix, ix));
-        ay2 = __fmul2_rn(ay2, make_float2(iy, iy));
     }
     acc_x = ax2;
     acc_y = ay2;

@@ -124,7 +124,8 @@ P3M_STAGE(stage_cell_build) {
 }
 P3M_STAGE(stage_slots) {
     const SlotsArgs a = reinterpret_cast<const SlotsArgs*>(args)[sb.x];
-    C::cell_slots_body(sb.y, a.cell_start, a.cell_count, a.cell_mass, a.entries, a.p, a.slots);
+    C::cell_slots_body(sb.y, a.cell_start, a.cell_count, a.cell_mass, a.entries, a.W, a.H,
+                       a.gravity, a.total_mass, a.slots);
 }
 P3M_STAGE(stage_short_range_slots) {
     const ShortRangeArgs a = reinterpret_cast<const ShortRangeArgs*>(args)[sb.x];

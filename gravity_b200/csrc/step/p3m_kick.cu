@@ -65,15 +65,13 @@ __global__ void __launch_bounds__(256) interp_kick_kernel(
 // than two bodies is its monopole at the cell centre; one of up to two bodies
 // gives its entries; missing slots are massless at the centre, so they add
 // nothing. The short range then reads 24 bytes per cell instead of the
-// count -> start -> entries chain. A slot holds x, y in the scaled
-// coordinates of slot_scale (x aspect s, y s) and (G/M) s^2 m, the product
-// the pair term forms first; the two slots of a cell are stored interleaved,
-// (x0, x1, y0, y1) and (gm m0, gm m1).
+// count -> start -> entries chain. A slot holds x, y and G m / M_tot, the
+// product the pair term forms first; the two slots of a cell are stored
+// interleaved, (x0, x1, y0, y1) and (G m0 / M, G m1 / M).
 __device__ __forceinline__ void cell_slots_body(
     int block, const int* __restrict__ cell_start, const int* __restrict__ cell_count,
-    const uint32_t* __restrict__ cell_mass, const float4* __restrict__ entries,
-    const KickParams& p, float4* __restrict__ slots) {
-    const int W = p.W, H = p.H;
+    const uint32_t* __restrict__ cell_mass, const float4* __restrict__ entries, int W, int H,
+    float gravity, float total_mass, float4* __restrict__ slots) {
     const int index = block * blockDim.x + threadIdx.x;
     if (index >= W * H) return;
     const int row = index / W, col = index - row * W;
@@ -91,26 +89,29 @@ __device__ __forceinline__ void cell_slots_body(
         s0 = entries[start];
         if (count == 2) s1 = entries[start + 1];
     }
-    const SlotScale q = slot_scale(p);
+    const float g_over_m = gravity / total_mass;
     // Two planes: (x0, x1, y0, y1) for every cell, then (gm0, gm1), so that
     // each pair the packed FP32x2 pair term takes is loaded as one pair.
-    slots[index] = make_float4(s0.x * q.sx, s1.x * q.sx, s0.y * q.sy, s1.y * q.sy);
-    reinterpret_cast<float2*>(slots + (size_t)W * H)[index] = make_float2(q.gm * s0.z, q.gm * s1.z);
+    slots[index] = make_float4(s0.x, s1.x, s0.y, s1.y);
+    reinterpret_cast<float2*>(slots + (size_t)W * H)[index] =
+        make_float2(g_over_m * s0.z, g_over_m * s1.z);
 }
 
 __global__ void __launch_bounds__(256) cell_slots_kernel(
     const int* __restrict__ cell_start, const int* __restrict__ cell_count,
-    const uint32_t* __restrict__ cell_mass, const float4* __restrict__ entries, KickParams p,
-    float4* __restrict__ slots) {
+    const uint32_t* __restrict__ cell_mass, const float4* __restrict__ entries, int W, int H,
+    float gravity, float total_mass, float4* __restrict__ slots) {
     grid_dependency_wait();
-    cell_slots_body(blockIdx.x, cell_start, cell_count, cell_mass, entries, p, slots);
+    cell_slots_body(blockIdx.x, cell_start, cell_count, cell_mass, entries, W, H, gravity,
+                    total_mass, slots);
 }
 
 __global__ void __launch_bounds__(256) cell_slots_batched_kernel(
     const SlotsArgs* __restrict__ args, const int* __restrict__ first, int sims) {
     const int2 sb = batch_block(first, sims);
     const SlotsArgs a = args[sb.x];
-    cell_slots_body(sb.y, a.cell_start, a.cell_count, a.cell_mass, a.entries, a.p, a.slots);
+    cell_slots_body(sb.y, a.cell_start, a.cell_count, a.cell_mass, a.entries, a.W, a.H,
+                    a.gravity, a.total_mass, a.slots);
 }
 
 __global__ void __launch_bounds__(256) interp_kick_batched_kernel(
@@ -134,12 +135,13 @@ cudaError_t batched_interp_kick(const KickArgs* a, BatchGrid g, cudaStream_t s) 
 }
 
 cudaError_t launch_cell_slots(const int* cell_start, const int* cell_count,
-                              const uint32_t* cell_mass, const float4* entries,
-                              const KickParams& p, float4* slots, cudaStream_t stream) {
-    const int cells = p.W * p.H;
+                              const uint32_t* cell_mass, const float4* entries, int W, int H,
+                              float gravity, float total_mass, float4* slots,
+                              cudaStream_t stream) {
+    const int cells = W * H;
     if (cells <= 0) return cudaSuccess;
     launch_chained(cell_slots_kernel, (cells + 255) / 256, 256, 0, stream,
-        cell_start, cell_count, cell_mass, entries, p, slots);
+        cell_start, cell_count, cell_mass, entries, W, H, gravity, total_mass, slots);
     count_launches(1);
     return cudaGetLastError();
 }
