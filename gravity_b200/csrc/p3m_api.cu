@@ -203,6 +203,20 @@ void adjoint_free(p3m_ctx* ctx);
 
 void free_all(p3m_ctx* ctx) {
     adjoint_free(ctx);
+    for (cudaStream_t s : {ctx->up_stream, ctx->down_stream})
+        if (s) {
+            cudaStreamSynchronize(s);
+            cudaStreamDestroy(s);
+        }
+    ctx->up_stream = ctx->down_stream = nullptr;
+    for (cudaEvent_t* e : {&ctx->in_ready, &ctx->in_free, &ctx->out_ready, &ctx->out_free})
+        if (*e) {
+            cudaEventDestroy(*e);
+            *e = nullptr;
+        }
+    if (ctx->stage_in) cudaFree(ctx->stage_in);
+    if (ctx->stage_out) cudaFree(ctx->stage_out);
+    ctx->stage_in = ctx->stage_out = nullptr;
     if (ctx->side) cudaStreamSynchronize(ctx->side);
     if (ctx->ev_fork) cudaEventDestroy(ctx->ev_fork);
     if (ctx->ev_join) cudaEventDestroy(ctx->ev_join);
@@ -979,7 +993,53 @@ int p3m_synchronize(p3m_ctx* ctx) {
     if (!ctx) return P3M_ERR_INVALID_ARGUMENT;
     P3M_CUDA(ctx, queue_status_read(ctx));
     P3M_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    // p3m_step_io's copies (the last download follows the last step).
+    if (ctx->up_stream) P3M_CUDA(ctx, cudaStreamSynchronize(ctx->up_stream));
+    if (ctx->down_stream) P3M_CUDA(ctx, cudaStreamSynchronize(ctx->down_stream));
     return device_failures(ctx, true);
+}
+
+int p3m_step_io(p3m_ctx* ctx, int32_t n, const float* host_bodies_in4, float* host_bodies_out4) {
+    int st = check_n(ctx, n);
+    if (st != P3M_OK) return st;
+    if (!ctx->up_stream) {  // first call: the copy streams, staging buffers and events
+        const size_t cap = (size_t)ctx->cfg.capacity;
+        P3M_CUDA(ctx, cudaStreamCreateWithFlags(&ctx->up_stream, cudaStreamNonBlocking));
+        P3M_CUDA(ctx, cudaStreamCreateWithFlags(&ctx->down_stream, cudaStreamNonBlocking));
+        for (cudaEvent_t* e : {&ctx->in_ready, &ctx->in_free, &ctx->out_ready, &ctx->out_free})
+            P3M_CUDA(ctx, cudaEventCreateWithFlags(e, cudaEventDisableTiming));
+        if (cudaMalloc((void**)&ctx->stage_in, cap * sizeof(float4)) != cudaSuccess ||
+            cudaMalloc((void**)&ctx->stage_out, cap * sizeof(float4)) != cudaSuccess)
+            return fail(ctx, P3M_ERR_OUT_OF_MEMORY, "staging buffers of p3m_step_io");
+    }
+    const size_t bytes = (size_t)n * sizeof(float4);
+    if (host_bodies_in4 && n > 0) {
+        // The upload waits only until the previous step has taken the last
+        // upload out of the staging buffer, so it overlaps that step.
+        P3M_CUDA(ctx, cudaStreamWaitEvent(ctx->up_stream, ctx->in_free, 0));
+        P3M_CUDA(ctx, cudaMemcpyAsync(ctx->stage_in, host_bodies_in4, bytes, cudaMemcpyHostToDevice,
+                                      ctx->up_stream));
+        P3M_CUDA(ctx, cudaEventRecord(ctx->in_ready, ctx->up_stream));
+        P3M_CUDA(ctx, cudaStreamWaitEvent(ctx->stream, ctx->in_ready, 0));
+        P3M_CUDA(ctx, cudaMemcpyAsync(ctx->bodies, ctx->stage_in, bytes, cudaMemcpyDeviceToDevice,
+                                      ctx->stream));
+        P3M_CUDA(ctx, cudaEventRecord(ctx->in_free, ctx->stream));
+    }
+    st = one_step(ctx, n);
+    if (st != P3M_OK) return st;
+    if (host_bodies_out4 && n > 0) {
+        // The stepped bodies go to the staging buffer once the previous
+        // download has left it; the download then overlaps the next step.
+        P3M_CUDA(ctx, cudaStreamWaitEvent(ctx->stream, ctx->out_free, 0));
+        P3M_CUDA(ctx, cudaMemcpyAsync(ctx->stage_out, ctx->bodies, bytes, cudaMemcpyDeviceToDevice,
+                                      ctx->stream));
+        P3M_CUDA(ctx, cudaEventRecord(ctx->out_ready, ctx->stream));
+        P3M_CUDA(ctx, cudaStreamWaitEvent(ctx->down_stream, ctx->out_ready, 0));
+        P3M_CUDA(ctx, cudaMemcpyAsync(host_bodies_out4, ctx->stage_out, bytes,
+                                      cudaMemcpyDeviceToHost, ctx->down_stream));
+        P3M_CUDA(ctx, cudaEventRecord(ctx->out_free, ctx->down_stream));
+    }
+    return P3M_OK;
 }
 
 int p3m_set_lookback_fault(p3m_ctx* ctx, int32_t poll_limit, int32_t withheld_tile) {

@@ -508,6 +508,13 @@ struct p3m_ctx {
     // beside the deposit and FFT (fork / join events).
     cudaStream_t side = nullptr;
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+    // p3m_step_io: the host copies on their own streams (one per direction,
+    // so upload and download overlap), through device staging buffers; the
+    // events order each staging buffer's reuse. Created at the first call.
+    cudaStream_t up_stream = nullptr, down_stream = nullptr;
+    float4* stage_in = nullptr;
+    float4* stage_out = nullptr;
+    cudaEvent_t in_ready = nullptr, in_free = nullptr, out_ready = nullptr, out_free = nullptr;
     p3m::GridShape grid{};
     bool walls_supported = false;
     float aspect = 1.0f;

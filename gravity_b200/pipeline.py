@@ -213,6 +213,17 @@ class GravityPipeline:
     def step(self, active_bodies: int, steps: int = 1) -> None:
         self._check(self._lib.p3m_step(self._ctx, active_bodies, steps))
 
+    def step_io(self, n: int, bodies_in: np.ndarray | None = None,
+                bodies_out: np.ndarray | None = None) -> None:
+        """One step with its host copies pipelined (p3m_step_io): bodies_in
+        becomes the first n bodies before the step, the stepped bodies go to
+        bodies_out. Asynchronous: keep both arrays (page-locked for overlap)
+        alive and bodies_in unchanged until synchronize()."""
+        for a, what in ((bodies_in, "input"), (bodies_out, "output")):
+            if a is not None and (a.dtype != np.float32 or a.size < n * 4 or not a.flags.c_contiguous):
+                raise ValueError(f"{what} array must be contiguous float32 with n rows of 4")
+        self._check(self._lib.p3m_step_io(self._ctx, n, _ptr(bodies_in), _ptr(bodies_out)))
+
     def set_launch_shape(self, fft_lines: int = 0, short_range_threads: int = 256) -> None:
         """FFT lines per CTA (0: automatic) and short-range block size; the
         results do not depend on them."""

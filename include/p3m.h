@@ -169,6 +169,21 @@ int p3m_initialize_acceleration(p3m_ctx* ctx, int32_t n);
  * applyKick. Collisions, liquid and sleep are not part of this path. */
 int p3m_step(p3m_ctx* ctx, int32_t n, int32_t steps);
 
+/* step(n) with its host I/O pipelined against the neighbouring steps:
+ * host_bodies_in4 (may be NULL) becomes the first n bodies before the step,
+ * as p3m_upload_state would make it, and the stepped bodies go to
+ * host_bodies_out4 (may be NULL), as p3m_download_state would write them.
+ * The call only enqueues: the copies run on the context's own copy streams
+ * (one per direction) through device staging buffers (2 x 16 B per body of
+ * capacity, allocated at the first call), so the next call's upload overlaps
+ * this step and this step's download overlaps the next step. Both host
+ * arrays should be page-locked (p3m_host_alloc) for the copies to be
+ * asynchronous; they must stay valid, and host_bodies_in4 unchanged, until
+ * p3m_synchronize returns, which waits for every queued copy and reports
+ * device failures like a download. The reference re-uploads and reads back
+ * its SSBOs synchronously (GravityPipeline.kt:720-770, :378-443). */
+int p3m_step_io(p3m_ctx* ctx, int32_t n, const float* host_bodies_in4, float* host_bodies_out4);
+
 /* Launch shapes (results do not depend on them): FFT lines per CTA of the
  * row, column and inverse kernels (0: automatic, else 1..16, clamped to what
  * shared memory holds) and the short-range block (64, 128 or 256 threads).
