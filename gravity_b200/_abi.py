@@ -140,6 +140,7 @@ SIGNATURES = {
     "p3m_batch_set_persistent": (ctypes.c_int, [_vp, _i32, _i32]),
     "p3m_set_launch_shape": (ctypes.c_int, [_vp, _i32, _i32]),
     "p3m_step_io": (ctypes.c_int, [_vp, _i32, _vp, _vp]),
+    "p3m_batch_step_io": (ctypes.c_int, [_vp, _vp, _vp]),
     "p3m_autotune": (ctypes.c_int, [_vp, _i32, _i32, _vp]),
     "p3m_batch_set_barrier_fault": (ctypes.c_int, [_vp, _i32, _i32, _i32]),
     "p3m_batch_plan_info": (ctypes.c_int, [_vp, _vp]),

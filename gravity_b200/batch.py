@@ -78,6 +78,20 @@ class GravityBatch:
         per simulation inside one graph; the results are the same bits."""
         self._check(self._lib.p3m_batch_set_fused(self._b, 1 if enabled else 0))
 
+    def step_io(self, bodies_in: np.ndarray | None = None,
+                bodies_out: np.ndarray | None = None) -> None:
+        """One batch step with its host copies pipelined (p3m_batch_step_io):
+        bodies_in holds every simulation's bodies back to back (simulation
+        order, n rows each) and becomes their bodies before the step; the
+        stepped bodies go to bodies_out in the same layout. Asynchronous: keep
+        both arrays (page-locked for overlap) alive and bodies_in unchanged
+        until synchronize()."""
+        rows = sum(self.n)
+        for a, what in ((bodies_in, "input"), (bodies_out, "output")):
+            if a is not None and (a.dtype != np.float32 or a.size < rows * 4 or not a.flags.c_contiguous):
+                raise ValueError(f"{what} array must be contiguous float32 with sum(n) rows of 4")
+        self._check(self._lib.p3m_batch_step_io(self._b, _ptr(bodies_in), _ptr(bodies_out)))
+
     def set_persistent(self, enabled: bool, ctas_per_sm: int = 0) -> None:
         """One persistent launch per batch step, or one launch per stage (the
         default); ``ctas_per_sm`` 0 keeps as many CTAs per SM as stay

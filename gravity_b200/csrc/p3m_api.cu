@@ -1296,6 +1296,20 @@ struct p3m_batch {
     unsigned int reported_timeouts = 0;
     unsigned long long* phase_ns = nullptr;  // device: the last launch's phase stamps
     int32_t last_info[4] = {0, 0, 0, 0};     // of the last step's plan: see p3m_batch_plan_info
+    // p3m_batch_step_io: one copy stream per direction, device staging of all
+    // simulations' bodies back to back, the events that order the staging
+    // buffers' reuse, and the row-copy arguments between the staging and
+    // each simulation's current body buffer (keyed by counts and buffers).
+    cudaStream_t up_stream = nullptr, down_stream = nullptr;
+    float4* stage_in = nullptr;
+    float4* stage_out = nullptr;
+    cudaEvent_t in_ready = nullptr, in_free = nullptr, out_ready = nullptr, out_free = nullptr;
+    struct IoArgs {
+        std::vector<uint64_t> key;
+        void* dev = nullptr;  // RowCopy[sims], then the block prefix (sims + 1 ints)
+        int blocks = 0;
+    };
+    std::vector<IoArgs> io_args;
     struct Plan {
         std::vector<uint64_t> key;
         void* blob = nullptr;  // per-simulation arguments and block prefixes
@@ -1372,6 +1386,82 @@ int batch_enqueue(p3m_batch* b, const std::vector<char>& sort) {
 
 bool fused_supported(const p3m_batch* b);
 int batch_fused_step(p3m_batch* b, const std::vector<char>& sort, const std::vector<uint64_t>& key);
+
+// Rows of float4 between the I/O staging buffers and the simulations' body
+// buffers, every simulation in one launch (block b: local block b - first[s]
+// of simulation s).
+struct RowCopy {
+    const float4* src;
+    float4* dst;
+    int n;
+};
+
+__global__ void __launch_bounds__(256) batch_rows_copy_kernel(const RowCopy* __restrict__ copies,
+                                                              const int* __restrict__ first,
+                                                              int sims) {
+    const int2 sb = p3m::batch_block(first, sims);
+    const RowCopy c = copies[sb.x];
+    const int k = sb.y * 256 + (int)threadIdx.x;
+    if (k < c.n) c.dst[k] = c.src[k];
+}
+
+// The row copies of the batch's current bodies from (in) or to (out) the
+// staging buffer, simulation i at row sum(n[j], j < i); built once per set
+// of counts and body buffers and kept (the reorder cycles through a few).
+const p3m_batch::IoArgs* batch_io_args(p3m_batch* b, bool in) {
+    const size_t S = b->sims.size();
+    std::vector<uint64_t> key;
+    key.reserve(2 * S + 1);
+    key.push_back(in ? 1u : 0u);
+    for (size_t i = 0; i < S; ++i) {
+        key.push_back((uint64_t)(uintptr_t)b->sims[i]->bodies);
+        key.push_back((uint64_t)b->n[i]);
+    }
+    for (const auto& a : b->io_args)
+        if (a.key == key) return &a;
+    std::vector<RowCopy> copies(S);
+    std::vector<int> first(S + 1, 0);
+    long long row = 0;
+    for (size_t i = 0; i < S; ++i) {
+        float4* cur = b->sims[i]->bodies;
+        copies[i] = in ? RowCopy{b->stage_in + row, cur, b->n[i]}
+                       : RowCopy{cur, b->stage_out + row, b->n[i]};
+        first[i + 1] = first[i] + (b->n[i] + 255) / 256;
+        row += b->n[i];
+    }
+    const size_t cbytes = S * sizeof(RowCopy);
+    const size_t fbytes = (S + 1) * sizeof(int);
+    p3m_batch::IoArgs a;
+    a.key = key;
+    a.blocks = first[S];
+    if (cudaMalloc(&a.dev, cbytes + fbytes) != cudaSuccess) return nullptr;
+    // A new buffer: a blocking copy (the default stream does not wait for
+    // the batch's non-blocking streams).
+    if (cudaMemcpy(a.dev, copies.data(), cbytes, cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpy(static_cast<char*>(a.dev) + cbytes, first.data(), fbytes,
+                   cudaMemcpyHostToDevice) != cudaSuccess) {
+        cudaFree(a.dev);
+        return nullptr;
+    }
+    if (b->io_args.size() >= 16) {  // dropped only after its last use has run
+        cudaStreamSynchronize(b->stream);
+        cudaFree(b->io_args.front().dev);
+        b->io_args.erase(b->io_args.begin());
+    }
+    b->io_args.push_back(std::move(a));
+    return &b->io_args.back();
+}
+
+cudaError_t launch_io_copy(p3m_batch* b, const p3m_batch::IoArgs* a) {
+    if (a->blocks <= 0) return cudaSuccess;
+    const size_t cbytes = b->sims.size() * sizeof(RowCopy);
+    batch_rows_copy_kernel<<<a->blocks, 256, 0, b->stream>>>(
+        static_cast<const RowCopy*>(a->dev),
+        reinterpret_cast<const int*>(static_cast<const char*>(a->dev) + cbytes),
+        (int)b->sims.size());
+    p3m::count_launches(1);
+    return cudaGetLastError();
+}
 
 int batch_one_step(p3m_batch* b) {
     std::vector<char> sort(b->sims.size(), 0);
@@ -2216,6 +2306,16 @@ int p3m_batch_create(const p3m_config* configs, int32_t count, p3m_batch** out) 
 int p3m_batch_destroy(p3m_batch* b) {
     if (!b) return P3M_OK;
     cudaStreamSynchronize(b->stream);
+    for (cudaStream_t s : {b->up_stream, b->down_stream})
+        if (s) {
+            cudaStreamSynchronize(s);
+            cudaStreamDestroy(s);
+        }
+    for (cudaEvent_t e : {b->in_ready, b->in_free, b->out_ready, b->out_free})
+        if (e) cudaEventDestroy(e);
+    for (auto& a : b->io_args) cudaFree(a.dev);
+    if (b->stage_in) cudaFree(b->stage_in);
+    if (b->stage_out) cudaFree(b->stage_out);
     batch_drop_graphs(b);
     for (p3m_ctx* c : b->sims) p3m_destroy(c);
     cudaFree(b->sync);
@@ -2346,6 +2446,9 @@ int p3m_batch_set_fused(p3m_batch* b, int32_t enabled) {
 int p3m_batch_synchronize(p3m_batch* b) {
     if (!b) return P3M_ERR_INVALID_ARGUMENT;
     cudaError_t e = cudaStreamSynchronize(b->stream);
+    // p3m_batch_step_io's copies (the last download follows the last step).
+    if (e == cudaSuccess && b->up_stream) e = cudaStreamSynchronize(b->up_stream);
+    if (e == cudaSuccess && b->down_stream) e = cudaStreamSynchronize(b->down_stream);
     if (e != cudaSuccess) return batch_fail(b, P3M_ERR_CUDA, cudaGetErrorString(e));
     unsigned int gave_up = 0;  // grid-barrier waits that ran out, over all launches
     e = cudaMemcpy(&gave_up, b->sync + 1, sizeof(gave_up), cudaMemcpyDeviceToHost);
@@ -2356,6 +2459,58 @@ int p3m_batch_synchronize(p3m_batch* b) {
                           "a grid barrier of the persistent batch step gave up waiting (" +
                               std::to_string(gave_up) + " waits so far); the simulations' "
                               "state is incomplete and must be uploaded again");
+    }
+    return P3M_OK;
+}
+
+int p3m_batch_step_io(p3m_batch* b, const float* host_bodies_in4, float* host_bodies_out4) {
+    if (!b) return P3M_ERR_INVALID_ARGUMENT;
+    cudaError_t e = cudaSuccess;
+    if (!b->up_stream) {  // first call: copy streams, staging, events
+        size_t cap = 0;
+        for (p3m_ctx* c : b->sims) cap += (size_t)c->cfg.capacity;
+        e = cudaStreamCreateWithFlags(&b->up_stream, cudaStreamNonBlocking);
+        if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&b->down_stream, cudaStreamNonBlocking);
+        for (cudaEvent_t* ev : {&b->in_ready, &b->in_free, &b->out_ready, &b->out_free})
+            if (e == cudaSuccess) e = cudaEventCreateWithFlags(ev, cudaEventDisableTiming);
+        if (e != cudaSuccess) return batch_fail(b, P3M_ERR_CUDA, cudaGetErrorString(e));
+        if (cudaMalloc((void**)&b->stage_in, std::max<size_t>(cap, 1) * sizeof(float4)) != cudaSuccess ||
+            cudaMalloc((void**)&b->stage_out, std::max<size_t>(cap, 1) * sizeof(float4)) != cudaSuccess)
+            return batch_fail(b, P3M_ERR_OUT_OF_MEMORY, "staging buffers of p3m_batch_step_io");
+    }
+    long long rows = 0;
+    for (int v : b->n) rows += v;
+    const size_t bytes = (size_t)rows * sizeof(float4);
+    if (host_bodies_in4 && rows > 0) {
+        const p3m_batch::IoArgs* a = batch_io_args(b, true);
+        if (!a) return batch_fail(b, P3M_ERR_OUT_OF_MEMORY, "row-copy arguments");
+        // The upload waits only until the previous step has taken the last
+        // upload out of the staging buffer, so it overlaps that step.
+        e = cudaStreamWaitEvent(b->up_stream, b->in_free, 0);
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(b->stage_in, host_bodies_in4, bytes, cudaMemcpyHostToDevice, b->up_stream);
+        if (e == cudaSuccess) e = cudaEventRecord(b->in_ready, b->up_stream);
+        if (e == cudaSuccess) e = cudaStreamWaitEvent(b->stream, b->in_ready, 0);
+        if (e == cudaSuccess) e = launch_io_copy(b, a);
+        if (e == cudaSuccess) e = cudaEventRecord(b->in_free, b->stream);
+        if (e != cudaSuccess) return batch_fail(b, P3M_ERR_CUDA, cudaGetErrorString(e));
+    }
+    int st = batch_one_step(b);
+    if (st != P3M_OK) return st;
+    if (host_bodies_out4 && rows > 0) {
+        const p3m_batch::IoArgs* a = batch_io_args(b, false);  // the buffers after the step
+        if (!a) return batch_fail(b, P3M_ERR_OUT_OF_MEMORY, "row-copy arguments");
+        // The stepped bodies go to the staging buffer once the previous
+        // download has left it; the download then overlaps the next step.
+        e = cudaStreamWaitEvent(b->stream, b->out_free, 0);
+        if (e == cudaSuccess) e = launch_io_copy(b, a);
+        if (e == cudaSuccess) e = cudaEventRecord(b->out_ready, b->stream);
+        if (e == cudaSuccess) e = cudaStreamWaitEvent(b->down_stream, b->out_ready, 0);
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(host_bodies_out4, b->stage_out, bytes, cudaMemcpyDeviceToHost,
+                                b->down_stream);
+        if (e == cudaSuccess) e = cudaEventRecord(b->out_free, b->down_stream);
+        if (e != cudaSuccess) return batch_fail(b, P3M_ERR_CUDA, cudaGetErrorString(e));
     }
     return P3M_OK;
 }

@@ -362,6 +362,18 @@ int p3m_batch_autotune(p3m_batch* batch, int32_t trial_steps, int32_t* chosen);
  * needs every simulation at most 131,072 bodies; a batch with a larger one
  * runs the other form. */
 int p3m_batch_set_fused(p3m_batch* batch, int32_t enabled);
+/* One batch step with its host I/O pipelined against the neighbouring steps
+ * (p3m_step_io for the whole batch): host_bodies_in4 (may be NULL) holds
+ * every simulation's n bodies back to back, in simulation order, and becomes
+ * their bodies before the step; the stepped bodies go to host_bodies_out4
+ * (may be NULL) in the same layout. One copy per direction on the batch's
+ * copy streams, through device staging buffers (2 x 16 B per body of the
+ * simulations' capacities, allocated at the first call), and one row-copy
+ * launch each way between the staging and the simulations: the next call's
+ * upload overlaps this step and this step's download the next step. The
+ * arrays should be page-locked (p3m_host_alloc) and must stay valid, the
+ * input unchanged, until p3m_batch_synchronize returns. */
+int p3m_batch_step_io(p3m_batch* batch, const float* host_bodies_in4, float* host_bodies_out4);
 /* Persistent form of the fused step (default off; the autotuner picks the
  * faster form): one cooperative launch whose CTAs stay resident and run the
  * step's stages phase by phase, a bounded grid barrier between phases. Its
