@@ -42,6 +42,10 @@ namespace {
 constexpr int kThreads = 256;
 constexpr int kTileX = 256, kTileY = 16;  // at most; smaller meshes use the mesh size
 constexpr int kMaxRuns = 2 * (kTileY + 2);
+// tile_runs takes one lane of warp 0 per home row (TY + 2 of them) and
+// writes runs 2*lane and 2*lane + 1: every run slot is written only while
+// the home rows fit one warp.
+static_assert(kTileY + 2 <= 32, "tile_runs needs one lane per home row");
 constexpr int kTileCap = 16384;  // bodies a tile takes alone
 constexpr int kPiece = 2048;    // entries per piece of a heavy tile
 // Below this many bodies the entry-chunk kernel is used: a small mesh has
