@@ -52,6 +52,11 @@ __device__ __forceinline__ float2 local_acceleration(const TrajParams& P, float2
 }
 
 // accelerationAt (trajectory.comp:120-163): every lane returns the total.
+// A preview is one chain of dependent steps, so this is latency: the mesh
+// force's four taps are loaded first, and each lane's cells (c, c + 32, ...)
+// are taken two at a time with their count, start and mass loaded together,
+// so the stencil waits on fewer round trips. The arithmetic and its order
+// are those of one cell after the other.
 __device__ float2 acceleration_at(const TrajParams& P, float2 pos, const float2* __restrict__ force,
                                   const float4* __restrict__ entries,
                                   const int* __restrict__ cell_start,
@@ -60,34 +65,63 @@ __device__ float2 acceleration_at(const TrajParams& P, float2 pos, const float2*
     const KickParams& k = P.k;
     if (k.mutual == 0) return make_float2(k.field_x, k.field_y);
     const int lane = threadIdx.x & 31;
+    // interpolateForce's taps (:97-118).
+    const float gx = pos.x * (float)k.W - 0.5f, gy = pos.y * (float)k.H - 0.5f;
+    const float flx = floorf(gx), fly = floorf(gy);
+    const int bx = guard_coord(float_to_int(flx), k.MW), by = guard_coord(float_to_int(fly), k.MH);
+    const float tx = gx - flx, ty = gy - fly;
+    const int x0 = wrap_index(bx, k.MW), x1 = wrap_index(bx + 1, k.MW);
+    const int y0 = wrap_index(by, k.MH), y1 = wrap_index(by + 1, k.MH);
+    const float2 v00 = __ldg(&force[(size_t)y0 * k.MW + x0]);
+    const float2 v10 = __ldg(&force[(size_t)y0 * k.MW + x1]);
+    const float2 v01 = __ldg(&force[(size_t)y1 * k.MW + x0]);
+    const float2 v11 = __ldg(&force[(size_t)y1 * k.MW + x1]);
+
     float ax = 0.0f, ay = 0.0f;
     const int sx = 2 * k.rx + 1, cells = sx * (2 * k.ry + 1);
     const int hx = guard_coord(float_to_int(floorf(pos.x * (float)k.W)), k.W);
     const int hy = guard_coord(float_to_int(floorf(pos.y * (float)k.H)), k.H);
-    for (int c = lane; c < cells; c += 32) {
-        const int dy = c / sx - k.ry, dx = c % sx - k.rx;
-        const int cx = hx + dx, cy = hy + dy;
-        if (k.bounded != 0 && (cx < 0 || cy < 0 || cx >= k.W || cy >= k.H)) continue;
-        const int wx = wrap_index(cx, k.W), wy = wrap_index(cy, k.H);
-        const int index = wx + wy * k.W;
-        const int count = __ldg(&cell_count[index]);
-        const bool home = dx == 0 && dy == 0;
-        if (!home && count > k.exact) {
-            const float2 center = make_float2(((float)wx + 0.5f) / (float)k.W,
-                                              ((float)wy + 0.5f) / (float)k.H);
-            const float2 a = local_acceleration(P, center, pos,
-                                                (float)__ldg(&cell_mass[index]) / kCellMassUnits);
-            ax += a.x;
-            ay += a.y;
-        } else if (count > 0) {
-            const int limit = home ? k.home_limit : k.exact;
-            const int walk = count < limit ? count : limit;
-            const int start = __ldg(&cell_start[index]);
-            for (int e = 0; e < walk; ++e) {
-                const float4 o = __ldg(&entries[start + e]);
-                const float2 a = local_acceleration(P, make_float2(o.x, o.y), pos, o.z);
+    for (int base = lane; base < cells; base += 64) {
+        int index[2], wxs[2], wys[2], count[2], start[2];
+        uint32_t mass[2];
+        bool ok[2], home[2];
+#pragma unroll
+        for (int j = 0; j < 2; ++j) {
+            const int c = base + 32 * j;
+            const int dy = c / sx - k.ry, dx = c % sx - k.rx;
+            const int cx = hx + dx, cy = hy + dy;
+            ok[j] = c < cells && !(k.bounded != 0 && (cx < 0 || cy < 0 || cx >= k.W || cy >= k.H));
+            home[j] = dx == 0 && dy == 0;
+            wxs[j] = wrap_index(cx, k.W);
+            wys[j] = wrap_index(cy, k.H);
+            index[j] = wxs[j] + wys[j] * k.W;
+        }
+#pragma unroll
+        for (int j = 0; j < 2; ++j) {
+            count[j] = ok[j] ? __ldg(&cell_count[index[j]]) : 0;
+            start[j] = ok[j] ? __ldg(&cell_start[index[j]]) : 0;
+            mass[j] = ok[j] ? __ldg(&cell_mass[index[j]]) : 0u;
+        }
+#pragma unroll
+        for (int j = 0; j < 2; ++j) {
+            if (!ok[j]) continue;
+            if (!home[j] && count[j] > k.exact) {
+                const float2 center = make_float2(((float)wxs[j] + 0.5f) / (float)k.W,
+                                                  ((float)wys[j] + 0.5f) / (float)k.H);
+                const float2 a = local_acceleration(P, center, pos, (float)mass[j] / kCellMassUnits);
                 ax += a.x;
                 ay += a.y;
+            } else if (count[j] > 0) {
+                const int limit = home[j] ? k.home_limit : k.exact;
+                const int walk = count[j] < limit ? count[j] : limit;
+                const float4 o0 = __ldg(&entries[start[j]]);
+                const float4 o1 = walk > 1 ? __ldg(&entries[start[j] + 1]) : o0;
+                for (int e = 0; e < walk; ++e) {
+                    const float4 o = e == 0 ? o0 : (e == 1 ? o1 : __ldg(&entries[start[j] + e]));
+                    const float2 a = local_acceleration(P, make_float2(o.x, o.y), pos, o.z);
+                    ax += a.x;
+                    ay += a.y;
+                }
             }
         }
     }
@@ -100,17 +134,7 @@ __device__ float2 acceleration_at(const TrajParams& P, float2 pos, const float2*
     // taken anyway so that the lanes' step decisions cannot part.
     ax = __shfl_sync(0xffffffffu, ax, 0);
     ay = __shfl_sync(0xffffffffu, ay, 0);
-    // interpolateForce (:97-118) + the field, then the stencil sum.
-    const float gx = pos.x * (float)k.W - 0.5f, gy = pos.y * (float)k.H - 0.5f;
-    const float flx = floorf(gx), fly = floorf(gy);
-    const int bx = guard_coord(float_to_int(flx), k.MW), by = guard_coord(float_to_int(fly), k.MH);
-    const float tx = gx - flx, ty = gy - fly;
-    const int x0 = wrap_index(bx, k.MW), x1 = wrap_index(bx + 1, k.MW);
-    const int y0 = wrap_index(by, k.MH), y1 = wrap_index(by + 1, k.MH);
-    const float2 v00 = __ldg(&force[(size_t)y0 * k.MW + x0]);
-    const float2 v10 = __ldg(&force[(size_t)y0 * k.MW + x1]);
-    const float2 v01 = __ldg(&force[(size_t)y1 * k.MW + x0]);
-    const float2 v11 = __ldg(&force[(size_t)y1 * k.MW + x1]);
+    // The interpolated force + the field, then the stencil sum.
     const float lx = v00.x * (1.0f - tx) + v10.x * tx, ly = v00.y * (1.0f - tx) + v10.y * tx;
     const float ux = v01.x * (1.0f - tx) + v11.x * tx, uy = v01.y * (1.0f - tx) + v11.y * tx;
     float2 r;
