@@ -23,7 +23,9 @@
 namespace p3m {
 namespace {
 
-constexpr int kWarpsPerBlock = 4;
+// One preview (one warp) per CTA: a fan of a few hundred previews then
+// spreads over every SM instead of sharing a quarter of them.
+constexpr int kWarpsPerBlock = 1;
 constexpr int kVerticesPerStep = 6;  // GravityPipeline.kt:1623
 
 struct TrajParams {
