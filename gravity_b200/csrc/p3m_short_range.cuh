@@ -157,12 +157,7 @@ __device__ __forceinline__ StageBox stage_slots(bool valid, int hx, int hy,
     StageBox box;
     box.x0 = x0 - RX;
     box.y0 = y0 - RY;
-    const long long used = (long long)x1 - x0 + 1 + 2 * RX;  // columns the stencils read
-    // Row pitch padded to 4 mod 16 cells: a quarter warp of Morton-ordered
-    // targets (2 x 4 home cells) then reads its 16-byte slots from 8
-    // distinct bank groups, and a half warp (4 x 4) its 8-byte ones from 16,
-    // for every stencil offset; with a pitch of 0 mod 8 the rows collide.
-    const long long bw = used + ((4 - used) & 15);
+    const long long bw = (long long)x1 - x0 + 1 + 2 * RX;
     const long long bh = (long long)y1 - y0 + 1 + 2 * RY;
     box.w = (int)bw;
     box.staged = bw * bh <= kStageCells;
@@ -180,9 +175,8 @@ __device__ __forceinline__ StageBox stage_slots(bool valid, int hx, int hy,
                 if (c < cells) {
                     const int r = c / box.w;
                     const int cx = box.x0 + (c - r * box.w), cy = box.y0 + r;
-                    // Cells beyond a wall, and the padding, are never read.
-                    if (c - r * box.w < used &&
-                        (!p.bounded || (cx >= 0 && cx < p.W && cy >= 0 && cy < p.H))) {
+                    // Cells beyond a wall are never read.
+                    if (!p.bounded || (cx >= 0 && cx < p.W && cy >= 0 && cy < p.H)) {
                         const int cell = wrap_index(cy, p.H) * p.W + wrap_index(cx, p.W);
                         va[u] = __ldg(&slots[cell]);
                         vb[u] = __ldg(&slots_b[cell]);
