@@ -1,6 +1,6 @@
 """bench.py's multi-process contract on CPU (world size 2, gloo).
 
-The driver launches `bench.py --gpus N` under torchrun, one rank per GPU:
+A multi-GPU run launches `bench.py --gpus N` under torchrun, one rank per GPU:
 rank 0 alone prints the JSON line, the others exit 0, and device times are
 the maximum over ranks. These tests run the parts of that path that need no
 GPU: the reference arm under a two-rank torchrun, and the max-over-ranks
