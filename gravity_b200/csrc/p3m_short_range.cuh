@@ -263,11 +263,7 @@ __device__ __forceinline__ void stencil_sum(
                              __fadd2_rn(make_float2(s0.z, s0.w), oy), s1, ax2, ay2);
                 continue;
             }
-            // Count and start are loaded together (the start of a cell that
-            // is not walked is simply unused): a walked cell then waits on
-            // two round trips, count and start, then the entries, not three.
             const int count = __ldg(&cell_count[index]);
-            const int start = __ldg(&cell_start[index]);
             if (count == 0) continue;
             if (!home && count > p.exact) {
                 const float mass = (float)__ldg(&cell_mass[index]) * (1.0f / kCellMassUnits);
@@ -281,6 +277,7 @@ __device__ __forceinline__ void stencil_sum(
                 // the filler of an odd count have mass 0 and add nothing.
                 const int limit = home ? p.home_limit : p.exact;
                 const int walk = count < limit ? count : limit;
+                const int start = __ldg(&cell_start[index]);
                 const float2 sx = make_float2(shift_x[a], shift_x[a]);
                 const float2 sy = make_float2(shift_y, shift_y);
                 for (int e = 0; e < walk; e += 2) {
