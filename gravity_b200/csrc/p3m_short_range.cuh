@@ -229,7 +229,14 @@ __device__ __forceinline__ void stencil_sum(
     }
     const float2 neg_t = make_float2(-t.x, -t.y);
     float2 ax2 = make_float2(0.0f, 0.0f), ay2 = make_float2(0.0f, 0.0f);
-#pragma unroll
+    // The two-slot form unrolls the whole stencil (straight-line slot loads
+    // and pair terms); the list walk keeps its rows rolled: unrolled, its
+    // 49 branching cell walks outgrew the instruction cache (instruction-
+    // fetch stalls dominated its ncu profile). Both kernels are held to 64
+    // registers (4 CTAs per SM), which the rolled walk needs: without the
+    // bound it took 94 in the batched kernel and lost a third of the warps.
+    constexpr int kRowUnroll = EXACT == 2 ? 2 * RY + 1 : 1;
+#pragma unroll kRowUnroll
     for (int b = 0; b < 2 * RY + 1; ++b) {
         const int cy = hy + b - RY;
         if (p.bounded && (cy < 0 || cy >= p.H)) continue;
@@ -353,7 +360,7 @@ __device__ __forceinline__ void short_range_body(
 }
 
 template <int RX, int RY, int EXACT>
-__global__ void __launch_bounds__(256) short_range_kernel(
+__global__ void __launch_bounds__(256, 4) short_range_kernel(
     const float4* __restrict__ bodies, const float4* __restrict__ entries,
     const int* __restrict__ cell_start, const int* __restrict__ cell_count,
     const uint32_t* __restrict__ cell_mass, const float4* __restrict__ slots,
@@ -369,7 +376,7 @@ __global__ void __launch_bounds__(256) short_range_kernel(
 }
 
 template <int RX, int RY, int EXACT>
-__global__ void __launch_bounds__(256) short_range_batched_kernel(
+__global__ void __launch_bounds__(256, 4) short_range_batched_kernel(
     const ShortRangeArgs* __restrict__ args, const int* __restrict__ first, int sims) {
     const int2 sb = batch_block(first, sims);
     const ShortRangeArgs a = args[sb.x];
