@@ -734,13 +734,17 @@ __global__ void __launch_bounds__(kSortThreads) radix_hist_batched_kernel(
     radix_hist_body(sb.y, a.keys_in, a.n, a.shift, a.bits, a.tiles, a.hist);
 }
 
-__global__ void __launch_bounds__(kSortThreads) radix_scatter_batched_kernel(
+// The look-back scatter's CTA shape (512 threads of 8 keys: 64 registers,
+// twice the warps per SM of 256 threads of 16 keys at 127 registers) on
+// the same 4096-key tiles; a stable sort's output does not depend on it.
+__global__ void __launch_bounds__(kLookbackThreads) radix_scatter_batched_kernel(
     const RadixArgs* __restrict__ args, const int* __restrict__ first, int sims) {
     const int2 sb = batch_block(first, sims);
     const RadixArgs a = args[sb.x];
-    __shared__ ScatterShared<kSortMaxRadix> sm;
-    radix_scatter_body<false, kSortMaxRadix>(sm, sb.y, a.keys_in, a.vals_in, a.keys_out,
-                                             a.vals_out, a.n, a.shift, a.bits, a.tiles, a.hist);
+    __shared__ ScatterShared<kSortMaxRadix, kLookbackThreads> sm;
+    radix_scatter_body<false, kSortMaxRadix, kLookbackThreads, kLookbackItems>(
+        sm, sb.y, a.keys_in, a.vals_in, a.keys_out, a.vals_out, a.n, a.shift, a.bits, a.tiles,
+        a.hist);
 }
 
 __global__ void __launch_bounds__(kScanThreads) scan_batched_kernel(
@@ -980,7 +984,7 @@ int radix_scan_limit() { return kScanBlock; }
 P3M_BATCHED(batched_morton_keys, MortonArgs, morton_keys_batched_kernel, kBatchThreads)
 P3M_BATCHED(batched_radix_hist, RadixArgs, radix_hist_batched_kernel, kSortThreads)
 P3M_BATCHED(batched_scan, ScanArgs, scan_batched_kernel, kScanThreads)
-P3M_BATCHED(batched_radix_scatter, RadixArgs, radix_scatter_batched_kernel, kSortThreads)
+P3M_BATCHED(batched_radix_scatter, RadixArgs, radix_scatter_batched_kernel, kLookbackThreads)
 P3M_BATCHED(batched_permute, PermuteArgs, permute_batched_kernel, kBatchThreads)
 P3M_BATCHED(batched_cell_build, CellBuildArgs, cell_build_batched_kernel, kBatchThreads)
 P3M_BATCHED(batched_zero, ZeroArgs, zero_batched_kernel, kBatchThreads)
