@@ -1779,7 +1779,7 @@ int build_fused(p3m_batch* b, const std::vector<char>& sort, p3m_batch::Plan& pl
             role[mut[j]].sv = vin[j];
             ca.push_back({kin[j], vin[j], role[mut[j]].bodies, role[mut[j]].materials,
                           c->cell_start, c->cell_count, c->cell_mass, c->entries, b->n[mut[j]]});
-            cb.push_back((b->n[mut[j]] + 255) / 256);
+            cb.push_back((b->n[mut[j]] + p3m::kCellBuildBlockEntries - 1) / p3m::kCellBuildBlockEntries);
         }
         fb.stage(ca, cb, p3m::batched_cell_build, p3m::kPStageCellBuild, ++phase, 0);
     }

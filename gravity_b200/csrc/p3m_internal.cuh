@@ -386,6 +386,10 @@ struct PermuteArgs {
     const uint32_t* order; const float4* bodies; const float2* accel; const float4* materials;
     float4* bodies_out; float2* accel_out; float4* materials_out; uint32_t* destinations; int n;
 };
+// The cell build's entries per 256-thread block (two runs of 32 per warp):
+// every form (single context, batched, persistent) cuts its blocks so.
+constexpr int kCellBuildItems = 2;
+constexpr int kCellBuildBlockEntries = 256 * kCellBuildItems;
 struct CellBuildArgs {
     const uint32_t* keys; const uint32_t* ids; const float4* bodies; const float4* materials;
     int* cell_start; int* cell_count; uint32_t* cell_mass; float4* entries; int n;

@@ -685,8 +685,9 @@ __device__ __forceinline__ void build_finish(const BuildItem& it, int n, int* ce
     }
 }
 
-// One entry per thread: block b covers entries [256 b, 256 b + 256) (the
-// batched and persistent forms' block).
+// Each warp takes kCellBuildItems runs of 32 consecutive entries and issues
+// all their gathers before it uses the first, so twice the gathers are in
+// flight: block b of 256 threads covers entries [512 b, 512 b + 512).
 __device__ __forceinline__ void cell_build_body(int block, const uint32_t* __restrict__ keys,
                                                 const uint32_t* __restrict__ ids, int n,
                                                 const float4* __restrict__ bodies,
@@ -694,16 +695,18 @@ __device__ __forceinline__ void cell_build_body(int block, const uint32_t* __res
                                                 int* cell_start, int* cell_count,
                                                 uint32_t* cell_mass, float4* entries,
                                                 int fill_cells) {
-    BuildItem it;
-    build_load_keys(it, block * blockDim.x + threadIdx.x, keys, ids, n);
-    build_gather(it, bodies, materials);
-    build_finish(it, n, cell_start, cell_count, cell_mass, entries, fill_cells);
+    const int warp_base =
+        (block * (blockDim.x >> 5) + (threadIdx.x >> 5)) * (32 * kCellBuildItems);
+    BuildItem it[kCellBuildItems];
+#pragma unroll
+    for (int j = 0; j < kCellBuildItems; ++j)
+        build_load_keys(it[j], warp_base + 32 * j + (threadIdx.x & 31), keys, ids, n);
+#pragma unroll
+    for (int j = 0; j < kCellBuildItems; ++j) build_gather(it[j], bodies, materials);
+#pragma unroll
+    for (int j = 0; j < kCellBuildItems; ++j)
+        build_finish(it[j], n, cell_start, cell_count, cell_mass, entries, fill_cells);
 }
-
-// Entries per thread of the single-context cell build: each warp takes
-// kBuildItems runs of 32 consecutive entries and issues all their gathers
-// before it uses the first, so twice the gathers are in flight.
-constexpr int kBuildItems = 2;
 
 __global__ void cell_build_kernel(const uint32_t* __restrict__ keys, const uint32_t* __restrict__ ids,
                                   int n, const float4* __restrict__ bodies,
@@ -714,16 +717,8 @@ __global__ void cell_build_kernel(const uint32_t* __restrict__ keys, const uint3
     // A sort whose look-back gave up leaves keys and IDs that are not a
     // permutation: build nothing (every cell stays empty).
     if (sort_failed != nullptr && *sort_failed != 0u) return;
-    const int warp_base = (blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5)) * (32 * kBuildItems);
-    BuildItem it[kBuildItems];
-#pragma unroll
-    for (int j = 0; j < kBuildItems; ++j)
-        build_load_keys(it[j], warp_base + 32 * j + (threadIdx.x & 31), keys, ids, n);
-#pragma unroll
-    for (int j = 0; j < kBuildItems; ++j) build_gather(it[j], bodies, materials);
-#pragma unroll
-    for (int j = 0; j < kBuildItems; ++j)
-        build_finish(it[j], n, cell_start, cell_count, cell_mass, entries, fill_cells);
+    cell_build_body(blockIdx.x, keys, ids, n, bodies, materials, cell_start, cell_count, cell_mass,
+                    entries, fill_cells);
 }
 
 // ------------------------------------------------------- batched launches
@@ -999,7 +994,7 @@ cudaError_t launch_cell_build(const uint32_t* keys, const uint32_t* ids, int n, 
             return cudaMemsetAsync(cell_start, 0, ((size_t)fill_cells + 1) * sizeof(int), stream);
         return cudaSuccess;
     }
-    launch_chained(cell_build_kernel, blocks_for(n, 256 * kBuildItems), 256, 0, stream, keys, ids, n, bodies, materials,
+    launch_chained(cell_build_kernel, blocks_for(n, kCellBuildBlockEntries), 256, 0, stream, keys, ids, n, bodies, materials,
                                                               cell_start, cell_count, cell_mass,
                                                               entries, fill_cells, sort_failed);
     count_launches(1);
