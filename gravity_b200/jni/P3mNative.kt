@@ -40,6 +40,11 @@ internal object P3mNative {
     external fun setMassExcess(ctx: Long, excess: Float): Int
     external fun initializeAcceleration(ctx: Long, n: Int): Int
     external fun step(ctx: Long, n: Int, steps: Int): Int
+    /** One step with its upload and read-back pipelined against the
+     *  neighbouring steps (p3m_step_io): [bodiesIn] becomes the first [n]
+     *  bodies, the stepped bodies go to [bodiesOut]. Direct buffers, left
+     *  untouched until [synchronize]. */
+    external fun stepIo(ctx: Long, n: Int, bodiesIn: FloatBuffer?, bodiesOut: FloatBuffer?): Int
     external fun synchronize(ctx: Long): Int
 
     /** p3m_status -> the reference's exceptions: invalid argument, capacity and

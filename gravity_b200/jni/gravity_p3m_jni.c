@@ -128,6 +128,15 @@ JNIEXPORT jint JNICALL FN(step)(JNIEnv* env, jclass cls, jlong h, jint n, jint s
     return p3m_step(CTX(h), n, steps);
 }
 
+/* A frame's upload, step and read-back with the copies pipelined against the
+ * neighbouring frames (uploadBodies :720-770, step, the readback :378-443):
+ * both buffers must be direct and stay untouched until synchronize. */
+JNIEXPORT jint JNICALL FN(stepIo)(JNIEnv* env, jclass cls, jlong h, jint n, jobject bodies_in,
+                                  jobject bodies_out) {
+    (void)cls;
+    return p3m_step_io(CTX(h), n, direct(env, bodies_in), direct(env, bodies_out));
+}
+
 /* Waits for the context's work; reports device-detected failures. */
 JNIEXPORT jint JNICALL FN(synchronize)(JNIEnv* env, jclass cls, jlong h) {
     (void)env; (void)cls;

@@ -27,6 +27,7 @@ jint Java_dev_gravity_P3mNative_destroy(JNIEnv*, jclass, jlong);
 jstring Java_dev_gravity_P3mNative_lastError(JNIEnv*, jclass, jlong);
 jint Java_dev_gravity_P3mNative_download(JNIEnv*, jclass, jlong, jint, jobject, jobject);
 jint Java_dev_gravity_P3mNative_step(JNIEnv*, jclass, jlong, jint, jint);
+jint Java_dev_gravity_P3mNative_stepIo(JNIEnv*, jclass, jlong, jint, jobject, jobject);
 
 /* GravityFieldConfig defaults (GravityConfig.kt:641-654) with the given grid. */
 int harness_create(int grid_width, int grid_height, long long* handle, char* message, int cap) {
@@ -49,4 +50,8 @@ int harness_download(long long handle, int n, float* bodies) {
 
 int harness_step(long long handle, int n, int steps) {
     return Java_dev_gravity_P3mNative_step(&env, NULL, handle, n, steps);
+}
+
+int harness_step_io(long long handle, int n, float* bodies_in, float* bodies_out) {
+    return Java_dev_gravity_P3mNative_stepIo(&env, NULL, handle, n, bodies_in, bodies_out);
 }

@@ -40,6 +40,8 @@ def harness(tmp_path_factory):
     h.harness_destroy.argtypes = [ctypes.c_longlong]
     h.harness_download.argtypes = [ctypes.c_longlong, ctypes.c_int, ctypes.c_void_p]
     h.harness_step.argtypes = [ctypes.c_longlong, ctypes.c_int, ctypes.c_int]
+    h.harness_step_io.argtypes = [ctypes.c_longlong, ctypes.c_int, ctypes.c_void_p,
+                                  ctypes.c_void_p]
     del lib
     return h
 
@@ -73,3 +75,5 @@ def test_null_context_calls_are_argument_errors(harness):
     buf = (ctypes.c_float * 16)()
     assert harness.harness_download(0, 4, ctypes.cast(buf, ctypes.c_void_p)) == _abi.P3M_ERR_INVALID_ARGUMENT
     assert harness.harness_step(0, 4, 1) == _abi.P3M_ERR_INVALID_ARGUMENT
+    assert harness.harness_step_io(0, 4, ctypes.cast(buf, ctypes.c_void_p),
+                                   ctypes.cast(buf, ctypes.c_void_p)) == _abi.P3M_ERR_INVALID_ARGUMENT
