@@ -118,7 +118,7 @@ __device__ __forceinline__ void pair_add2_gm(const PairConst& k, float2 dx, floa
 constexpr int kStageCells = 1536;
 
 struct StageBox {
-    int x0, y0, w;  // box origin (unwrapped cell coordinates) and width
+    int x0, y0, w, h;  // box origin (unwrapped cell coordinates), width, height
     bool staged;
 };
 
@@ -128,13 +128,11 @@ struct StageBox {
 // from shared memory instead of each lane fetching its 48 cells through L1.
 // A CTA whose box is larger than kStageCells (a patch split across the torus
 // seam, or sparse bodies) reads the table from global memory. All threads of
-// the CTA take part (none may have returned).
+// the CTA take part (none may have returned). stage_box finds the box (one
+// barrier); stage_fill loads it (another barrier), so a caller can issue
+// loads of its own between the two.
 template <int RX, int RY>
-__device__ __forceinline__ StageBox stage_slots(bool valid, int hx, int hy,
-                                                const float4* __restrict__ slots,
-                                                const float2* __restrict__ slots_b,
-                                                const KickParams& p, float4* st_a, float2* st_b,
-                                                int* red) {
+__device__ __forceinline__ StageBox stage_box(bool valid, int hx, int hy, int* red) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, warps = blockDim.x >> 5;
     const int mnx = __reduce_min_sync(0xffffffffu, valid ? hx : 0x7fffffff);
     const int mxx = __reduce_max_sync(0xffffffffu, valid ? hx : (int)0x80000000);
@@ -161,8 +159,15 @@ __device__ __forceinline__ StageBox stage_slots(bool valid, int hx, int hy,
     const long long bh = (long long)y1 - y0 + 1 + 2 * RY;
     box.w = (int)bw;
     box.staged = bw * bh <= kStageCells;
+    box.h = box.staged ? (int)bh : 0;
+    return box;
+}
+
+__device__ __forceinline__ void stage_fill(const StageBox& box, const float4* __restrict__ slots,
+                                           const float2* __restrict__ slots_b,
+                                           const KickParams& p, float4* st_a, float2* st_b) {
     if (box.staged) {
-        const int cells = (int)(bw * bh);
+        const int cells = box.w * box.h;
         constexpr int kBatch = 4;
         for (int c0 = threadIdx.x; c0 < cells; c0 += kBatch * blockDim.x) {
             float4 va[kBatch];
@@ -177,9 +182,16 @@ __device__ __forceinline__ StageBox stage_slots(bool valid, int hx, int hy,
                     const int cx = box.x0 + (c - r * box.w), cy = box.y0 + r;
                     // Cells beyond a wall are never read.
                     if (!p.bounded || (cx >= 0 && cx < p.W && cy >= 0 && cy < p.H)) {
-                        const int cell = wrap_index(cy, p.H) * p.W + wrap_index(cx, p.W);
+                        const int wx = wrap_index(cx, p.W), wy = wrap_index(cy, p.H);
+                        const int cell = wy * p.W + wx;
                         va[u] = __ldg(&slots[cell]);
                         vb[u] = __ldg(&slots_b[cell]);
+                        // The slots moved to the box's image of the cell, as
+                        // the global-table path shifts them per stencil cell.
+                        const float sx = (float)(cx - wx) * (1.0f / (float)p.W);
+                        const float sy = (float)(cy - wy) * (1.0f / (float)p.H);
+                        va[u] = make_float4(va[u].x + sx, va[u].y + sx, va[u].z + sy,
+                                            va[u].w + sy);
                     }
                 }
             }
@@ -194,29 +206,56 @@ __device__ __forceinline__ StageBox stage_slots(bool valid, int hx, int hy,
         }
     }
     __syncthreads();
-    return box;
 }
+
+// One step of a list walk: entries o0 and o1 (o1 present when has1) of a
+// cell whose image shift is (sx, sy), against the target at -(ntx, nty). The
+// target itself and the filler of an odd count have mass 0 and add nothing.
+__device__ __forceinline__ void walk_step(const PairConst& k, float4 o0, float4 o1, bool has1,
+                                          uint32_t id, float2 sx, float2 sy, float2 ntx,
+                                          float2 nty, float2& ax2, float2& ay2) {
+    const float m0 = __float_as_uint(o0.w) != id ? o0.z : 0.0f;
+    const float m1 = has1 && __float_as_uint(o1.w) != id ? o1.z : 0.0f;
+    // (o + shift) - t, rounded as the scalar form does.
+    const float2 dx = __fadd2_rn(__fadd2_rn(make_float2(o0.x, o1.x), sx), ntx);
+    const float2 dy = __fadd2_rn(__fadd2_rn(make_float2(o0.y, o1.y), sy), nty);
+    pair_add2_gm(k, dx, dy,
+                 __fmul2_rn(make_float2(k.g_over_m, k.g_over_m), make_float2(m0, m1)), ax2,
+                 ay2);
+}
+
+// The home cell of the two-slot form, read before the stencil: its list walk
+// (min(count, home_limit) entries from `start`) and the first two entries,
+// loaded while the CTA stages its slots.
+struct HomeCell {
+    int walk, start;
+    float4 e0, e1;
+};
 
 // The stencil sum of one target (its position t, ID id, home cell hx, hy),
 // accumulated per packed half: the two slots of a non-home cell (EXACT = 2),
 // two list entries at a time in a walked cell, and a monopole in .x.
 // STAGED: the slots come from the CTA's shared-memory box (base `sbase`, row
 // pitch `bw`), else from the global table. The two instantiations keep the
-// CTA-uniform choice out of the unrolled 49-cell loop.
+// CTA-uniform choice out of the unrolled 49-cell loop. The two-slot form sums
+// the home cell (`home`) first, then the other cells row by row; the list
+// form takes every cell, the home cell included, row by row.
 template <int RX, int RY, int EXACT, bool STAGED>
 __device__ __forceinline__ void stencil_sum(
     float4 t, uint32_t id, int hx, int hy, const PairConst& k, const KickParams& p,
     const float4* __restrict__ entries, const int* __restrict__ cell_start,
     const int* __restrict__ cell_count, const uint32_t* __restrict__ cell_mass,
     const float4* __restrict__ slots, const float2* __restrict__ slots_b, const float4* st_a,
-    const float2* st_b, int sbase, int bw, float2& acc_x, float2& acc_y) {
+    const float2* st_b, int sbase, int bw, const HomeCell& home_cell, float2& acc_x,
+    float2& acc_y) {
     const float inv_w = 1.0f / (float)p.W, inv_h = 1.0f / (float)p.H;
-    // Per stencil column: wrapped column, periodic image shift, validity.
-    // off_x: the image shift less the target's x, so that a source at x on
-    // that column is at dx = x + off_x (exactly x - t.x where no wrap).
+    // Per stencil column: wrapped column, periodic image shift, validity. A
+    // source at x on a column is at dx = (x + shift) - t.x, rounded twice as
+    // written (exactly x - t.x where the column did not wrap). The staged
+    // slots carry their shift already, so the staged form keeps none of
+    // these per column but the validity.
     int col[2 * RX + 1];
     float shift_x[2 * RX + 1];
-    float off_x[2 * RX + 1];
     bool ok_x[2 * RX + 1];
 #pragma unroll
     for (int a = 0; a < 2 * RX + 1; ++a) {
@@ -224,11 +263,23 @@ __device__ __forceinline__ void stencil_sum(
         const int wx = wrap_index(cx, p.W);
         col[a] = wx;
         shift_x[a] = (float)(cx - wx) * inv_w;
-        off_x[a] = shift_x[a] - t.x;
         ok_x[a] = !p.bounded || (cx >= 0 && cx < p.W);
     }
     const float2 neg_t = make_float2(-t.x, -t.y);
+    const float2 ntx = make_float2(neg_t.x, neg_t.x), nty = make_float2(neg_t.y, neg_t.y);
     float2 ax2 = make_float2(0.0f, 0.0f), ay2 = make_float2(0.0f, 0.0f);
+    if (EXACT == 2 && home_cell.walk > 0) {
+        // The home cell never wraps: no image shift.
+        const float2 zero = make_float2(0.0f, 0.0f);
+        walk_step(k, home_cell.e0, home_cell.e1, home_cell.walk > 1, id, zero, zero, ntx, nty,
+                  ax2, ay2);
+        for (int e = 2; e < home_cell.walk; e += 2) {
+            const float4 o0 = __ldg(&entries[home_cell.start + e]);
+            const bool has1 = e + 1 < home_cell.walk;
+            const float4 o1 = has1 ? __ldg(&entries[home_cell.start + e + 1]) : o0;
+            walk_step(k, o0, o1, has1, id, zero, zero, ntx, nty, ax2, ay2);
+        }
+    }
     // The two-slot form unrolls the whole stencil (straight-line slot loads
     // and pair terms); the list walk keeps its rows rolled: unrolled, its
     // 49 branching cell walks outgrew the instruction cache (instruction-
@@ -244,30 +295,33 @@ __device__ __forceinline__ void stencil_sum(
         const int row = wy * p.W;
         const float shift_y = (float)(cy - wy) * inv_h;
         const float cyr = ((float)wy + 0.5f) * inv_h;  // wrapped row centre
-        const float off_y = shift_y - t.y;
 #pragma unroll
         for (int a = 0; a < 2 * RX + 1; ++a) {
             if (!ok_x[a]) continue;
             const int index = row + col[a];
             const bool home = (a == RX) && (b == RY);
-            if (EXACT == 2 && !home) {
+            if (EXACT == 2 && home) continue;  // summed first
+            if (EXACT == 2) {
                 // The cell's two slots, prepared once per step (cell_slots):
                 // (x0, x1, y0, y1) and (G m0 / M_tot, G m1 / M_tot), so each
                 // packed operand is one loaded register pair.
                 float4 s0;
-                float2 s1;
+                float2 s1, dx, dy;
                 if (STAGED) {
                     const int si = sbase + b * bw + a;
                     s0 = st_a[si];
                     s1 = st_b[si];
+                    dx = __fadd2_rn(make_float2(s0.x, s0.y), ntx);
+                    dy = __fadd2_rn(make_float2(s0.z, s0.w), nty);
                 } else {
                     s0 = __ldg(&slots[index]);
                     s1 = __ldg(&slots_b[index]);
+                    const float2 sx = make_float2(shift_x[a], shift_x[a]);
+                    const float2 sy = make_float2(shift_y, shift_y);
+                    dx = __fadd2_rn(__fadd2_rn(make_float2(s0.x, s0.y), sx), ntx);
+                    dy = __fadd2_rn(__fadd2_rn(make_float2(s0.z, s0.w), sy), nty);
                 }
-                const float2 ox = make_float2(off_x[a], off_x[a]);
-                const float2 oy = make_float2(off_y, off_y);
-                pair_add2_gm(k, __fadd2_rn(make_float2(s0.x, s0.y), ox),
-                             __fadd2_rn(make_float2(s0.z, s0.w), oy), s1, ax2, ay2);
+                pair_add2_gm(k, dx, dy, s1, ax2, ay2);
                 continue;
             }
             const int count = __ldg(&cell_count[index]);
@@ -280,8 +334,7 @@ __device__ __forceinline__ void stencil_sum(
                 ax2.x = ax;
                 ay2.x = ay;
             } else {
-                // The list walk, two entries at a time; the target itself and
-                // the filler of an odd count have mass 0 and add nothing.
+                // The list walk, two entries at a time.
                 const int limit = home ? p.home_limit : p.exact;
                 const int walk = count < limit ? count : limit;
                 const int start = __ldg(&cell_start[index]);
@@ -291,17 +344,7 @@ __device__ __forceinline__ void stencil_sum(
                     const float4 o0 = __ldg(&entries[start + e]);
                     const bool has1 = e + 1 < walk;
                     const float4 o1 = has1 ? __ldg(&entries[start + e + 1]) : o0;
-                    const float m0 = __float_as_uint(o0.w) != id ? o0.z : 0.0f;
-                    const float m1 = has1 && __float_as_uint(o1.w) != id ? o1.z : 0.0f;
-                    // (o + shift) - t, rounded as the scalar form does.
-                    const float2 dx = __fadd2_rn(__fadd2_rn(make_float2(o0.x, o1.x), sx),
-                                                 make_float2(neg_t.x, neg_t.x));
-                    const float2 dy = __fadd2_rn(__fadd2_rn(make_float2(o0.y, o1.y), sy),
-                                                 make_float2(neg_t.y, neg_t.y));
-                    pair_add2_gm(k, dx, dy,
-                                 __fmul2_rn(make_float2(k.g_over_m, k.g_over_m),
-                                            make_float2(m0, m1)),
-                                 ax2, ay2);
+                    walk_step(k, o0, o1, has1, id, sx, sy, ntx, nty, ax2, ay2);
                 }
             }
         }
@@ -335,14 +378,30 @@ __device__ __forceinline__ void short_range_body(
     const int hx = guard_coord(float_to_int(floorf(t.x * (float)p.W)), p.W);
     const int hy = guard_coord(float_to_int(floorf(t.y * (float)p.H)), p.H);
 
-    StageBox box{0, 0, 0, false};
+    StageBox box{0, 0, 0, 0, false};
+    HomeCell home{0, 0, make_float4(0.0f, 0.0f, 0.0f, 0.0f), make_float4(0.0f, 0.0f, 0.0f, 0.0f)};
     int sbase = 0;
     float4* st_a = nullptr;
     float2* st_b = nullptr;
     if (EXACT == 2) {
         st_a = sm->a;
         st_b = sm->b;
-        box = stage_slots<RX, RY>(valid, hx, hy, slots, slots_b, p, sm->a, sm->b, sm->red);
+        // The home cell's count and start go out with the body; its first
+        // two entries between the staging barriers. Their round trips then
+        // overlap the staging instead of stalling the stencil.
+        int count = 0;
+        if (valid) {
+            const int cell = hy * p.W + hx;
+            count = __ldg(&cell_count[cell]);
+            home.start = __ldg(&cell_start[cell]);
+        }
+        home.walk = count < p.home_limit ? count : p.home_limit;
+        box = stage_box<RX, RY>(valid, hx, hy, sm->red);
+        stage_fill(box, slots, slots_b, p, sm->a, sm->b);
+        if (home.walk > 0) {
+            home.e0 = __ldg(&entries[home.start]);
+            home.e1 = home.walk > 1 ? __ldg(&entries[home.start + 1]) : home.e0;
+        }
         if (!valid) return;
         if (box.staged) sbase = (hy - RY - box.y0) * box.w + (hx - RX - box.x0);
     }
@@ -351,11 +410,11 @@ __device__ __forceinline__ void short_range_body(
     if (EXACT == 2 && box.staged)
         stencil_sum<RX, RY, EXACT, true>(t, id, hx, hy, k, p, entries, cell_start, cell_count,
                                          cell_mass, slots, slots_b, st_a, st_b, sbase, box.w,
-                                         acc_x, acc_y);
+                                         home, acc_x, acc_y);
     else
         stencil_sum<RX, RY, EXACT, false>(t, id, hx, hy, k, p, entries, cell_start, cell_count,
                                           cell_mass, slots, slots_b, st_a, st_b, sbase, box.w,
-                                          acc_x, acc_y);
+                                          home, acc_x, acc_y);
     a_short[id] = make_float2(acc_x.x + acc_x.y, acc_y.x + acc_y.y);
 }
 
