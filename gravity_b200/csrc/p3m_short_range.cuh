@@ -168,6 +168,11 @@ __device__ __forceinline__ void stage_fill(const StageBox& box, const float4* __
                                            const KickParams& p, float4* st_a, float2* st_b) {
     if (box.staged) {
         const int cells = box.w * box.h;
+        // Row of box cell c: floor((c + 0.5) / w) in FP32 instead of an
+        // integer division. (c + 0.5) / w lies at least 0.5 / w from an
+        // integer, and for c < kStageCells the two roundings move it by less
+        // than 2e-4 / w, so the floor is exact (checked for every w and c).
+        const float inv_w = 1.0f / (float)box.w;
         constexpr int kBatch = 4;
         for (int c0 = threadIdx.x; c0 < cells; c0 += kBatch * blockDim.x) {
             float4 va[kBatch];
@@ -178,7 +183,7 @@ __device__ __forceinline__ void stage_fill(const StageBox& box, const float4* __
                 va[u] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
                 vb[u] = make_float2(0.0f, 0.0f);
                 if (c < cells) {
-                    const int r = c / box.w;
+                    const int r = (int)(((float)c + 0.5f) * inv_w);
                     const int cx = box.x0 + (c - r * box.w), cy = box.y0 + r;
                     // Cells beyond a wall are never read.
                     if (!p.bounded || (cx >= 0 && cx < p.W && cy >= 0 && cy < p.H)) {
