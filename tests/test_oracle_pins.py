@@ -169,7 +169,8 @@ def test_walls_need_the_doubled_mesh_to_fit():
 @pytest.mark.parametrize("n,scale", [(50_000, 65536), (100_000, 40000), (400_000, 10000),
                                      (8_000_000, 500)])
 def test_mass_scale(n, scale):
-    """GravityPipeline.kt:1546-1547; the survey's per-workload table."""
+    """GravityPipeline.kt:1546-1547: the fixed-point mass scale falls as the
+    body count grows, so the summed density stays inside 32 bits."""
     assert mass_scale_for(n) == scale
     assert oracle.mass_scale(n) == scale
 
