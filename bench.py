@@ -34,7 +34,10 @@ Printed (rank 0, one JSON line):
   roofline  the dominant stage's algorithmic bytes / its event-timed average
             duration, against the measured HBM copy bandwidth; every stage's
             fraction is in `stages`, the deposit's and the kick's also in
-            `roofline_hbm_stages`.
+            `roofline_hbm_stages`. The short range is bound by its exp2 and
+            reciprocal operations, not by DRAM: `roofline.xu` gives that
+            floor (the MUFU unit's rate at the sampled SM clock) and the
+            fraction of it reached.
   force_rms_err_vs_fp64_by_form  RMS force error against the FP64 direct sum
             on one seeded 4096-body subsample for the int64 form, the uint32
             form and the CPU oracle's FP32 path.
@@ -287,6 +290,30 @@ class ClockSampler:
 
 
 # -------------------------------------------------------------- CPU baseline
+def short_range_xu(sc, ms_per_launch: float, clk) -> dict | None:
+    """The exp2/reciprocal floor of the two-slot short range: per body and
+    non-home stencil cell two exp2 and two reciprocals (one pair term per
+    slot), on the MUFU unit's 16 results per clock per SM. The home cell's
+    walk adds a few more, so the floor is a lower bound. None for the list
+    form (the exact limit is not 2, or under one body per two cells)."""
+    import torch
+    from gravity_b200.config import neighbor_radii
+
+    g = sc.config.gravity
+    cells = g.grid_width * g.grid_height
+    if g.exact_neighbor_body_limit != 2 or 2 * sc.n < cells or not ms_per_launch:
+        return None
+    rx, ry = neighbor_radii(sc.config)
+    ops = 4 * ((2 * rx + 1) * (2 * ry + 1) - 1) * sc.n
+    sms = torch.cuda.get_device_properties(0).multi_processor_count
+    mhz = (clk or {}).get("sm_mhz") or (clk or {}).get("sm_max_mhz")
+    if not mhz:
+        return None
+    floor_ms = ops / (16.0 * sms * mhz * 1e6) * 1e3
+    return {"unit": "MUFU ops (ex2, rcp)", "ops_per_launch": ops, "per_sm_clock": 16,
+            "sms": sms, "sm_mhz": mhz, "floor_ms": floor_ms, "frac": floor_ms / ms_per_launch}
+
+
 def cpu_oracle_rate(sc, budget_s: float, threads: int | None = None, warmup: int = 1,
                     max_steps: int | None = None):
     """bodies*steps/s of the CPU oracle on this workload: initialisation and
@@ -700,6 +727,8 @@ def run_b200(args, ws, rank, local):
             plain = {"workload": "plummer_walls", "config": workload_config(psc, args, "plummer_walls"),
                      "value": pm["value"], "ms_per_step": pm["ms_per_step"], "steps": psteps,
                      "e2e": pm["e2e"], "force_rms_err_vs_fp64": perr, "stages": prow,
+                     "short_range_xu": short_range_xu(
+                         psc, prow.get("short_range", {}).get("ms_per_launch"), clk),
                      "autotuned": pm["autotuned"], "gpu_launches": pm["launches"]}
 
     if rank == 0:
@@ -730,7 +759,9 @@ def run_b200(args, ws, rank, local):
             "autotuned": m["autotuned"],
             "roofline": {"bound": "hbm", "kernel": dominant, "achieved": achieved, "peak": peak,
                          "unit": "GB/s", "frac": achieved / peak if achieved else None,
-                         "traffic": traffic, "peak_source": peak_kind},
+                         "traffic": traffic, "peak_source": peak_kind,
+                         "xu": short_range_xu(sc, dom["ms_per_launch"], clk)
+                         if dominant == "short_range" else None},
             "roofline_hbm_stages": {k: stage_rows[k]["frac_of_measured_hbm"]
                                     for k in ("deposit", "kick") if k in stage_rows},
             "stages": stage_rows,
