@@ -292,17 +292,23 @@ __device__ __forceinline__ void stencil_sum(
     // registers (4 CTAs per SM), which the rolled walk needs: without the
     // bound it took 94 in the batched kernel and lost a third of the warps.
     constexpr int kRowUnroll = EXACT == 2 ? 2 * RY + 1 : 1;
+    // The staged two-slot loop takes every stencil cell: the stage holds
+    // massless slots beyond a wall, whose terms are exact zeros (G m = 0
+    // times a finite weight), and adding a zero leaves the accumulators'
+    // bits as they are (they start at +0 and never become -0), the same
+    // bits as skipping the cell as the other paths do.
+    constexpr bool kWallChecks = !(EXACT == 2 && STAGED);
 #pragma unroll kRowUnroll
     for (int b = 0; b < 2 * RY + 1; ++b) {
         const int cy = hy + b - RY;
-        if (p.bounded && (cy < 0 || cy >= p.H)) continue;
+        if (kWallChecks && p.bounded && (cy < 0 || cy >= p.H)) continue;
         const int wy = wrap_index(cy, p.H);
         const int row = wy * p.W;
         const float shift_y = (float)(cy - wy) * inv_h;
         const float cyr = ((float)wy + 0.5f) * inv_h;  // wrapped row centre
 #pragma unroll
         for (int a = 0; a < 2 * RX + 1; ++a) {
-            if (!ok_x[a]) continue;
+            if (kWallChecks && !ok_x[a]) continue;
             const int index = row + col[a];
             const bool home = (a == RX) && (b == RY);
             if (EXACT == 2 && home) continue;  // summed first
