@@ -173,7 +173,10 @@ __device__ __forceinline__ void stage_fill(const StageBox& box, const float4* __
         // integer, and for c < kStageCells the two roundings move it by less
         // than 2e-4 / w, so the floor is exact (checked for every w and c).
         const float inv_w = 1.0f / (float)box.w;
-        constexpr int kBatch = 4;
+        // Two cells per thread per round: 512 at 256 threads, a typical box
+        // (about 22 x 22) in one round, with registers left for the home
+        // cell's entries in flight meanwhile.
+        constexpr int kBatch = 2;
         for (int c0 = threadIdx.x; c0 < cells; c0 += kBatch * blockDim.x) {
             float4 va[kBatch];
             float2 vb[kBatch];
@@ -408,11 +411,11 @@ __device__ __forceinline__ void short_range_body(
         }
         home.walk = count < p.home_limit ? count : p.home_limit;
         box = stage_box<RX, RY>(valid, hx, hy, sm->red);
-        stage_fill(box, slots, slots_b, p, sm->a, sm->b);
         if (home.walk > 0) {
             home.e0 = __ldg(&entries[home.start]);
             home.e1 = home.walk > 1 ? __ldg(&entries[home.start + 1]) : home.e0;
         }
+        stage_fill(box, slots, slots_b, p, sm->a, sm->b);
         if (!valid) return;
         if (box.staged) sbase = (hy - RY - box.y0) * box.w + (hx - RX - box.x0);
     }
