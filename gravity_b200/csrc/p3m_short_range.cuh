@@ -246,7 +246,7 @@ struct HomeCell {
 // STAGED: the slots come from the CTA's shared-memory box (base `sbase`, row
 // pitch `bw`), else from the global table. The two instantiations keep the
 // CTA-uniform choice out of the unrolled 49-cell loop. The two-slot form sums
-// the home cell (`home`) first, then the other cells row by row; the list
+// the home cell (`home_cell`) first, then the other cells row by row; the list
 // form takes every cell, the home cell included, row by row.
 template <int RX, int RY, int EXACT, bool STAGED>
 __device__ __forceinline__ void stencil_sum(
