@@ -188,7 +188,8 @@ __device__ __forceinline__ void stage_fill(const StageBox& box, const float4* __
                 if (c < cells) {
                     const int r = (int)(((float)c + 0.5f) * inv_w);
                     const int cx = box.x0 + (c - r * box.w), cy = box.y0 + r;
-                    // Cells beyond a wall are never read.
+                    // Cells beyond a wall are never read: their slots stay
+                    // massless zeros.
                     if (!p.bounded || (cx >= 0 && cx < p.W && cy >= 0 && cy < p.H)) {
                         const int wx = wrap_index(cx, p.W), wy = wrap_index(cy, p.H);
                         const int cell = wy * p.W + wx;
@@ -260,8 +261,8 @@ __device__ __forceinline__ void stencil_sum(
     // Per stencil column: wrapped column, periodic image shift, validity. A
     // source at x on a column is at dx = (x + shift) - t.x, rounded twice as
     // written (exactly x - t.x where the column did not wrap). The staged
-    // slots carry their shift already, so the staged form keeps none of
-    // these per column but the validity.
+    // slots carry their shift already, so the staged two-slot loop needs
+    // none of these per column.
     int col[2 * RX + 1];
     float shift_x[2 * RX + 1];
     bool ok_x[2 * RX + 1];
